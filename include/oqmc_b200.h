@@ -1,0 +1,149 @@
+/*
+ * oqmc_b200.h -- C ABI of liboqmc_b200.so, the B200 (sm_100a) kernels for
+ * the GTO variational Monte Carlo hot path of OmegaQMC: Slater-Jastrow
+ * wavefunction evaluation and single-electron Metropolis sweeps.
+ *
+ * Conventions
+ *  - All array arguments are DEVICE pointers (plain memory the caller owns;
+ *    the library borrows them for the duration of the enqueued work), except
+ *    the oqmc_system_desc tables, which are host memory read at create time.
+ *  - Walkers are (W, n_e, 3) FP64 arrays, electrons in the reference's spin
+ *    layout: spin up at even positions, spin down at odd positions.
+ *  - Work is enqueued on the caller's stream (cudaStream_t passed as void*;
+ *    NULL = legacy default stream) and the call returns without waiting,
+ *    except oqmc_get_flags, which synchronises the stream.
+ *  - Every function returns 0 on success or a negative OQ_ERR_* code and
+ *    never aborts; oqmc_last_error() describes the last failure.
+ *  - A context is bound to the device that was current at create time and
+ *    is not thread-safe: use one context per host thread / stream.
+ *
+ * The reference (myung-group/OmegaQMC) is Python/JAX with no native layer:
+ * each entry point below replaces a jitted JAX function of the reference,
+ * cited beside it as path:line within that project.
+ */
+#ifndef OQMC_B200_H
+#define OQMC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OQ_OK 0
+#define OQ_ERR_ARG (-1)
+#define OQ_ERR_CUDA (-2)
+#define OQ_ERR_NAN (-3)
+#define OQ_ERR_SINGULAR (-4)
+#define OQ_ERR_TIMEOUT (-5)
+#define OQ_ERR_UNSUPPORTED (-6)
+#define OQ_ERR_NOMEM (-7)
+
+/* kernel flag bits reported by oqmc_get_flags */
+#define OQ_FLAG_NAN 1u
+#define OQ_FLAG_SINGULAR 2u
+
+/* precision of the sampler state and move arithmetic */
+#define OQ_PREC_FP64 0   /* everything FP64 */
+#define OQ_PREC_MIXED 1  /* FP32 AO/MO/inverse, FP64 refresh + accumulation */
+
+typedef struct oqmc_ctx oqmc_ctx;
+
+/*
+ * Molecular system.  Basis functions are grouped by exponent list: group g
+ * is one basis entry of one atom (OmegaQMC/psi/shell.py:150-256 read_shell,
+ * psi/gto.py:890-913 _parse_shells) with nprim[g] exponents shared by
+ * ncol[g] contracted shells (the columns of a general contraction).  Shells
+ * are numbered group by group, column by column; AOs follow in the order of
+ * _angular_cartesian (psi/gto.py:607-671), 2*am+1 per shell.
+ */
+typedef struct {
+  int natm;              /* nuclei */
+  int nbf;               /* spherical AOs */
+  int nocc;              /* occupied orbitals per spin (n_up == n_dn) */
+  int n_e;               /* electrons = 2 * nocc */
+  const double* nuc;     /* natm*3, bohr */
+  const double* Z;       /* natm nuclear charges */
+  int ngroup;
+  const int* group_atom;   /* ngroup */
+  const int* group_am;     /* ngroup */
+  const int* group_nprim;  /* ngroup */
+  const int* group_ncol;   /* ngroup, 1..4 */
+  const double* alpha;     /* sum(nprim) exponents, group-major */
+  const double* norm;      /* sum(nprim*ncol): for g, for column, for prim */
+  const int* shell_cusp;   /* sum(ncol) flags: cusp-corrected s shell */
+  const double* C;         /* nbf*nocc occupied MO coefficients, row-major */
+  int has_j1;
+  const double* j1;        /* natm*2 Pade (a, b) per atom */
+  int has_j2;
+  const double* j2;        /* 4: like a, like b, unlike a, unlike b */
+  int cusp;
+  const double* cusp_rc;   /* natm */
+  const double* cusp_q0;   /* natm */
+  const double* cusp_coeff;/* natm*8 */
+  double e_nn;             /* nuclear repulsion (eps-softened) */
+} oqmc_system_desc;
+
+/* Library version string. */
+const char* oqmc_version(void);
+
+/* Build a context on the current device.  Replaces _PsiGTO.__init__
+ * (OmegaQMC/psi/gto.py:820-844) / get_psi_fun (gto.py:2601-2621). */
+int oqmc_create(oqmc_ctx** out, const oqmc_system_desc* desc);
+int oqmc_destroy(oqmc_ctx* ctx);
+/* Text of the last error of ctx (or of the last failed oqmc_create when
+ * ctx is NULL). */
+const char* oqmc_last_error(const oqmc_ctx* ctx);
+
+/* Full FP64 evaluation of W walkers: log|psi| (W), grad log|psi| (W,n_e,3),
+ * per-electron Laplacian of log|psi| (W,n_e) and local-energy parts (W,4:
+ * ee, en, ke, total incl. e_nn).  grad/lap/eparts may be NULL.
+ * Replaces vmap(log_trial_wavefunction) (psi/gto.py:2220-2254) together
+ * with vmap(local_energy_ee/en/ke) (gto.py:2432-2451, 2506-2579) and
+ * _local_energy_batch (OmegaQMC/vmc_gto.py:801-812). */
+int oqmc_eval(oqmc_ctx* ctx, const double* walkers, int W, double* logpsi,
+              double* grad, double* lap, double* eparts, void* stream);
+
+/* log|psi| only (value path). Replaces _log_psi_batch
+ * (OmegaQMC/vmc_gto.py:790-797). */
+int oqmc_log_psi(oqmc_ctx* ctx, const double* walkers, int W, double* logpsi,
+                 void* stream);
+
+/* Bytes of sampler state for W walkers at a precision (inverse Slater
+ * matrices and log|det|). */
+size_t oqmc_state_bytes(const oqmc_ctx* ctx, int W, int precision);
+
+/* Full FP64 LU refresh of the sampler state from positions (the periodic
+ * recompute that bounds Sherman-Morrison drift). */
+int oqmc_refresh(oqmc_ctx* ctx, const double* walkers, int W, void* state,
+                 int precision, void* stream);
+
+/* n_sweeps single-electron Metropolis sweeps over all walkers (positions
+ * updated in place), measuring the local energy after every
+ * measure_every-th sweep.  sums: (n_sweeps/measure_every, 8) doubles that
+ * are ACCUMULATED into (zero them first): sum ee, en, ke, E_L, E_L^2,
+ * accepted moves, finite-E_L walkers.  el_trace: optional
+ * (n_meas, W) per-walker E_L.  eparts_last: optional (W,4) parts of the
+ * last measurement.  Random numbers: Philox4x32-10 keyed by seed, counter
+ * (walker, step_base + sweep, electron).  walkers_per_block: CTA size (32,
+ * 64 or 128; 0 = default).  Replaces the production scan body
+ * (OmegaQMC/vmc_gto.py:985-1034) and metropolis_move_1w (841-905). */
+int oqmc_sweeps(oqmc_ctx* ctx, double* walkers, int W, void* state,
+                int precision, int n_sweeps, int measure_every, double step,
+                uint64_t seed, uint64_t step_base, double* sums,
+                double* el_trace, double* eparts_last, int walkers_per_block,
+                void* stream);
+
+/* Exponent threshold above which an exponent group is evaluated in FP64
+ * near its nucleus in the mixed build (default 50.0; <= 0 disables). */
+int oqmc_set_split(oqmc_ctx* ctx, double tight_alpha);
+
+/* Synchronise `stream`, return the OR of kernel flag bits since the last
+ * clear in *flags and optionally clear them. */
+int oqmc_get_flags(oqmc_ctx* ctx, unsigned* flags, int clear, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OQMC_B200_H */

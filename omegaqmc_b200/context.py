@@ -1,0 +1,192 @@
+"""Device context: a :class:`~omegaqmc_b200.system.System` uploaded to one GPU.
+
+``GTOContext`` packs the system into the C ABI's ``oqmc_system_desc`` and
+wraps every entry point with torch CUDA tensors as the buffers.  torch only
+allocates device memory and provides streams; all arithmetic runs in the
+library's kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .system import System
+
+__all__ = ["GTOContext", "require_cuda"]
+
+
+def require_cuda():
+    if not torch.cuda.is_available():
+        raise RuntimeError(
+            "omegaqmc_b200 needs a CUDA device (sm_100a); there is no CPU path")
+
+
+def _dptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _stream_ptr(stream):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def pack_system(system: System):
+    """Arrays of the C descriptor (kept alive by the returned dict)."""
+    groups = system.prim_groups()
+    g_atom, g_am, g_np, g_nc, alpha, norm, cusp = [], [], [], [], [], [], []
+    order = []
+    for iat, a, shell_ids in groups:
+        shs = [system.shells[i] for i in shell_ids]
+        am = shs[0].am
+        if any(s.am != am for s in shs):
+            raise ValueError("mixed angular momenta in one basis entry")
+        g_atom.append(iat)
+        g_am.append(am)
+        g_np.append(len(a))
+        g_nc.append(len(shs))
+        alpha.extend(a.tolist())
+        for s in shs:
+            norm.extend(s.norm.tolist())
+            cusp.append(int(s.is_cusp))
+            order.append(s)
+    # the library numbers AOs group by group; check it matches the system
+    ao = 0
+    for s in order:
+        if s.isgs != ao:
+            raise ValueError("shell AO order does not follow exponent groups")
+        ao += s.nsgs
+    arr = {
+        "nuc": np.ascontiguousarray(system.nuc, dtype=np.float64).ravel(),
+        "Z": np.ascontiguousarray(system.Z, dtype=np.float64),
+        "group_atom": np.array(g_atom, dtype=np.int32),
+        "group_am": np.array(g_am, dtype=np.int32),
+        "group_nprim": np.array(g_np, dtype=np.int32),
+        "group_ncol": np.array(g_nc, dtype=np.int32),
+        "alpha": np.array(alpha, dtype=np.float64),
+        "norm": np.array(norm, dtype=np.float64),
+        "shell_cusp": np.array(cusp, dtype=np.int32),
+        "C": np.ascontiguousarray(system.C, dtype=np.float64).ravel(),
+        "j1": np.ascontiguousarray(system.j1, dtype=np.float64).ravel(),
+        "j2": np.ascontiguousarray(system.j2, dtype=np.float64).ravel(),
+        "cusp_rc": np.ascontiguousarray(system.cusp_rc, dtype=np.float64),
+        "cusp_q0": np.ascontiguousarray(system.cusp_q0, dtype=np.float64),
+        "cusp_coeff": np.ascontiguousarray(system.cusp_coeff, dtype=np.float64).ravel(),
+    }
+    d = L.SystemDesc()
+    d.natm = system.natm
+    d.nbf = system.nbf
+    d.nocc = system.nocc
+    d.n_e = system.n_e
+    d.ngroup = len(groups)
+    d.has_j1 = int(system.has_j1)
+    d.has_j2 = int(system.has_j2)
+    d.cusp = int(system.cusp)
+    d.e_nn = system.e_nn
+    for k, v in arr.items():
+        ct = ctypes.c_int if v.dtype == np.int32 else ctypes.c_double
+        setattr(d, k, v.ctypes.data_as(ctypes.POINTER(ct)))
+    return d, arr
+
+
+class GTOContext:
+    """One system on one CUDA device (the current one at construction)."""
+
+    def __init__(self, system: System, device=None):
+        require_cuda()
+        self.lib = L.load()
+        self.system = system
+        self.device = torch.device("cuda", torch.cuda.current_device()
+                                   if device is None else torch.device(device).index)
+        self.n_e = system.n_e
+        self.nocc = system.nocc
+        desc, self._keep = pack_system(system)
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            code = self.lib.oqmc_create(ctypes.byref(h), ctypes.byref(desc))
+        L.check(code, None)
+        self._h = h
+
+    # -- lifetime --------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self.lib.oqmc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, code):
+        L.check(code, self._h)
+
+    # -- helpers ----------------------------------------------------------
+    def walkers_tensor(self, X):
+        """(W, n_e, 3) float64 contiguous CUDA tensor on this device."""
+        t = torch.as_tensor(X, dtype=torch.float64)
+        if t.ndim == 2:
+            t = t.unsqueeze(0)
+        if t.ndim != 3 or t.shape[1] != self.n_e or t.shape[2] != 3:
+            raise ValueError(f"walkers must be (W, {self.n_e}, 3), got {tuple(t.shape)}")
+        return t.to(self.device).contiguous()
+
+    def flags(self, clear=True, stream=None):
+        f = ctypes.c_uint(0)
+        self._check(self.lib.oqmc_get_flags(self._h, ctypes.byref(f), int(clear),
+                                            _stream_ptr(stream)))
+        return f.value
+
+    # -- evaluation -----------------------------------------------------
+    def evaluate(self, X, want_grad=True, want_lap=True, stream=None):
+        """Full FP64 evaluation; returns a dict of CUDA tensors."""
+        X = self.walkers_tensor(X)
+        W = X.shape[0]
+        opt = dict(dtype=torch.float64, device=self.device)
+        logpsi = torch.empty(W, **opt)
+        grad = torch.empty(W, self.n_e, 3, **opt) if want_grad else None
+        lap = torch.empty(W, self.n_e, **opt) if want_lap else None
+        ep = torch.empty(W, 4, **opt)
+        self._check(self.lib.oqmc_eval(self._h, _dptr(X), W, _dptr(logpsi), _dptr(grad),
+                                       _dptr(lap), _dptr(ep), _stream_ptr(stream)))
+        out = {"logpsi": logpsi, "e_ee": ep[:, 0], "e_en": ep[:, 1], "e_ke": ep[:, 2],
+               "e_loc": ep[:, 3]}
+        if want_grad:
+            out["grad"] = grad
+        if want_lap:
+            out["lap"] = lap
+        return out
+
+    def log_psi(self, X, stream=None):
+        X = self.walkers_tensor(X)
+        out = torch.empty(X.shape[0], dtype=torch.float64, device=self.device)
+        self._check(self.lib.oqmc_log_psi(self._h, _dptr(X), X.shape[0], _dptr(out),
+                                          _stream_ptr(stream)))
+        return out
+
+    # -- sampler ------------------------------------------------------------
+    def state_bytes(self, W, precision):
+        return int(self.lib.oqmc_state_bytes(self._h, int(W), int(precision)))
+
+    def new_state(self, W, precision):
+        return torch.empty(self.state_bytes(W, precision), dtype=torch.uint8,
+                           device=self.device)
+
+    def refresh(self, X, state, precision, stream=None):
+        self._check(self.lib.oqmc_refresh(self._h, _dptr(X), X.shape[0], _dptr(state),
+                                          int(precision), _stream_ptr(stream)))
+
+    def sweeps(self, X, state, precision, n_sweeps, step, seed, step_base, sums,
+               measure_every=1, el_trace=None, eparts_last=None, walkers_per_block=0,
+               stream=None):
+        self._check(self.lib.oqmc_sweeps(
+            self._h, _dptr(X), X.shape[0], _dptr(state), int(precision), int(n_sweeps),
+            int(measure_every), float(step), ctypes.c_uint64(seed & (2**64 - 1)),
+            ctypes.c_uint64(step_base), _dptr(sums), _dptr(el_trace), _dptr(eparts_last),
+            int(walkers_per_block), _stream_ptr(stream)))
+
+    def set_split(self, tight_alpha):
+        self._check(self.lib.oqmc_set_split(self._h, float(tight_alpha)))

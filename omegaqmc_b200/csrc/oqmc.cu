@@ -1,0 +1,367 @@
+// liboqmc_b200: C ABI over the sm_100a kernels of the GTO-VMC hot path.
+// Host code: validation, the device system tables, launch configuration.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "oqmc_launch.h"
+#include "../../include/oqmc_b200.h"
+
+struct oqmc_ctx {
+  int device;
+  int nocc, n_e, nbf, natm;
+  OqSystem hsys;
+  OqSplit hsplit;
+  OqSystem* d_sys;
+  OqSplit* d_split;
+  double* d_C64;
+  float* d_C32;
+  unsigned* d_flags;
+  double tight_alpha;
+  char err[512];
+};
+
+static thread_local char g_create_err[512] = "";
+
+static int set_err(oqmc_ctx* ctx, int code, const char* fmt, const char* extra = "") {
+  char* dst = ctx ? ctx->err : g_create_err;
+  snprintf(dst, 512, fmt, extra);
+  return code;
+}
+
+#define OQ_CUDA(ctx, call)                                                    \
+  do {                                                                        \
+    cudaError_t _e = (call);                                                  \
+    if (_e != cudaSuccess) return set_err(ctx, OQ_ERR_CUDA, "CUDA error: %s", \
+                                          cudaGetErrorString(_e));            \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// f and g harmonics as monomial tables (am = 3, 4), the polynomials of
+// _angular_cartesian (OmegaQMC/psi/gto.py:607-671).
+// ---------------------------------------------------------------------------
+static void build_harm_table(OqHarmTable& t) {
+  memset(&t, 0, sizeof(t));
+  struct Term { double c; int i, j, k; };
+  const double cf1 = sqrt(2.5) * 0.5, cf2 = 3.0 * cf1, cf3 = sqrt(15.0),
+               cf4 = sqrt(1.5) * 0.5, cf5 = sqrt(6.0), cf6 = 1.5, cf7 = cf3 * 0.5;
+  const double cg1 = 2.9580398915498085, cg2 = 6.2749501990055672,
+               cg3 = 2.0916500663351894, cg4 = 1.1180339887498949,
+               cg5 = 6.7082039324993694, cg6 = 2.3717082451262845,
+               cg7 = 3.1622776601683795, cg8 = 0.55901699437494745,
+               cg9 = 3.3541019662496847, cg10 = 0.73950997288745213,
+               cg11 = 4.4370598373247132;
+  std::vector<std::vector<Term>> f = {
+      {{cf2, 2, 1, 0}, {-cf1, 0, 3, 0}},
+      {{cf3, 1, 1, 1}},
+      {{cf5, 0, 1, 2}, {-cf4, 2, 1, 0}, {-cf4, 0, 3, 0}},
+      {{1.0, 0, 0, 3}, {-cf6, 2, 0, 1}, {-cf6, 0, 2, 1}},
+      {{cf5, 1, 0, 2}, {-cf4, 3, 0, 0}, {-cf4, 1, 2, 0}},
+      {{cf7, 2, 0, 1}, {-cf7, 0, 2, 1}},
+      {{-cf2, 1, 2, 0}, {cf1, 3, 0, 0}}};
+  std::vector<std::vector<Term>> g = {
+      {{cg1, 3, 1, 0}, {-cg1, 1, 3, 0}},
+      {{cg2, 2, 1, 1}, {-cg3, 0, 3, 1}},
+      {{-cg4, 3, 1, 0}, {-cg4, 1, 3, 0}, {cg5, 1, 1, 2}},
+      {{-cg6, 2, 1, 1}, {-cg6, 0, 3, 1}, {cg7, 0, 1, 3}},
+      {{0.375, 4, 0, 0}, {0.375, 0, 4, 0}, {0.75, 2, 2, 0}, {1.0, 0, 0, 4},
+       {-3.0, 2, 0, 2}, {-3.0, 0, 2, 2}},
+      {{-cg6, 3, 0, 1}, {-cg6, 1, 2, 1}, {cg7, 1, 0, 3}},
+      {{-cg8, 4, 0, 0}, {cg8, 0, 4, 0}, {cg9, 2, 0, 2}, {-cg9, 0, 2, 2}},
+      {{-cg2, 1, 2, 1}, {cg3, 3, 0, 1}},
+      {{cg10, 4, 0, 0}, {cg10, 0, 4, 0}, {-cg11, 2, 2, 0}}};
+  int n = 0;
+  const std::vector<std::vector<Term>>* tabs[2] = {&f, &g};
+  for (int a = 0; a < 2; ++a) {
+    const auto& tab = *tabs[a];
+    for (size_t c = 0; c < tab.size(); ++c) {
+      t.first[a][c] = n;
+      for (const Term& x : tab[c]) {
+        t.coef[n] = x.c;
+        t.pow[n] = x.i | (x.j << 4) | (x.k << 8);
+        ++n;
+      }
+    }
+    t.first[a][tab.size()] = n;
+  }
+}
+
+static bool nocc_supported(int n) {
+  switch (n) {
+    case 1: case 2: case 3: case 4: case 5: case 6: case 7: case 8:
+    case 10: case 12: case 14: case 16: return true;
+    default: return false;
+  }
+}
+
+// Switch over the instantiated determinant sizes; EXPR uses N.
+#define OQ_CASE(N, EXPR) \
+  case N: {              \
+    EXPR(N);             \
+  } break;
+#define OQ_SWITCH(nocc, EXPR)                                                       \
+  switch (nocc) {                                                                   \
+    OQ_CASE(1, EXPR) OQ_CASE(2, EXPR) OQ_CASE(3, EXPR) OQ_CASE(4, EXPR)             \
+    OQ_CASE(5, EXPR) OQ_CASE(6, EXPR) OQ_CASE(7, EXPR) OQ_CASE(8, EXPR)             \
+    OQ_CASE(10, EXPR) OQ_CASE(12, EXPR) OQ_CASE(14, EXPR) OQ_CASE(16, EXPR)         \
+    default: err = cudaErrorInvalidValue;                                           \
+  }
+
+static OqLaunch make_launch(const oqmc_ctx* ctx, void* stream, size_t smem) {
+  OqLaunch L;
+  L.sys = ctx->d_sys; L.split = ctx->d_split; L.C64 = ctx->d_C64; L.C32 = ctx->d_C32;
+  L.flags = ctx->d_flags; L.stream = (cudaStream_t)stream; L.smem = smem;
+  return L;
+}
+
+static void compute_split(oqmc_ctx* ctx) {
+  OqSystem& S = ctx->hsys;
+  for (int g = 0; g < OQ_MAX_GROUP; ++g) ctx->hsplit.r2[g] = 0.0;
+  if (!(ctx->tight_alpha > 0.0)) return;
+  for (int g = 0; g < S.ngroup; ++g) {
+    double r2 = 0.0;
+    for (int p = 0; p < S.g_n[g]; ++p) {
+      const double a = S.alpha[S.g_off[g] + p];
+      if (a > ctx->tight_alpha) r2 = fmax(r2, 25.0 / a);
+    }
+    ctx->hsplit.r2[g] = r2;
+  }
+}
+
+extern "C" {
+
+const char* oqmc_version(void) { return "oqmc_b200 0.1.0 (sm_100a)"; }
+
+const char* oqmc_last_error(const oqmc_ctx* ctx) { return ctx ? ctx->err : g_create_err; }
+
+int oqmc_create(oqmc_ctx** out, const oqmc_system_desc* d) {
+  if (!out || !d) return set_err(nullptr, OQ_ERR_ARG, "null argument%s");
+  *out = nullptr;
+  if (d->natm < 1 || d->natm > OQ_MAX_NUC)
+    return set_err(nullptr, OQ_ERR_UNSUPPORTED, "natm out of range (1..16)%s");
+  if (d->n_e != 2 * d->nocc)
+    return set_err(nullptr, OQ_ERR_UNSUPPORTED, "only closed shells (n_e = 2 nocc)%s");
+  if (!nocc_supported(d->nocc))
+    return set_err(nullptr, OQ_ERR_UNSUPPORTED,
+                   "nocc must be one of 1-8, 10, 12, 14, 16%s");
+  if (d->nbf < d->nocc || d->nbf > OQ_MAX_BF)
+    return set_err(nullptr, OQ_ERR_UNSUPPORTED, "nbf out of range%s");
+  if (d->ngroup < 1 || d->ngroup > OQ_MAX_GROUP)
+    return set_err(nullptr, OQ_ERR_UNSUPPORTED, "too many exponent groups%s");
+  oqmc_ctx* ctx = new (std::nothrow) oqmc_ctx();
+  if (!ctx) return set_err(nullptr, OQ_ERR_NOMEM, "out of host memory%s");
+  memset(&ctx->hsys, 0, sizeof(OqSystem));
+  OqSystem& S = ctx->hsys;
+  S.natm = d->natm; S.nbf = d->nbf; S.nocc = d->nocc; S.n_e = d->n_e;
+  S.ngroup = d->ngroup; S.has_j1 = d->has_j1; S.has_j2 = d->has_j2; S.cusp = d->cusp;
+  S.e_nn = d->e_nn;
+  for (int i = 0; i < d->natm; ++i) {
+    for (int c = 0; c < 3; ++c) S.nuc[i][c] = d->nuc[3 * i + c];
+    S.Z[i] = d->Z[i];
+    if (d->has_j1) { S.j1a[i] = d->j1[2 * i]; S.j1b[i] = d->j1[2 * i + 1]; }
+    if (d->cusp) {
+      S.rc[i] = d->cusp_rc[i]; S.q0[i] = d->cusp_q0[i];
+      for (int k = 0; k < 8; ++k) S.cc[i][k] = d->cusp_coeff[8 * i + k];
+    }
+  }
+  if (d->has_j2) for (int k = 0; k < 4; ++k) S.j2[k] = d->j2[k];
+  int prim = 0, shell = 0, normo = 0, ao = 0;
+  for (int g = 0; g < d->ngroup; ++g) {
+    const int np = d->group_nprim[g], nc = d->group_ncol[g], am = d->group_am[g];
+    const int ia = d->group_atom[g];
+    if (np < 1 || nc < 1 || nc > OQ_MAX_COL || am < 0 || am > 4 || ia < 0 || ia >= d->natm ||
+        prim + np > OQ_MAX_PRIM || shell + nc > OQ_MAX_SHELL || normo + np * nc > OQ_MAX_NORM) {
+      delete ctx;
+      return set_err(nullptr, OQ_ERR_UNSUPPORTED, "basis group out of supported range%s");
+    }
+    S.g_iat[g] = ia; S.g_off[g] = prim; S.g_n[g] = np; S.g_shell0[g] = shell;
+    S.g_ncol[g] = nc; S.g_am[g] = am;
+    for (int p = 0; p < np; ++p) S.alpha[prim + p] = d->alpha[prim + p];
+    for (int k = 0; k < nc; ++k) {
+      S.s_ao[shell + k] = ao;
+      S.s_norm[shell + k] = normo;
+      S.s_cusp[shell + k] = (d->cusp && am == 0) ? d->shell_cusp[shell + k] : 0;
+      for (int p = 0; p < np; ++p) S.norm[normo + p] = d->norm[normo + p];
+      normo += np;
+      ao += 2 * am + 1;
+    }
+    prim += np;
+    shell += nc;
+  }
+  S.nshell = shell;
+  S.nprim_total = prim;
+  if (ao != d->nbf) {
+    delete ctx;
+    return set_err(nullptr, OQ_ERR_ARG, "group table does not add up to nbf AOs%s");
+  }
+  ctx->nocc = d->nocc; ctx->n_e = d->n_e; ctx->nbf = d->nbf; ctx->natm = d->natm;
+  ctx->tight_alpha = 50.0;
+  compute_split(ctx);
+  cudaGetDevice(&ctx->device);
+  build_harm_table(S.harm);
+  std::vector<float> c32((size_t)d->nbf * d->nocc);
+  for (size_t i = 0; i < c32.size(); ++i) c32[i] = (float)d->C[i];
+  cudaError_t e = cudaSuccess;
+  e = (e == cudaSuccess) ? cudaMalloc(&ctx->d_sys, sizeof(OqSystem)) : e;
+  e = (e == cudaSuccess) ? cudaMalloc(&ctx->d_split, sizeof(OqSplit)) : e;
+  e = (e == cudaSuccess) ? cudaMalloc(&ctx->d_C64, sizeof(double) * c32.size()) : e;
+  e = (e == cudaSuccess) ? cudaMalloc(&ctx->d_C32, sizeof(float) * c32.size()) : e;
+  e = (e == cudaSuccess) ? cudaMalloc(&ctx->d_flags, sizeof(unsigned)) : e;
+  e = (e == cudaSuccess) ? cudaMemcpy(ctx->d_sys, &S, sizeof(OqSystem), cudaMemcpyHostToDevice) : e;
+  e = (e == cudaSuccess) ? cudaMemcpy(ctx->d_split, &ctx->hsplit, sizeof(OqSplit), cudaMemcpyHostToDevice) : e;
+  e = (e == cudaSuccess) ? cudaMemcpy(ctx->d_C64, d->C, sizeof(double) * c32.size(), cudaMemcpyHostToDevice) : e;
+  e = (e == cudaSuccess) ? cudaMemcpy(ctx->d_C32, c32.data(), sizeof(float) * c32.size(), cudaMemcpyHostToDevice) : e;
+  e = (e == cudaSuccess) ? cudaMemset(ctx->d_flags, 0, sizeof(unsigned)) : e;
+  if (e != cudaSuccess) {
+    set_err(nullptr, OQ_ERR_CUDA, "CUDA error in create: %s", cudaGetErrorString(e));
+    oqmc_destroy(ctx);
+    return OQ_ERR_CUDA;
+  }
+  *out = ctx;
+  return OQ_OK;
+}
+
+int oqmc_destroy(oqmc_ctx* ctx) {
+  if (!ctx) return OQ_OK;
+  cudaFree(ctx->d_sys);
+  cudaFree(ctx->d_split);
+  cudaFree(ctx->d_C64);
+  cudaFree(ctx->d_C32);
+  cudaFree(ctx->d_flags);
+  delete ctx;
+  return OQ_OK;
+}
+
+int oqmc_set_split(oqmc_ctx* ctx, double tight_alpha) {
+  if (!ctx) return OQ_ERR_ARG;
+  ctx->tight_alpha = tight_alpha;
+  compute_split(ctx);
+  OQ_CUDA(ctx, cudaMemcpy(ctx->d_split, &ctx->hsplit, sizeof(OqSplit), cudaMemcpyHostToDevice));
+  return OQ_OK;
+}
+
+static size_t smem_sys_c64(const oqmc_ctx* ctx) {
+  return sizeof(OqSystem) + sizeof(double) * ctx->nbf * ctx->nocc;
+}
+
+int oqmc_eval(oqmc_ctx* ctx, const double* X, int W, double* logpsi, double* grad,
+              double* lap, double* eparts, void* stream) {
+  if (!ctx) return OQ_ERR_ARG;
+  if (W < 0 || (W > 0 && (!X || !logpsi))) return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
+  if (W == 0) return OQ_OK;
+  const OqLaunch L = make_launch(ctx, stream, smem_sys_c64(ctx));
+  cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_eval_##N(L, X, W, logpsi, grad, lap, eparts)
+  OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+  OQ_CUDA(ctx, err);
+  return OQ_OK;
+}
+
+int oqmc_log_psi(oqmc_ctx* ctx, const double* X, int W, double* logpsi, void* stream) {
+  if (!ctx) return OQ_ERR_ARG;
+  if (W < 0 || (W > 0 && (!X || !logpsi))) return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
+  if (W == 0) return OQ_OK;
+  const OqLaunch L = make_launch(ctx, stream, smem_sys_c64(ctx));
+  cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_logpsi_##N(L, X, W, logpsi)
+  OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+  OQ_CUDA(ctx, err);
+  return OQ_OK;
+}
+
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+size_t oqmc_state_bytes(const oqmc_ctx* ctx, int W, int precision) {
+  if (!ctx || W < 0) return 0;
+  const size_t rs = precision == OQ_PREC_MIXED ? sizeof(float) : sizeof(double);
+  return align256((size_t)2 * ctx->nocc * ctx->nocc * W * rs) + align256((size_t)W * sizeof(double));
+}
+
+static void state_ptrs(const oqmc_ctx* ctx, void* state, int W, int precision, void** ainv,
+                       double** logdet) {
+  const size_t rs = precision == OQ_PREC_MIXED ? sizeof(float) : sizeof(double);
+  *ainv = state;
+  *logdet = reinterpret_cast<double*>(static_cast<char*>(state) +
+                                      align256((size_t)2 * ctx->nocc * ctx->nocc * W * rs));
+}
+
+int oqmc_refresh(oqmc_ctx* ctx, const double* X, int W, void* state, int precision,
+                 void* stream) {
+  if (!ctx) return OQ_ERR_ARG;
+  if (W < 0 || (W > 0 && (!X || !state)) || (precision != OQ_PREC_FP64 && precision != OQ_PREC_MIXED))
+    return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
+  if (W == 0) return OQ_OK;
+  void* ainv;
+  double* logdet;
+  state_ptrs(ctx, state, W, precision, &ainv, &logdet);
+  const OqLaunch L = make_launch(ctx, stream, smem_sys_c64(ctx));
+  const int mixed = precision == OQ_PREC_MIXED;
+  cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_refresh_##N(L, X, W, ainv, logdet, mixed)
+  OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+  OQ_CUDA(ctx, err);
+  return OQ_OK;
+}
+
+static size_t sweep_smem(const oqmc_ctx* ctx, int wpb, int precision) {
+  const size_t rs = precision == OQ_PREC_MIXED ? sizeof(float) : sizeof(double);
+  size_t b = sizeof(OqSystem) + sizeof(OqSplit);
+  b += ((size_t)ctx->nbf * ctx->nocc * rs + 15) & ~(size_t)15;
+  b += (size_t)3 * ctx->n_e * wpb * sizeof(double);
+  b += (size_t)2 * ctx->nocc * ctx->nocc * wpb * rs;
+  return b;
+}
+
+int oqmc_sweeps(oqmc_ctx* ctx, double* X, int W, void* state, int precision, int n_sweeps,
+                int measure_every, double step, uint64_t seed, uint64_t step_base,
+                double* sums, double* el_trace, double* eparts_last, int wpb,
+                void* stream) {
+  if (!ctx) return OQ_ERR_ARG;
+  if (W < 0 || n_sweeps < 0 || measure_every < 1 || !(step > 0.0) ||
+      (precision != OQ_PREC_FP64 && precision != OQ_PREC_MIXED))
+    return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
+  if (W == 0 || n_sweeps == 0) return OQ_OK;
+  if (!X || !state || (n_sweeps >= measure_every && !sums))
+    return set_err(ctx, OQ_ERR_ARG, "null buffer%s");
+  if (wpb == 0) wpb = 128;
+  if (wpb != 32 && wpb != 64 && wpb != 128)
+    return set_err(ctx, OQ_ERR_ARG, "walkers_per_block must be 32, 64 or 128%s");
+  size_t sm = sweep_smem(ctx, wpb, precision);
+  while (sm > 227 * 1024 && wpb > 32) { wpb /= 2; sm = sweep_smem(ctx, wpb, precision); }
+  if (sm > 227 * 1024)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED, "system too large for the shared-memory sweep kernel%s");
+  OqSweepArgs a;
+  memset(&a, 0, sizeof(a));
+  double* logdet;
+  state_ptrs(ctx, state, W, precision, &a.ainv, &logdet);
+  a.X = X; a.logdet = logdet; a.W = W; a.n_sweeps = n_sweeps; a.measure_every = measure_every;
+  a.step = step; a.seed = seed; a.step_base = step_base; a.sums = sums;
+  a.el_trace = el_trace; a.eparts_last = eparts_last; a.flags = ctx->d_flags;
+  const OqLaunch L = make_launch(ctx, stream, sm);
+  const int mixed = precision == OQ_PREC_MIXED;
+  cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_sweeps_##N(L, a, wpb, mixed)
+  OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+  OQ_CUDA(ctx, err);
+  return OQ_OK;
+}
+
+int oqmc_get_flags(oqmc_ctx* ctx, unsigned* flags, int clear, void* stream) {
+  if (!ctx || !flags) return OQ_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned h = 0;
+  OQ_CUDA(ctx, cudaMemcpyAsync(&h, ctx->d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  OQ_CUDA(ctx, cudaStreamSynchronize(s));
+  if (clear) OQ_CUDA(ctx, cudaMemsetAsync(ctx->d_flags, 0, sizeof(unsigned), s));
+  *flags = h;
+  return OQ_OK;
+}
+
+}  // extern "C"

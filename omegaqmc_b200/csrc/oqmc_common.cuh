@@ -1,0 +1,247 @@
+// Shared device-side pieces of the GTO Slater-Jastrow kernels (sm_100a).
+//
+// The system tables (nuclei, exponent groups, contracted shells, Jastrow and
+// cusp constants) live in one POD struct that every CTA copies into shared
+// memory once; all threads then read them as broadcasts.  Walker data is
+// laid out walker-minor ("structure of arrays") wherever consecutive threads
+// handle consecutive walkers, so global accesses coalesce.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define OQ_MAX_NUC 16
+#define OQ_MAX_GROUP 96
+#define OQ_MAX_SHELL 128
+#define OQ_MAX_PRIM 256
+#define OQ_MAX_NORM 512
+#define OQ_MAX_BF 160
+#define OQ_MAX_OCC 16
+#define OQ_MAX_E 32
+#define OQ_MAX_COL 4          // contraction columns sharing one exponent list
+#define OQ_MAX_TERMS 96       // monomial terms of the f and g harmonics
+
+// Harmonic monomial tables for am = 3, 4 (am <= 2 are hand-written).
+// term t of component c of am: coef * x^i y^j z^k, packed i | j<<4 | k<<8.
+struct OqHarmTable {
+  double coef[OQ_MAX_TERMS];
+  int pow[OQ_MAX_TERMS];
+  int first[2][10];        // [am-3][c] first term, [c+1] end
+};
+
+// Exponent group = one basis entry of one atom: nprim exponents shared by
+// ncol contracted shells (the columns of a general contraction).
+struct OqSystem {
+  int natm, nbf, nocc, n_e;
+  int ngroup, nshell, has_j1, has_j2;
+  int cusp, nprim_total, pad0, pad1;
+  double e_nn;
+  double nuc[OQ_MAX_NUC][3];
+  double Z[OQ_MAX_NUC];
+  double j1a[OQ_MAX_NUC], j1b[OQ_MAX_NUC];
+  double j2[4];                    // like a, like b, unlike a, unlike b
+  double rc[OQ_MAX_NUC], q0[OQ_MAX_NUC], cc[OQ_MAX_NUC][8];
+  int g_iat[OQ_MAX_GROUP], g_off[OQ_MAX_GROUP], g_n[OQ_MAX_GROUP];
+  int g_shell0[OQ_MAX_GROUP], g_ncol[OQ_MAX_GROUP], g_am[OQ_MAX_GROUP];
+  int s_ao[OQ_MAX_SHELL], s_norm[OQ_MAX_SHELL], s_cusp[OQ_MAX_SHELL];
+  int pad2;
+  double alpha[OQ_MAX_PRIM];
+  double norm[OQ_MAX_NORM];
+  OqHarmTable harm;
+};
+
+// Status codes shared by host and device.
+enum OqStatus {
+  OQ_OK = 0,
+  OQ_ERR_ARG = -1,
+  OQ_ERR_CUDA = -2,
+  OQ_ERR_NAN = -3,
+  OQ_ERR_SINGULAR = -4,
+  OQ_ERR_TIMEOUT = -5,
+  OQ_ERR_UNSUPPORTED = -6,
+  OQ_ERR_NOMEM = -7,
+};
+
+// Device flag bits written by kernels (OR-ed into a per-launch word).
+#define OQ_FLAG_NAN 1u
+#define OQ_FLAG_SINGULAR 2u
+
+
+// ---------------------------------------------------------------------------
+// Copy the system struct into shared memory (all threads cooperate).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void oq_load_system(OqSystem* dst, const OqSystem* src) {
+  const int n = sizeof(OqSystem) / 16;
+  const int4* s = reinterpret_cast<const int4*>(src);
+  int4* d = reinterpret_cast<int4*>(dst);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) d[i] = s[i];
+}
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw,
+// "Parallel random numbers: as easy as 1, 2, 3", SC'11).
+// ---------------------------------------------------------------------------
+struct OqU4 { uint32_t x, y, z, w; };
+
+__device__ __forceinline__ OqU4 oq_philox(OqU4 c, uint32_t k0, uint32_t k1) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+    uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+    OqU4 n;
+    n.x = hi1 ^ c.y ^ k0;
+    n.y = lo1;
+    n.z = hi0 ^ c.w ^ k1;
+    n.w = lo0;
+    c = n;
+    k0 += W0;
+    k1 += W1;
+  }
+  return c;
+}
+
+// uniform in (0, 1] from 32 random bits
+__device__ __forceinline__ double oq_u01(uint32_t v) {
+  return ((double)v + 1.0) * 2.3283064365386963e-10;
+}
+
+// Three standard normals and one uniform for a single-electron proposal.
+// Counter = (walker, step, electron, stream); key = seed.
+__device__ __forceinline__ void oq_move_randoms(uint64_t seed, uint32_t walker,
+                                                uint32_t step, uint32_t elec,
+                                                double n3[3], double& u) {
+  OqU4 c0 = {walker, step, elec, 0u};
+  OqU4 r0 = oq_philox(c0, (uint32_t)seed, (uint32_t)(seed >> 32));
+  OqU4 c1 = {walker, step, elec, 1u};
+  OqU4 r1 = oq_philox(c1, (uint32_t)seed, (uint32_t)(seed >> 32));
+  double a = sqrt(-2.0 * log(oq_u01(r0.x)));
+  double s, c;
+  sincospi(2.0 * oq_u01(r0.y), &s, &c);
+  double b = sqrt(-2.0 * log(oq_u01(r0.z)));
+  double s2, c2;
+  sincospi(2.0 * oq_u01(r0.w), &s2, &c2);
+  n3[0] = a * c;
+  n3[1] = a * s;
+  n3[2] = b * c2;
+  u = oq_u01(r1.x) - 2.3283064365386963e-10;   // in [0, 1)
+}
+
+// ---------------------------------------------------------------------------
+// Real solid harmonics (value and gradient), order of _angular_cartesian.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void oq_harm_d(T x, T y, T z, T Y[5], T dY[5][3]) {
+  const T cd1 = (T)1.7320508075688772;
+  const T cd2 = (T)0.8660254037844386;
+  Y[0] = cd1 * x * y;
+  Y[1] = cd1 * y * z;
+  Y[2] = (T)0.5 * ((T)2 * z * z - x * x - y * y);
+  Y[3] = cd1 * x * z;
+  Y[4] = cd2 * (x * x - y * y);
+  dY[0][0] = cd1 * y; dY[0][1] = cd1 * x; dY[0][2] = (T)0;
+  dY[1][0] = (T)0;    dY[1][1] = cd1 * z; dY[1][2] = cd1 * y;
+  dY[2][0] = -x;      dY[2][1] = -y;      dY[2][2] = (T)2 * z;
+  dY[3][0] = cd1 * z; dY[3][1] = (T)0;    dY[3][2] = cd1 * x;
+  dY[4][0] = cd1 * x; dY[4][1] = -cd1 * y; dY[4][2] = (T)0;
+}
+
+template <typename T>
+__device__ __forceinline__ T oq_ipow(T v, int n) {
+  T r = (T)1;
+  for (int i = 0; i < n; ++i) r *= v;
+  return r;
+}
+
+// component c of am (3 or 4) from the monomial table
+template <typename T>
+__device__ __forceinline__ void oq_harm_table(const OqHarmTable& H, int am, int c, T x,
+                                              T y, T z, T& Y, T dY[3]) {
+  Y = (T)0; dY[0] = dY[1] = dY[2] = (T)0;
+  const int t0 = H.first[am - 3][c], t1 = H.first[am - 3][c + 1];
+  for (int t = t0; t < t1; ++t) {
+    const T cf = (T)H.coef[t];
+    const int p = H.pow[t];
+    const int i = p & 15, j = (p >> 4) & 15, k = (p >> 8) & 15;
+    const T xi = oq_ipow(x, i), yj = oq_ipow(y, j), zk = oq_ipow(z, k);
+    Y += cf * xi * yj * zk;
+    if (i) dY[0] += cf * (T)i * oq_ipow(x, i - 1) * yj * zk;
+    if (j) dY[1] += cf * (T)j * xi * oq_ipow(y, j - 1) * zk;
+    if (k) dY[2] += cf * (T)k * xi * yj * oq_ipow(z, k - 1);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Cusp-corrected s orbital (value only and VGL), FP64.
+// f = c0 (1-b) R + b q0 e^{-Zr} (c1 + sum_{k=2..7} c_k s^k), s = r/rc,
+// b = 1 - 10 s^3 + 15 s^4 - 6 s^5 inside rc, 0 outside.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double oq_cusp_val(const OqSystem& S, int ia, double r,
+                                              double R) {
+  const double rc = S.rc[ia];
+  const double* c = S.cc[ia];
+  if (!(r < rc)) return c[0] * R;
+  const double s = r / rc;
+  const double s2 = s * s, s3 = s2 * s;
+  const double b = 1.0 - 10.0 * s3 + 15.0 * s3 * s - 6.0 * s3 * s2;
+  const double sl = S.q0[ia] * exp(-S.Z[ia] * r);
+  double poly = c[7];
+  for (int k = 6; k >= 2; --k) poly = poly * s + c[k];
+  poly = poly * s2 + c[1];
+  return c[0] * (1.0 - b) * R + b * sl * poly;
+}
+
+// (f, f'/r, f'' + 2 f'/r) given (R, R'/r, R'' + 2R'/r) of the plain s shell.
+__device__ __forceinline__ void oq_cusp_vgl(const OqSystem& S, int ia, double r,
+                                            double& R, double& Rp, double& Rl) {
+  const double rc = S.rc[ia];
+  const double* c = S.cc[ia];
+  const double c0 = c[0];
+  if (!(r < rc)) {
+    R *= c0; Rp *= c0; Rl *= c0;
+    return;
+  }
+  const double Z = S.Z[ia];
+  const double s = r / rc, oms = 1.0 - s;
+  const double s2 = s * s, s3 = s2 * s;
+  const double b = 1.0 - 10.0 * s3 + 15.0 * s3 * s - 6.0 * s3 * s2;
+  const double bp = -(30.0 / rc) * s2 * oms * oms;
+  const double bp_r = -(30.0 / (rc * rc * rc)) * r * oms * oms;
+  const double bpp = -(60.0 / (rc * rc)) * s * oms * (1.0 - 2.0 * s);
+  const double BL = bpp + 2.0 * bp_r;
+  const double Av = c0 * (1.0 - b) * R;
+  const double Ag = c0 * (-bp_r * R + (1.0 - b) * Rp);
+  const double Al = c0 * (-BL * R + (1.0 - b) * Rl - 2.0 * r * bp * Rp);
+  const double Sl = S.q0[ia] * exp(-Z * r);
+  // P = c1 + sum c_k s^k, P' and P'' in r
+  double P = c[7], P1 = 7.0 * c[7], P2 = 42.0 * c[7];
+  for (int k = 6; k >= 2; --k) {
+    P = P * s + c[k];
+    P1 = P1 * s + k * c[k];
+    P2 = P2 * s + k * (k - 1) * c[k];
+  }
+  P = P * s2 + c[1];
+  P1 = P1 * s / rc;
+  P2 = P2 / (rc * rc);
+  const double Q = b * Sl * P;
+  const double Qp = bp * Sl * P - Z * b * Sl * P + b * Sl * P1;
+  const double Qpp = bpp * Sl * P + Z * Z * b * Sl * P + b * Sl * P2 +
+                     2.0 * (-Z * bp * Sl * P + bp * Sl * P1 - Z * b * Sl * P1);
+  const double Qg = Qp / r;
+  R = Av + Q;
+  Rp = Ag + Qg;
+  Rl = Al + Qpp + 2.0 * Qg;
+}
+
+// Padé u(r) = a r / (1 + b r) and (u'/r, u'' + 2u'/r)
+template <typename T>
+__device__ __forceinline__ T oq_pade(T a, T b, T r) { return a * r / ((T)1 + b * r); }
+
+template <typename T>
+__device__ __forceinline__ void oq_pade_vgl(T a, T b, T r, T& up_r, T& lap) {
+  const T den = (T)1 + b * r;
+  const T up = a / (den * den);
+  const T upp = (T)-2 * a * b / (den * den * den);
+  up_r = up / r;
+  lap = upp + (T)2 * up / r;
+}

@@ -1,0 +1,28 @@
+// Host-side launchers, one set per determinant size NOCC.  Each set lives in
+// its own translation unit (oqmc_inst.cu compiled with -DOQ_N=<NOCC>) so the
+// template instantiations build in parallel.
+#pragma once
+#include <cuda_runtime.h>
+#include "oqmc_sweep.cuh"
+
+struct OqLaunch {
+  const OqSystem* sys;
+  const OqSplit* split;
+  const double* C64;
+  const float* C32;
+  unsigned* flags;
+  cudaStream_t stream;
+  size_t smem;
+};
+
+#define OQ_DECL_LAUNCHERS(N)                                                          \
+  cudaError_t oq_eval_##N(const OqLaunch& L, const double* X, int W, double* logpsi,  \
+                          double* grad, double* lap, double* eparts);                 \
+  cudaError_t oq_logpsi_##N(const OqLaunch& L, const double* X, int W, double* logpsi); \
+  cudaError_t oq_refresh_##N(const OqLaunch& L, const double* X, int W, void* ainv,   \
+                             double* logdet, int mixed);                              \
+  cudaError_t oq_sweeps_##N(const OqLaunch& L, const OqSweepArgs& a, int wpb, int mixed);
+
+#define OQ_NOCC_LIST(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(10) X(12) X(14) X(16)
+
+OQ_NOCC_LIST(OQ_DECL_LAUNCHERS)

@@ -1,0 +1,434 @@
+"""Molecular system description for the GTO Slater–Jastrow wavefunction.
+
+This module turns a PySCF-style mean-field object (or the light-weight
+:class:`Mole` / :class:`MeanField` stand-ins defined here) into the flat
+tables the CUDA kernels read: nuclei, contracted shells with normalised
+primitive coefficients, occupied MO coefficients, Padé Jastrow parameters
+and cusp-correction constants.
+
+Conventions follow the reference trial wavefunction:
+
+* Shell normalisation restates ``read_shell`` (``OmegaQMC/psi/shell.py:150-256``):
+  s and p contractions are renormalised over the contraction, d/f/g shells
+  carry primitive normalisation only.  A general contraction (several
+  coefficient columns sharing one exponent list) becomes one shell per column.
+* The cusp-corrected shell of each atom is the first coefficient column of
+  the atom's first basis entry (``OmegaQMC/psi/gto.py:890-913``), with
+  ``rc = 0.1`` for hydrogen and ``0.2`` otherwise (``gto.py:873-876``).
+* Spherical AO order within a shell is that of ``_angular_cartesian``
+  (``gto.py:607-671``); AOs are numbered atom by atom, entry by entry,
+  column by column.
+* Electrons alternate spin: up at even, down at odd positions
+  (``OmegaQMC/spin_layout.py:56-80``); only closed shells (n_up == n_down)
+  are supported, as in the reference's single-determinant path
+  (``gto.py:846-888`` takes one ``mo_coeff[:, :nocc]`` for both spins).
+* Padé J1 without cusp correction fixes ``a = -Z`` (``gto.py:1526-1560``).
+"""
+from __future__ import annotations
+
+import math
+import warnings
+from dataclasses import dataclass, field
+
+import numpy as np
+
+__all__ = [
+    "Mole", "MeanField", "Shell", "System", "read_shell", "build_system",
+    "ELEMENT_Z", "parse_params_corr",
+]
+
+ELEMENT_Z = {
+    "H": 1, "He": 2, "Li": 3, "Be": 4, "B": 5, "C": 6, "N": 7, "O": 8,
+    "F": 9, "Ne": 10, "Na": 11, "Mg": 12, "Al": 13, "Si": 14, "P": 15,
+    "S": 16, "Cl": 17, "Ar": 18,
+}
+ANG_TO_BOHR = 1.0 / 0.52917721092
+PI32 = math.pi ** 1.5
+
+
+# --------------------------------------------------------------------------
+# Duck-typed PySCF objects
+# --------------------------------------------------------------------------
+class Mole:
+    """Minimal stand-in for ``pyscf.gto.Mole`` as read by the GTO path.
+
+    Only the attributes the reference's trial wavefunction touches are
+    provided: ``_atom``, ``_basis``, ``atom_coords``, ``atom_charges``,
+    ``atom_symbol``, ``natm``, ``tot_electrons``, ``nelec``, ``basis``,
+    ``charge``, ``spin``, ``elements`` and ``groupname``.
+
+    Args:
+        atoms: ``[(symbol, (x, y, z)), ...]`` or a PySCF-style string
+            ``"O 0 0 0; H 0 0 1.8"``.
+        basis: ``{symbol: [[am, [alpha, c1, c2, ...], ...], ...]}`` in
+            PySCF's internal (``mol._basis``) format.
+        unit: ``"Bohr"`` (default) or ``"Angstrom"``.
+        basis_name: label stored in ``mol.basis``.
+    """
+
+    def __init__(self, atoms, basis, unit="Bohr", charge=0, spin=0,
+                 basis_name="gen"):
+        if isinstance(atoms, str):
+            atoms = _parse_atom_string(atoms)
+        u = unit.lower()
+        if u in ("bohr", "au", "a.u."):
+            fac = 1.0
+        elif u in ("angstrom", "ang", "a"):
+            fac = ANG_TO_BOHR
+        else:
+            raise ValueError(f"unknown unit {unit!r}")
+        self._atom = [(str(s), tuple(float(c) * fac for c in xyz))
+                      for s, xyz in atoms]
+        for s, _ in self._atom:
+            if s not in ELEMENT_Z:
+                raise ValueError(f"unknown element {s!r}")
+            if s not in basis:
+                raise ValueError(f"no basis given for element {s!r}")
+        self._basis = {s: basis[s] for s, _ in self._atom}
+        self.basis = basis_name
+        self.charge = int(charge)
+        self.spin = int(spin)
+        self.unit = "Bohr"
+        self.groupname = "C1"
+
+    @property
+    def natm(self):
+        return len(self._atom)
+
+    @property
+    def elements(self):
+        return [s for s, _ in self._atom]
+
+    def atom_symbol(self, i):
+        return self._atom[i][0]
+
+    def atom_coords(self, unit="Bohr"):
+        c = np.array([xyz for _, xyz in self._atom], dtype=np.float64)
+        if unit.lower() in ("angstrom", "ang"):
+            c = c / ANG_TO_BOHR
+        return c
+
+    def atom_charges(self):
+        return np.array([ELEMENT_Z[s] for s, _ in self._atom], dtype=np.int64)
+
+    def tot_electrons(self):
+        return int(self.atom_charges().sum()) - self.charge
+
+    @property
+    def nelec(self):
+        n = self.tot_electrons()
+        nb = (n - self.spin) // 2
+        return (n - nb, nb)
+
+    @property
+    def nao(self):
+        return sum(s.nsgs for s in build_shells(self))
+
+
+class MeanField:
+    """Minimal stand-in for a converged ``pyscf.scf.RHF`` object.
+
+    ``mo_coeff`` is ``(nao, nmo)`` over the spherical AOs in the order of
+    :func:`build_shells`; ``mo_occ`` marks occupied columns with 2.
+    """
+
+    def __init__(self, mol, mo_coeff, mo_occ=None):
+        self.mol = mol
+        self.mo_coeff = np.asarray(mo_coeff, dtype=np.float64)
+        if mo_occ is None:
+            nocc = mol.tot_electrons() // 2
+            mo_occ = np.zeros(self.mo_coeff.shape[1])
+            mo_occ[:nocc] = 2.0
+        self.mo_occ = np.asarray(mo_occ, dtype=np.float64)
+
+
+def _parse_atom_string(s):
+    out = []
+    for line in s.replace(";", "\n").splitlines():
+        line = line.strip()
+        if not line:
+            continue
+        parts = line.split()
+        out.append((parts[0], tuple(float(p) for p in parts[1:4])))
+    return out
+
+
+# --------------------------------------------------------------------------
+# Shells
+# --------------------------------------------------------------------------
+@dataclass
+class Shell:
+    """One contracted shell (one coefficient column of a basis entry).
+
+    Mirrors ``ShellType`` (``OmegaQMC/psi/shell.py:8-31``)."""
+    am: int
+    iat: int
+    isgs: int
+    nsgs: int
+    alpha: np.ndarray
+    norm: np.ndarray
+    is_cusp: bool = False
+    entry: int = 0          # index of the basis entry on its atom
+    column: int = 0         # contraction column within the entry
+
+    @property
+    def nprim(self):
+        return len(self.alpha)
+
+
+_NSGS = {0: 1, 1: 3, 2: 5, 3: 7, 4: 9}
+
+
+def read_shell(entry, iat, isgs):
+    """Normalised shells of one PySCF basis entry ``[am, [a, c...], ...]``.
+
+    Restates ``read_shell`` (``OmegaQMC/psi/shell.py:150-256``): primitive
+    factor ``(2a/pi)^(3/4)`` times ``sqrt(4a)`` (p), ``4a/sqrt(3)`` (d),
+    ``(4a)^(3/2)/sqrt(15)`` (f), ``(4a)^2/sqrt(105)`` (g); s and p shells are
+    then renormalised over the contraction (``shell.py:180-218``).
+    """
+    am = int(entry[0])
+    rows = entry[1:]
+    if rows and not isinstance(rows[0], (list, tuple, np.ndarray)):
+        # PySCF may carry a kappa scalar after am; it does not change
+        # the non-relativistic shell.
+        rows = rows[1:]
+    prim = np.array(rows, dtype=np.float64)
+    if prim.ndim != 2 or prim.shape[1] < 2:
+        raise ValueError(f"bad basis entry {entry!r}")
+    if am not in _NSGS:
+        raise NotImplementedError(f"Angular momentum {am} not yet implemented")
+    alphas = prim[:, 0]
+    out = []
+    cnorm0 = np.exp(0.75 * np.log(2.0 * alphas / np.pi))
+    iu, ju = np.triu_indices(len(alphas), k=0)
+    diag = iu == ju
+    for ic in range(1, prim.shape[1]):
+        c = prim[:, ic]
+        if am == 0:
+            norm = c * cnorm0
+            asum = alphas[iu] + alphas[ju]
+            terms = norm[iu] * norm[ju] / (asum * np.sqrt(asum))
+            terms = np.where(diag, terms, 2.0 * terms)
+            norm = norm * (1.0 / np.sqrt(np.sum(terms) * PI32))
+        elif am == 1:
+            norm = c * cnorm0 * np.sqrt(4.0 * alphas)
+            asum = alphas[iu] + alphas[ju]
+            terms = 0.5 * norm[iu] * norm[ju] / (asum * asum * np.sqrt(asum))
+            terms = np.where(diag, terms, 2.0 * terms)
+            norm = norm * (1.0 / np.sqrt(np.sum(terms) * PI32))
+        elif am == 2:
+            norm = c * cnorm0 * (4.0 * alphas) / np.sqrt(3.0)
+        elif am == 3:
+            norm = c * cnorm0 * (4.0 * alphas) ** 1.5 / np.sqrt(15.0)
+        else:
+            norm = c * cnorm0 * (4.0 * alphas) ** 2 / np.sqrt(105.0)
+        out.append(Shell(am=am, iat=iat, isgs=isgs, nsgs=_NSGS[am],
+                         alpha=alphas.copy(), norm=np.asarray(norm),
+                         column=ic - 1))
+        isgs += _NSGS[am]
+    return out
+
+
+def build_shells(mol, cusp=False):
+    """All shells of ``mol`` in AO order (``gto.py:890-913``)."""
+    shells = []
+    isgs = 0
+    for ia, (sym, _) in enumerate(mol._atom):
+        for ish, entry in enumerate(mol._basis[sym]):
+            for jsh, sh in enumerate(read_shell(entry, ia, isgs)):
+                sh.entry = ish
+                sh.is_cusp = bool(cusp and ish == 0 and jsh == 0)
+                isgs = sh.isgs + sh.nsgs
+                shells.append(sh)
+    return shells
+
+
+# --------------------------------------------------------------------------
+# Jastrow parameters
+# --------------------------------------------------------------------------
+def parse_params_corr(params_corr, mol, cusp):
+    """Per-atom Padé J1 ``(a, b)`` and J2 like/unlike ``(a, b)``.
+
+    Returns ``(has_j1, j1_ab (natm, 2), has_j2, j2 (2, 2))`` where ``j2[0]``
+    is the like-spin pair and ``j2[1]`` the unlike-spin pair.  Restates
+    ``J1_ab`` (``gto.py:1526-1560``): with cusp-corrected orbitals each
+    element carries ``[a, b]``; without them ``a = -Z`` and the entry is
+    ``b`` (an ``[a, b]`` entry warns and its ``a`` is ignored; any other
+    length raises ``ValueError``).  Keys other than ``J1_pade`` and
+    ``J2_pade`` raise ``NotImplementedError`` (B-spline and three-body
+    Jastrows are not part of this path).
+    """
+    params_corr = {} if params_corr is None else dict(params_corr)
+    extra = [k for k in params_corr if k not in ("J1_pade", "J2_pade")]
+    if extra:
+        raise NotImplementedError(
+            f"Jastrow terms {extra} are not supported; only J1_pade and "
+            "J2_pade are implemented on this path")
+    natm = mol.natm
+    Z = mol.atom_charges().astype(np.float64)
+    j1 = np.zeros((natm, 2))
+    has_j1 = "J1_pade" in params_corr and len(params_corr["J1_pade"]) > 0
+    if has_j1:
+        p1 = params_corr["J1_pade"]
+        for ia in range(natm):
+            sym = mol.atom_symbol(ia)
+            if sym not in p1:
+                raise KeyError(f"J1_pade has no entry for element {sym!r}")
+            p = np.ravel(np.asarray(p1[sym], dtype=np.float64))
+            if cusp:
+                if p.shape[0] != 2:
+                    raise ValueError(
+                        f"J1_pade['{sym}'] must be [a, b] with cusp-"
+                        "corrected orbitals")
+                j1[ia] = p
+            else:
+                if p.shape[0] not in (1, 2):
+                    raise ValueError(
+                        f"J1_pade['{sym}'] has {p.shape[0]} entries; "
+                        "expected b or [a, b].")
+                if p.shape[0] == 2:
+                    warnings.warn(
+                        f"J1_pade['{sym}'] = [a, b] without cusp correction:"
+                        " a is fixed at -Z and the given a is ignored.  "
+                        "Pass b alone.", stacklevel=3)
+                j1[ia] = (-Z[ia], p[-1])
+    j2 = np.zeros((2, 2))
+    has_j2 = "J2_pade" in params_corr
+    if has_j2:
+        p2 = params_corr["J2_pade"]
+        if not isinstance(p2, dict):
+            raise TypeError("J2_pade must be a dict with 'like' and 'unlike'")
+        for k, key in enumerate(("like", "unlike")):
+            v = np.ravel(np.asarray(p2[key], dtype=np.float64))
+            if v.shape[0] < 2:
+                raise ValueError(f"J2_pade['{key}'] needs [a, b]")
+            j2[k] = v[:2]
+    return has_j1, j1, has_j2, j2
+
+
+# --------------------------------------------------------------------------
+# Flattened system
+# --------------------------------------------------------------------------
+@dataclass
+class System:
+    """Flat, kernel-ready description of one molecule and its trial state.
+
+    Exponent sharing: shells of the same atom and basis entry (the columns
+    of a general contraction) share their exponential factors, so the
+    kernels evaluate each distinct ``exp(-alpha r^2)`` once per electron
+    position (``pgroup``).
+    """
+    nuc: np.ndarray            # (natm, 3) bohr
+    Z: np.ndarray              # (natm,) float
+    shells: list
+    C: np.ndarray              # (nbf, nocc) occupied MO coefficients
+    n_up: int
+    n_dn: int
+    has_j1: bool
+    j1: np.ndarray             # (natm, 2)
+    has_j2: bool
+    j2: np.ndarray             # (2, 2) like, unlike
+    cusp: bool
+    cusp_rc: np.ndarray        # (natm,)
+    cusp_q0: np.ndarray        # (natm,)
+    cusp_coeff: np.ndarray     # (natm, 8)
+    symbols: list = field(default_factory=list)
+
+    @property
+    def natm(self):
+        return self.nuc.shape[0]
+
+    @property
+    def nbf(self):
+        return self.C.shape[0]
+
+    @property
+    def nocc(self):
+        return self.C.shape[1]
+
+    @property
+    def n_e(self):
+        return self.n_up + self.n_dn
+
+    @property
+    def e_nn(self):
+        """Nuclear repulsion with the reference's eps-softened distance
+        (``gto.py:2406-2430``)."""
+        eps = np.finfo(np.float64).eps
+        e = 0.0
+        for i in range(self.natm):
+            for j in range(i + 1, self.natm):
+                d = self.nuc[i] - self.nuc[j]
+                e += self.Z[i] * self.Z[j] / np.sqrt(np.dot(d, d) + eps)
+        return float(e)
+
+    def prim_groups(self):
+        """Distinct exponent sets: list of (iat, alpha array, [shell ids])."""
+        groups = {}
+        order = []
+        for i, sh in enumerate(self.shells):
+            key = (sh.iat, sh.entry)
+            if key not in groups:
+                groups[key] = (sh.iat, sh.alpha, [])
+                order.append(key)
+            groups[key][2].append(i)
+        return [groups[k] for k in order]
+
+    def n_exp(self):
+        """Distinct exponentials per electron position."""
+        return sum(len(a) for _, a, _ in self.prim_groups())
+
+    def n_prim_ref(self):
+        """Exponentials per position as the reference evaluates them
+        (one set per contraction column)."""
+        return sum(sh.nprim for sh in self.shells)
+
+
+def build_system(mf, params_corr=None, params_cusp=None):
+    """Build a :class:`System` from a PySCF-style mean-field object.
+
+    Args:
+        mf: object with ``mol`` (see :class:`Mole`), ``mo_coeff`` and
+            ``mo_occ``.
+        params_corr: Jastrow dict ``{"J1_pade": {sym: b or [a, b]},
+            "J2_pade": {"like": [a, b], "unlike": [a, b]}}``.
+        params_cusp: ``{sym: {"q0": float, "coeff": (8,)}}`` or None for no
+            cusp correction (``gto.py:846-888``).
+    """
+    mol = mf.mol
+    n_e = mol.tot_electrons()
+    n_up, n_dn = mol.nelec
+    if n_up != n_dn:
+        raise NotImplementedError(
+            "only closed-shell single determinants are supported "
+            f"(n_up={n_up}, n_dn={n_dn})")
+    nocc = int(np.count_nonzero(np.asarray(mf.mo_occ) > 0))
+    if nocc != n_up:
+        raise ValueError(f"mo_occ marks {nocc} occupied orbitals, expected "
+                         f"{n_up} for {n_e} electrons")
+    cusp = params_cusp is not None
+    shells = build_shells(mol, cusp=cusp)
+    nbf = shells[-1].isgs + shells[-1].nsgs
+    C = np.ascontiguousarray(np.asarray(mf.mo_coeff, dtype=np.float64)[:, :nocc])
+    if C.shape[0] != nbf:
+        raise ValueError(f"mo_coeff has {C.shape[0]} rows, basis has {nbf}")
+    natm = mol.natm
+    Z = mol.atom_charges().astype(np.float64)
+    rc = np.zeros(natm)
+    q0 = np.zeros(natm)
+    coeff = np.zeros((natm, 8))
+    if cusp:
+        for ia in range(natm):
+            sym = mol.atom_symbol(ia)
+            rc[ia] = 0.1 if Z[ia] == 1 else 0.2
+            q0[ia] = float(params_cusp[sym]["q0"])
+            cf = np.ravel(np.asarray(params_cusp[sym]["coeff"], dtype=np.float64))
+            if cf.shape[0] != 8:
+                raise ValueError(f"cusp coeff for {sym} must have 8 entries")
+            coeff[ia] = cf
+    has_j1, j1, has_j2, j2 = parse_params_corr(params_corr, mol, cusp)
+    return System(nuc=mol.atom_coords(unit="Bohr"), Z=Z, shells=shells, C=C,
+                  n_up=n_up, n_dn=n_dn, has_j1=has_j1, j1=j1, has_j2=has_j2,
+                  j2=j2, cusp=cusp, cusp_rc=rc, cusp_q0=q0,
+                  cusp_coeff=coeff, symbols=mol.elements)

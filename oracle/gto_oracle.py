@@ -1,0 +1,391 @@
+"""CPU FP64 oracle for the GTO Slater–Jastrow evaluation (TEST INFRASTRUCTURE).
+
+This module is the checker, never the product: only ``tests/``, the smoke
+entry point and the CPU-baseline leg of the benchmark may import it.  It
+restates the reference's per-walker evaluation in numpy, vectorised over
+walkers, line by line from:
+
+* ``OmegaQMC/psi/shell.py:37-148``   cusp-corrected s orbital (value, VGL)
+* ``OmegaQMC/psi/gto.py:607-725``    real solid harmonics and their gradients
+* ``OmegaQMC/psi/gto.py:781-811``    contracted radial value, R'/r, Laplacian
+* ``OmegaQMC/psi/gto.py:1012-1056``  AO values (``cgs_sph_get``)
+* ``OmegaQMC/psi/gto.py:1101-1214``  AO/MO value-gradient-Laplacian
+* ``OmegaQMC/psi/gto.py:728-778``    Slater assembly (inverse, Gamma, lap)
+* ``OmegaQMC/psi/gto.py:1278-1290``  log|det| of the up and down blocks
+* ``OmegaQMC/psi/gto.py:1493-1649``  Padé J1/J2 value and VGL
+* ``OmegaQMC/psi/gto.py:2220-2254``  log|psi| = log|det| + J
+* ``OmegaQMC/psi/gto.py:2406-2451``  eps-softened Coulomb terms
+* ``OmegaQMC/psi/gto.py:2506-2579``  analytic kinetic energy
+
+It is pinned against outputs of the reference's own source (run under a
+numpy/torch stand-in for JAX, ``tests/golden/make_golden.py``) and against
+the relations the reference's tests check (closed-form J1, the ``np.dot``
+cusp form, analytic versus autodiff-Hessian kinetic energy).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+EPS = float(np.finfo(np.float64).eps)
+MIN_DIST_THRESHOLD = 1e-4   # OmegaQMC/constants.py:23
+
+# ---------------------------------------------------------------------------
+# Real solid harmonics as monomial tables: Y_c = sum coef * x^i y^j z^k.
+# The polynomials are those of _angular_cartesian (gto.py:607-671).
+# ---------------------------------------------------------------------------
+_cd1 = math.sqrt(3.0)
+_cd2 = _cd1 * 0.5
+_cf1 = math.sqrt(2.5) * 0.5
+_cf2 = 3.0 * _cf1
+_cf3 = math.sqrt(15.0)
+_cf4 = math.sqrt(1.5) * 0.5
+_cf5 = math.sqrt(6.0)
+_cf6 = 1.5
+_cf7 = _cf3 * 0.5
+_cg = [None, 2.9580398915498085, 6.2749501990055672, 2.0916500663351894,
+       1.1180339887498949, 6.7082039324993694, 2.3717082451262845,
+       3.1622776601683795, 0.55901699437494745, 3.3541019662496847,
+       0.73950997288745213, 4.4370598373247132]
+
+HARMONICS = {
+    0: [[(1.0, 0, 0, 0)]],
+    1: [[(1.0, 1, 0, 0)], [(1.0, 0, 1, 0)], [(1.0, 0, 0, 1)]],
+    2: [[(_cd1, 1, 1, 0)],
+        [(_cd1, 0, 1, 1)],
+        [(1.0, 0, 0, 2), (-0.5, 2, 0, 0), (-0.5, 0, 2, 0)],
+        [(_cd1, 1, 0, 1)],
+        [(_cd2, 2, 0, 0), (-_cd2, 0, 2, 0)]],
+    3: [[(_cf2, 2, 1, 0), (-_cf1, 0, 3, 0)],
+        [(_cf3, 1, 1, 1)],
+        [(_cf5, 0, 1, 2), (-_cf4, 2, 1, 0), (-_cf4, 0, 3, 0)],
+        [(1.0, 0, 0, 3), (-_cf6, 2, 0, 1), (-_cf6, 0, 2, 1)],
+        [(_cf5, 1, 0, 2), (-_cf4, 3, 0, 0), (-_cf4, 1, 2, 0)],
+        [(_cf7, 2, 0, 1), (-_cf7, 0, 2, 1)],
+        [(-_cf2, 1, 2, 0), (_cf1, 3, 0, 0)]],
+    4: [[(_cg[1], 3, 1, 0), (-_cg[1], 1, 3, 0)],
+        [(_cg[2], 2, 1, 1), (-_cg[3], 0, 3, 1)],
+        [(-_cg[4], 3, 1, 0), (-_cg[4], 1, 3, 0), (_cg[5], 1, 1, 2)],
+        [(-_cg[6], 2, 1, 1), (-_cg[6], 0, 3, 1), (_cg[7], 0, 1, 3)],
+        [(0.375, 4, 0, 0), (0.375, 0, 4, 0), (0.75, 2, 2, 0), (1.0, 0, 0, 4),
+         (-3.0, 2, 0, 2), (-3.0, 0, 2, 2)],
+        [(-_cg[6], 3, 0, 1), (-_cg[6], 1, 2, 1), (_cg[7], 1, 0, 3)],
+        [(-_cg[8], 4, 0, 0), (_cg[8], 0, 4, 0), (_cg[9], 2, 0, 2),
+         (-_cg[9], 0, 2, 2)],
+        [(-_cg[2], 1, 2, 1), (_cg[3], 3, 0, 1)],
+        [(_cg[10], 4, 0, 0), (_cg[10], 0, 4, 0), (-_cg[11], 2, 2, 0)]],
+}
+
+
+def _pow(x, n):
+    return np.ones_like(x) if n == 0 else x ** n
+
+
+def harmonics(am, dr):
+    """Y (..., 2am+1) and grad Y (..., 2am+1, 3) at displacements dr (..., 3)."""
+    x, y, z = dr[..., 0], dr[..., 1], dr[..., 2]
+    comps = HARMONICS[am]
+    Y = np.zeros(dr.shape[:-1] + (len(comps),))
+    G = np.zeros(dr.shape[:-1] + (len(comps), 3))
+    for c, terms in enumerate(comps):
+        for coef, i, j, k in terms:
+            Y[..., c] += coef * _pow(x, i) * _pow(y, j) * _pow(z, k)
+            if i:
+                G[..., c, 0] += coef * i * _pow(x, i - 1) * _pow(y, j) * _pow(z, k)
+            if j:
+                G[..., c, 1] += coef * j * _pow(x, i) * _pow(y, j - 1) * _pow(z, k)
+            if k:
+                G[..., c, 2] += coef * k * _pow(x, i) * _pow(y, j) * _pow(z, k - 1)
+    return Y, G
+
+
+# ---------------------------------------------------------------------------
+# Cusp-corrected s orbital (shell.py:37-148)
+# ---------------------------------------------------------------------------
+def cusp_b(r, rc):
+    s = r / rc
+    return np.where(r < rc, 1.0 - 10.0 * s ** 3 + 15.0 * s ** 4 - 6.0 * s ** 5, 0.0)
+
+
+def cusp_s(r, rc, Z, rad_s, q0, coeff):
+    """f = c0 (1-b) R + b q0 e^{-Zr} (c1 + sum_{k=2..7} c_k (r/rc)^k)."""
+    b = cusp_b(r, rc)
+    sl = q0 * np.exp(-Z * r)
+    s = r / rc
+    poly = coeff[1] + sum(coeff[k] * s ** k for k in range(2, 8))
+    return coeff[0] * (1.0 - b) * rad_s + b * sl * poly
+
+
+def cusp_s_vgl(r, rc, Z, R, Rp_r, Rlap, q0, coeff):
+    """(f, f'/r, f'' + 2 f'/r) of the cusp-corrected s orbital.
+
+    The (1-b) R part is division free as in ``shell.py:107-130``; the
+    polynomial part Q = b q0 e^{-Zr} P(r) is differentiated analytically
+    (the reference uses scalar autodiff, ``shell.py:132-147``) and keeps the
+    plain ``Q'/r`` division."""
+    s = r / rc
+    oms = 1.0 - s
+    inside = r < rc
+    b = np.where(inside, 1.0 - 10.0 * s ** 3 + 15.0 * s ** 4 - 6.0 * s ** 5, 0.0)
+    bp = np.where(inside, -(30.0 / rc) * s ** 2 * oms ** 2, 0.0)
+    bp_r = np.where(inside, -(30.0 / rc ** 3) * r * oms ** 2, 0.0)
+    bpp = np.where(inside, -(60.0 / rc ** 2) * s * oms * (1.0 - 2.0 * s), 0.0)
+    BL = bpp + 2.0 * bp_r
+    c0 = coeff[0]
+    A_val = c0 * (1.0 - b) * R
+    A_gr = c0 * (-bp_r * R + (1.0 - b) * Rp_r)
+    A_lap = c0 * (-BL * R + (1.0 - b) * Rlap - 2.0 * r * bp * Rp_r)
+    S = q0 * np.exp(-Z * r)
+    P = coeff[1] + sum(coeff[k] * s ** k for k in range(2, 8))
+    P1 = sum(k * coeff[k] * s ** (k - 1) for k in range(2, 8)) / rc
+    P2 = sum(k * (k - 1) * coeff[k] * s ** (k - 2) for k in range(2, 8)) / rc ** 2
+    Q = b * S * P
+    Qp = bp * S * P - Z * b * S * P + b * S * P1
+    Qpp = (bpp * S * P + Z * Z * b * S * P + b * S * P2
+           + 2.0 * (-Z * bp * S * P + bp * S * P1 - Z * b * S * P1))
+    Qp = np.where(inside, Qp, 0.0)
+    Qpp = np.where(inside, Qpp, 0.0)
+    Q_gr = Qp / r
+    return A_val + Q, A_gr + Q_gr, A_lap + Qpp + 2.0 * Q_gr
+
+
+# ---------------------------------------------------------------------------
+# AO evaluation
+# ---------------------------------------------------------------------------
+def _shell_disp(system, sh, x):
+    dr = x - system.nuc[sh.iat]
+    r2 = np.sum(dr * dr, axis=-1)
+    return dr, r2, np.sqrt(r2)
+
+
+def ao_value(system, x):
+    """AO values (..., nbf) at positions x (..., 3) (``gto.py:1012-1056``)."""
+    out = np.zeros(x.shape[:-1] + (system.nbf,))
+    for sh in system.shells:
+        dr, r2, r = _shell_disp(system, sh, x)
+        R = np.sum(np.exp(-sh.alpha * r2[..., None]) * sh.norm, axis=-1)
+        if sh.am == 0 and sh.is_cusp:
+            ia = sh.iat
+            v = cusp_s(r, system.cusp_rc[ia], system.Z[ia], R,
+                       system.cusp_q0[ia], system.cusp_coeff[ia])[..., None]
+        else:
+            Y, _ = harmonics(sh.am, dr)
+            v = R[..., None] * Y
+        out[..., sh.isgs:sh.isgs + sh.nsgs] = v
+    return out
+
+
+def ao_vgl(system, x):
+    """AO value (..., nbf), gradient (..., nbf, 3), Laplacian (..., nbf)
+    (``gto.py:781-811, 1101-1186``)."""
+    shp = x.shape[:-1]
+    val = np.zeros(shp + (system.nbf,))
+    grad = np.zeros(shp + (system.nbf, 3))
+    lap = np.zeros(shp + (system.nbf,))
+    for sh in system.shells:
+        dr, r2, r = _shell_disp(system, sh, x)
+        e = np.exp(-sh.alpha * r2[..., None]) * sh.norm
+        R = np.sum(e, axis=-1)
+        Rp = np.sum(-2.0 * sh.alpha * e, axis=-1)
+        Rl = np.sum((4.0 * sh.alpha ** 2 * r2[..., None] - 6.0 * sh.alpha) * e, axis=-1)
+        sl = slice(sh.isgs, sh.isgs + sh.nsgs)
+        if sh.am == 0:
+            if sh.is_cusp:
+                ia = sh.iat
+                R, Rp, Rl = cusp_s_vgl(r, system.cusp_rc[ia], system.Z[ia], R, Rp,
+                                       Rl, system.cusp_q0[ia], system.cusp_coeff[ia])
+            val[..., sl] = R[..., None]
+            grad[..., sl, :] = (Rp[..., None] * dr)[..., None, :]
+            lap[..., sl] = Rl[..., None]
+        else:
+            Y, gY = harmonics(sh.am, dr)
+            val[..., sl] = R[..., None] * Y
+            grad[..., sl, :] = (Rp[..., None, None] * dr[..., None, :] * Y[..., None]
+                                + R[..., None, None] * gY)
+            lap[..., sl] = (Rl + 2.0 * sh.am * Rp)[..., None] * Y
+    return val, grad, lap
+
+
+def mo_value(system, X):
+    """MO values (W, n_e, nocc) (``gto.py:1058-1070``)."""
+    return ao_value(system, X) @ system.C
+
+
+def mo_vgl(system, X):
+    """MO value/gradient/Laplacian (``gto.py:1188-1214``)."""
+    v, g, l = ao_vgl(system, X)
+    return (v @ system.C, np.einsum("...ax,am->...mx", g, system.C),
+            l @ system.C)
+
+
+# ---------------------------------------------------------------------------
+# Slater determinant
+# ---------------------------------------------------------------------------
+def log_slater(system, X):
+    """log|det up| + log|det down| (``gto.py:1278-1290``)."""
+    mo = mo_value(system, X)
+    _, la = np.linalg.slogdet(mo[:, 0::2, :])
+    _, lb = np.linalg.slogdet(mo[:, 1::2, :])
+    return la + lb
+
+
+def slater_assemble(mo_val, mo_grad, mo_lap):
+    """(log|det|, grad_e (W,n_e,3), lap_e (W,n_e)) (``gto.py:728-778``)."""
+    W, n_e, _ = mo_val.shape
+    grad = np.zeros((W, n_e, 3))
+    lap = np.zeros((W, n_e))
+    logv = np.zeros(W)
+    for off in (0, 1):
+        S = mo_val[:, off::2, :]
+        G = mo_grad[:, off::2, :, :]
+        L = mo_lap[:, off::2, :]
+        A = np.linalg.inv(S)
+        Gam = np.einsum("wji,wijx->wix", A, G)
+        lp = np.einsum("wji,wij->wi", A, L) - np.sum(Gam * Gam, axis=-1)
+        _, ld = np.linalg.slogdet(S)
+        logv += ld
+        grad[:, off::2] = Gam
+        lap[:, off::2] = lp
+    return logv, grad, lap
+
+
+# ---------------------------------------------------------------------------
+# Padé Jastrow
+# ---------------------------------------------------------------------------
+def _pairs(n_e):
+    return np.triu_indices(n_e, k=1)
+
+
+def jastrow_value(system, X):
+    """J1 + J2 (``gto.py:1500-1573``)."""
+    W, n_e, _ = X.shape
+    J = np.zeros(W)
+    if system.has_j2:
+        i, j = _pairs(n_e)
+        d = X[:, i] - X[:, j]
+        r = np.sqrt(np.sum(d * d, axis=-1))
+        same = (i % 2) == (j % 2)
+        a = np.where(same, system.j2[0, 0], system.j2[1, 0])
+        b = np.where(same, system.j2[0, 1], system.j2[1, 1])
+        # like and unlike sums are separate in the reference
+        u = a * r / (1.0 + b * r)
+        J += np.sum(u * same, axis=-1) + np.sum(u * (~same), axis=-1)
+    if system.has_j1:
+        d = X[:, None, :, :] - system.nuc[None, :, None, :]
+        r = np.sqrt(np.sum(d * d, axis=-1))            # (W, natm, n_e)
+        a = system.j1[:, 0][None, :, None]
+        b = system.j1[:, 1][None, :, None]
+        J += np.sum(a * r / (1.0 + b * r), axis=(1, 2))
+    return J
+
+
+def jastrow_vgl(system, X):
+    """Per-electron gradient and Laplacian of J1 + J2 (``gto.py:1575-1649``)."""
+    W, n_e, _ = X.shape
+    grad = np.zeros((W, n_e, 3))
+    lap = np.zeros((W, n_e))
+    if system.has_j2:
+        i, j = _pairs(n_e)
+        d = X[:, i] - X[:, j]
+        r = np.sqrt(np.sum(d * d, axis=-1))
+        same = (i % 2) == (j % 2)
+        a = np.where(same, system.j2[0, 0], system.j2[1, 0])
+        b = np.where(same, system.j2[0, 1], system.j2[1, 1])
+        den = 1.0 + b * r
+        up = a / (den * den)
+        upp = -2.0 * a * b / (den * den * den)
+        gp = (up / r)[..., None] * d
+        lp = upp + 2.0 * up / r
+        for k in range(len(i)):
+            grad[:, i[k]] += gp[:, k]
+            grad[:, j[k]] -= gp[:, k]
+            lap[:, i[k]] += lp[:, k]
+            lap[:, j[k]] += lp[:, k]
+    if system.has_j1:
+        d = X[:, :, None, :] - system.nuc[None, None, :, :]
+        r = np.sqrt(np.sum(d * d, axis=-1))            # (W, n_e, natm)
+        a = system.j1[:, 0][None, None, :]
+        b = system.j1[:, 1][None, None, :]
+        den = 1.0 + b * r
+        up = a / (den * den)
+        upp = -2.0 * a * b / (den * den * den)
+        grad += np.sum((up / r)[..., None] * d, axis=2)
+        lap += np.sum(upp + 2.0 * up / r, axis=2)
+    return grad, lap
+
+
+# ---------------------------------------------------------------------------
+# Energies
+# ---------------------------------------------------------------------------
+def e_ee(X):
+    """sum_{i<j} 1/sqrt(r^2 + eps) (``gto.py:2406-2440``)."""
+    n_e = X.shape[1]
+    i, j = _pairs(n_e)
+    d = X[:, i] - X[:, j]
+    return np.sum(1.0 / np.sqrt(np.sum(d * d, axis=-1) + EPS), axis=-1)
+
+
+def e_en(system, X):
+    """-sum Z / sqrt(r^2 + eps) (``gto.py:2445-2451``)."""
+    d = X[:, :, None, :] - system.nuc[None, None, :, :]
+    return np.sum(-system.Z[None, None, :] / np.sqrt(np.sum(d * d, axis=-1) + EPS),
+                  axis=(1, 2))
+
+
+def log_psi(system, X):
+    """log|psi| (``gto.py:2220-2254``)."""
+    X = np.asarray(X, dtype=np.float64)
+    return log_slater(system, X) + jastrow_value(system, X)
+
+
+def evaluate(system, X):
+    """Full per-walker evaluation.
+
+    Returns a dict with ``logpsi`` (W,), ``grad`` (W, n_e, 3) =
+    grad log|psi|, ``lap`` (W, n_e) = per-electron Laplacian of log|psi|,
+    ``e_ee``, ``e_en``, ``e_ke`` and ``e_loc`` = ee + en + ke + nn, following
+    ``local_energy_ke`` (``gto.py:2506-2579``) and ``_local_energy_batch``
+    (``OmegaQMC/vmc_gto.py:801-812``)."""
+    X = np.asarray(X, dtype=np.float64)
+    mv, mg, ml = mo_vgl(system, X)
+    _, gs, ls = slater_assemble(mv, mg, ml)
+    gj, lj = jastrow_vgl(system, X)
+    grad = gs + gj
+    lap = ls + lj
+    ke = -0.5 * (np.sum(lap, axis=-1) + np.sum(grad * grad, axis=(1, 2)))
+    ee = e_ee(X)
+    en = e_en(system, X)
+    return {"logpsi": log_psi(system, X), "grad": grad, "lap": lap,
+            "e_ee": ee, "e_en": en, "e_ke": ke,
+            "e_loc": ee + en + ke + system.e_nn}
+
+
+def local_energy(system, X):
+    return evaluate(system, X)["e_loc"]
+
+
+# ---------------------------------------------------------------------------
+# Statistics: do_binning_analysis (OmegaQMC/utils.py:86-150)
+# ---------------------------------------------------------------------------
+def binning_analysis(a):
+    """(mean, serr, sdev, kappa); kappa = 1 + 2 sum_{k>=1} ac_k summed until
+    the first negative normalised autocorrelation."""
+    a = np.asarray(a, dtype=np.float64)
+    n = a.shape[0]
+    xbar = a.mean()
+    sdev = a.std()
+    x = a - xbar
+    nfft = 1 << int(math.ceil(math.log2(max(2 * n - 1, 1))))
+    fx = np.fft.rfft(x, nfft)
+    ac = np.fft.irfft(fx * np.conj(fx), nfft)[:n]
+    if ac[0] == 0:
+        return xbar, 0.0, sdev, 1.0
+    ac = ac / ac[0]
+    kappa = 1.0
+    for k in range(1, n):
+        if ac[k] < 0:
+            break
+        kappa += 2.0 * ac[k]
+    serr = sdev * math.sqrt(kappa / n)
+    return float(xbar), float(serr), float(sdev), float(kappa)

@@ -1,0 +1,277 @@
+"""Generate golden vectors by running the reference's own wavefunction code.
+
+Run in a container that has the reference checkout (read-only) at
+``/root/reference`` (override with ``OMEGAQMC_REF``)::
+
+    python tests/golden/make_golden.py
+
+JAX and PySCF are not installed, so the reference modules
+``OmegaQMC/psi/shell.py``, ``OmegaQMC/psi/gto.py`` and ``OmegaQMC/utils.py``
+are imported unmodified from the checkout with ``jax_standin`` registered as
+``jax`` (torch float64 underneath) and empty stand-ins for PySCF/h5py module
+imports that the evaluation never calls.  The molecule is passed as a
+duck-typed mean-field object built from this package's :class:`Mole`.
+
+For each case the script stores the system specification (atoms, basis,
+occupied MOs, Jastrow and cusp parameters), seeded walker configurations and
+the reference's per-walker outputs: ``log_trial_wavefunction``,
+``local_energy_ee/en/ke``, ``local_energy_nn``, the analytic gradient of
+log|psi| (the ``grad_flat`` that ``local_energy_ke`` builds,
+``gto.py:2513-2575``) and the per-electron Laplacian.  It also stores one
+``do_binning_analysis`` result (``utils.py:86-150``) on a seeded series.
+"""
+from __future__ import annotations
+
+import importlib
+import json
+import os
+import sys
+import types
+import warnings
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+import jax_standin  # noqa: E402
+
+jax_standin.install()
+import torch  # noqa: E402
+
+from omegaqmc_b200.system import Mole, MeanField, ELEMENT_Z  # noqa: E402
+from omegaqmc_b200 import molecules as M  # noqa: E402
+
+REF = os.environ.get("OMEGAQMC_REF", "/root/reference")
+
+
+def _stub(name, **attrs):
+    m = types.ModuleType(name)
+    for k, v in attrs.items():
+        setattr(m, k, v)
+    sys.modules[name] = m
+    return m
+
+
+def load_reference():
+    """Import the reference's shell/gto/utils modules from the checkout."""
+    _stub("h5py")
+    _stub("pyscf", __config__=types.SimpleNamespace(),
+          gto=types.SimpleNamespace(Mole=type("Mole", (), {})))
+    _stub("pyscf.gto", Mole=type("Mole", (), {}))
+    _stub("pyscf.gto.basis", _format_basis_name=lambda s: s)
+    _stub("pyscf.lib", logger=types.SimpleNamespace(), param=types.SimpleNamespace())
+    _stub("pyscf.data")
+    _stub("pyscf.data.elements", MASSES=[0.0] * 120, ELEMENTS_PROTON={},
+          _atom_symbol=lambda s: s)
+    pkg = types.ModuleType("OmegaQMC")
+    pkg.__path__ = [os.path.join(REF, "OmegaQMC")]
+    sys.modules["OmegaQMC"] = pkg
+    psi = types.ModuleType("OmegaQMC.psi")
+    psi.__path__ = [os.path.join(REF, "OmegaQMC", "psi")]
+    sys.modules["OmegaQMC.psi"] = psi
+    utils = importlib.import_module("OmegaQMC.utils")
+    shell = importlib.import_module("OmegaQMC.psi.shell")
+    gto = importlib.import_module("OmegaQMC.psi.gto")
+    return gto, shell, utils
+
+
+class _RefMole:
+    """Adapter exposing this package's Mole with tensor charges."""
+
+    def __init__(self, mol):
+        self._m = mol
+        self._atom = mol._atom
+        self._basis = mol._basis
+        self.natm = mol.natm
+        self.basis = mol.basis
+        self.elements = mol.elements
+        self.charge = mol.charge
+
+    def atom_charges(self):
+        return torch.tensor(self._m.atom_charges(), dtype=torch.int64)
+
+    def tot_electrons(self):
+        return self._m.tot_electrons()
+
+    def atom_symbol(self, i):
+        return self._m.atom_symbol(i)
+
+    def atom_coords(self, unit="Bohr"):
+        return self._m.atom_coords(unit)
+
+
+class _RefMF:
+    def __init__(self, mf):
+        self.mol = _RefMole(mf.mol)
+        self.mo_coeff = torch.tensor(mf.mo_coeff)
+        self.mo_occ = mf.mo_occ
+
+
+def _walkers(mol, n, sigma, seed):
+    rng = np.random.default_rng(seed)
+    Z = mol.atom_charges()
+    idx = np.repeat(np.arange(mol.natm), Z)
+    nuc = mol.atom_coords()
+    return nuc[idx][None] + sigma * rng.standard_normal((n, len(idx), 3))
+
+
+def _to_json(obj):
+    if isinstance(obj, dict):
+        return {k: _to_json(v) for k, v in obj.items()}
+    if isinstance(obj, (list, tuple)):
+        return [_to_json(v) for v in obj]
+    if isinstance(obj, np.ndarray):
+        return obj.tolist()
+    if isinstance(obj, (np.floating, np.integer)):
+        return obj.item()
+    return obj
+
+
+def fg_test_system():
+    """Small system whose basis has f and g shells (am 3, 4)."""
+    basis = {
+        "Be": [[0, [40.0, 0.3, -0.1], [8.0, 0.6, -0.2], [1.5, 0.3, 0.7]],
+               [1, [3.0, 0.4], [0.7, 0.7]],
+               [2, [1.1, 1.0]],
+               [3, [0.9, 1.0]],
+               [4, [0.8, 1.0]]],
+        "H": [[0, [5.0, 0.2], [0.9, 0.6], [0.25, 0.4]], [1, [0.7, 1.0]]],
+    }
+    atoms = [("Be", (0.0, 0.1, -0.3)), ("H", (0.2, -0.1, 2.4)),
+             ("H", (-0.3, 0.2, -2.9))]
+    return Mole(atoms, basis)
+
+
+CASES = {
+    # name: (mol builder, use cusp, params builder, sigma, n walkers)
+    "h2_sto3g": (lambda: M.named_system("H2"), False,
+                 lambda mol: {"J2_pade": {"like": np.array([0.25, 1.0]),
+                                          "unlike": np.array([0.5, 1.0])}},
+                 0.5, 24),
+    "h2o_nocusp": (lambda: M.named_system("H2O"), False,
+                   lambda mol: {"J1_pade": {"O": np.array(0.9), "H": np.array(0.4)},
+                                "J2_pade": {"like": np.array([0.25, 0.6]),
+                                            "unlike": np.array([0.5, 0.4])}},
+                   0.6, 24),
+    "h2o_cusp": (lambda: M.named_system("H2O"), True,
+                 lambda mol: {"J1_pade": {"O": np.array([-0.4, 0.9]),
+                                          "H": np.array([-0.1, 0.5])},
+                              "J2_pade": {"like": np.array([0.25, 1.0]),
+                                          "unlike": np.array([0.5, 1.0])}},
+                 0.6, 24),
+    "lih_cusp": (lambda: M.named_system("LiH"), True,
+                 lambda mol: {"J2_pade": {"like": np.array([0.25, 0.8]),
+                                          "unlike": np.array([0.5, 0.8])}},
+                 1.0, 16),
+    "n2_nocusp": (lambda: M.named_system("N2"), False,
+                  lambda mol: {"J1_pade": {"N": np.array(1.1)},
+                               "J2_pade": {"like": np.array([0.25, 1.0]),
+                                           "unlike": np.array([0.5, 1.0])}},
+                  0.7, 8),
+    "fg_shells": (fg_test_system, True,
+                  lambda mol: {"J1_pade": {"Be": np.array([-0.3, 0.8]),
+                                           "H": np.array([-0.05, 0.6])},
+                               "J2_pade": {"like": np.array([0.25, 0.7]),
+                                           "unlike": np.array([0.5, 0.7])}},
+                  0.8, 12),
+    "nojastrow": (lambda: M.named_system("LiH"), False, lambda mol: {}, 1.0, 8),
+}
+
+
+def run_case(gto, name, seed):
+    mk, cusp, mkp, sigma, nw = CASES[name]
+    mol = mk()
+    mf = M.MeanField(mol, M.seeded_mo_coeff(mol, seed=seed))
+    params = mkp(mol)
+    pcusp = M.synthetic_cusp_params(mol, seed=seed + 11) if cusp else None
+    X = _walkers(mol, nw, sigma, seed + 101)
+    rmf = _RefMF(mf)
+    obj = gto._PsiGTO(rmf, params_cusp=(
+        {s: {"q0": torch.tensor(v["q0"]), "coeff": torch.tensor(v["coeff"])}
+         for s, v in pcusp.items()} if cusp else None))
+    nuc = torch.tensor(mol.atom_coords())
+    tp = {}
+    for k, v in params.items():
+        if isinstance(v, dict):
+            tp[k] = {kk: torch.tensor(np.asarray(vv, dtype=np.float64))
+                     for kk, vv in v.items()}
+    out = {k: [] for k in ("logpsi", "e_ee", "e_en", "e_ke", "grad", "lap")}
+    for w in range(nw):
+        x = torch.tensor(X[w])
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            lp = obj.log_trial_wavefunction(x, nuc, tp)
+            ke = obj.local_energy_ke(x, nuc, tp)
+            _, gs, ls = obj._log_slater_analytic(x, nuc)
+            grad = gs.reshape(-1)
+            lap = ls
+            if "J1_pade" in tp:
+                g, L = obj._J1_pade_vgl(x, nuc, tp["J1_pade"])
+                grad = grad + g.reshape(-1)
+                lap = lap + L
+            if "J2_pade" in tp:
+                g, L = obj._J2_pade_vgl(x, tp["J2_pade"])
+                grad = grad + g.reshape(-1)
+                lap = lap + L
+        out["logpsi"].append(float(lp))
+        out["e_ke"].append(float(ke))
+        out["e_ee"].append(float(obj.local_energy_ee(x)))
+        out["e_en"].append(float(obj.local_energy_en(x, nuc)))
+        out["grad"].append(grad.detach().numpy().reshape(-1, 3))
+        out["lap"].append(lap.detach().numpy())
+    e_nn = float(obj.local_energy_nn(nuc))
+    # the autodiff-Hessian kinetic energy on the first walkers
+    ke_h = []
+    for w in range(min(3, nw)):
+        x = torch.tensor(X[w])
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            ke_h.append(float(obj._local_energy_ke_hessian(x, nuc, tp)))
+    spec = {"atoms": mol._atom, "basis": mol._basis, "cusp": pcusp,
+            "params_corr": params}
+    res = {k: np.array(v) for k, v in out.items()}
+    res.update(X=X, mo_coeff=mf.mo_coeff, mo_occ=mf.mo_occ, e_nn=e_nn,
+               e_ke_hessian=np.array(ke_h),
+               spec=np.array(json.dumps(_to_json(spec))))
+    return res
+
+
+def main():
+    gto, shell, utils = load_reference()
+    os.makedirs(HERE, exist_ok=True)
+    for k, name in enumerate(CASES):
+        res = run_case(gto, name, seed=k)
+        np.savez_compressed(os.path.join(HERE, f"golden_{name}.npz"), **res)
+        print(f"{name}: {len(res['logpsi'])} walkers, logpsi[0]={res['logpsi'][0]:.12f}")
+    # binning analysis on a seeded AR(1) series
+    rng = np.random.default_rng(42)
+    x = np.zeros(2000)
+    for i in range(1, 2000):
+        x[i] = 0.8 * x[i - 1] + rng.standard_normal()
+    xbar, serr, sdev, kappa = utils.do_binning_analysis(torch.tensor(x))
+    np.savez_compressed(os.path.join(HERE, "golden_binning.npz"), series=x,
+                        result=np.array([float(xbar), float(serr), float(sdev),
+                                         float(kappa)]))
+    # the cusp-s value at the radii the reference's sharding test uses
+    rng = np.random.default_rng(0)
+    coeff = rng.normal(size=8)
+    rs = np.array([0.0, 0.03, 0.11, 0.2, 0.5])
+    vals = [float(shell.evaluate_cusp_s(torch.tensor(r), 0.25, 8.0, 0.7, 1.3,
+                                        torch.tensor(coeff))) for r in rs]
+    # VGL at radii inside and outside rc
+    rv = np.array([0.013, 0.05, 0.12, 0.19, 0.31])
+    vgl = []
+    for r in rv:
+        f, fp, fl = shell.evaluate_cusp_s_vgl(torch.tensor(r), 0.2, 8.0, 0.7, -1.1,
+                                              3.3, 1.3, torch.tensor(coeff))
+        vgl.append([float(f), float(fp), float(fl)])
+    np.savez_compressed(os.path.join(HERE, "golden_cusp.npz"), coeff=coeff,
+                        r=rs, val=np.array(vals), r_vgl=rv, vgl=np.array(vgl))
+    print("binning kappa", float(kappa))
+
+
+if __name__ == "__main__":
+    main()
