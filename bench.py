@@ -1,0 +1,389 @@
+"""Benchmark: decorrelated samples/s of GTO-VMC, H2O cc-pVDZ-shaped, 65,536 walkers.
+
+One step = one sweep of all walkers: every electron proposes a single-electron
+Gaussian move (exact Metropolis acceptance, Sherman-Morrison inverse update),
+then the local energy of every walker is evaluated and reduced.  A full FP64
+LU refresh of each inverse runs every 50 sweeps inside the timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision mixed|fp64] [--system H2O] [--walkers 65536]
+
+value     = walkers x sweeps/s / tau_int(E_L)  (decorrelated samples/s, all ranks)
+tau_int   = kappa of the reference's do_binning_analysis (OmegaQMC/utils.py:86-150)
+            on the walker-mean E_L series (sweeps); from the timed series when it
+            has >= 1000 sweeps, else from an untimed 2000-sweep run.
+e2e       = the same metric through the public API with host buffers: every step
+            copies the walker positions host->device (pinned), runs the sweep
+            and copies positions + the step's reductions back.
+--impl reference  times the reference algorithm (all-electron moves, log|psi|
+            recomputed twice per step, E_L every step) restated in C/OpenMP on
+            all host cores.
+Multi-GPU: one process per GPU, independent walker sets (replicas; no
+collective on the data path), value summed over ranks, time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+REFRESH_EVERY = 50
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--system", default="H2O")
+    ap.add_argument("--walkers", type=int, default=65536)
+    ap.add_argument("--step-size", type=float, default=0.0)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+STEP_DEFAULT = {"H2": 0.6, "LiH": 0.5, "H2O": 0.3, "N2": 0.3, "H2O_dimer": 0.3}
+
+
+def build_system(name):
+    from omegaqmc_b200 import molecules as M
+    from omegaqmc_b200.system import build_system as bs
+    mf = M.make_mf(name)
+    params = M.default_params_corr(mf.mol)
+    if name == "H2":
+        params = {"J2_pade": params["J2_pade"]}
+    return bs(mf, params)
+
+
+def work_per_walker_sweep(s, acc=0.5):
+    """Algorithmic work of one sweep of one walker (FMA = 2 flops).
+
+    Moves (per electron): distinct exponentials; radial sums 2 flops per
+    (primitive, column); angular 3 (p) / 17 (d) / 12*(2l+1) (f, g); MO row
+    2 nbf nocc; ratio vector 2 nocc^2; Sherman-Morrison 2 nocc^2 x acceptance;
+    Jastrow change 2 x 14 flops per other particle.  Local energy (per
+    electron): exponentials; radial VGL 6 flops per (primitive, column);
+    angular VGL 12 per AO; MO VGL 10 nbf nocc; Slater assembly 8 nocc + 6;
+    Jastrow VGL 20 per partner; Coulomb 10 per pair.
+    """
+    groups = s.prim_groups()
+    n_exp = sum(len(a) for _, a, _ in groups)
+    rad = sum(len(a) * len(ids) for _, a, ids in groups)
+    ang_v = sum({0: 0, 1: 3, 2: 17}.get(sh.am, 12 * (2 * sh.am + 1)) for sh in s.shells)
+    ne, no, nb, nn = s.n_e, s.nocc, s.nbf, s.natm
+    move = 2 * rad + ang_v + 2 * nb * no + 2 * no * no + 2 * no * no * acc + 28 * (ne - 1 + nn)
+    el = 6 * rad + 12 * nb + 10 * nb * no + 8 * no + 6 + 20 * (ne - 1 + nn)
+    coul = 10 * (ne * (ne - 1) // 2 + ne * nn)
+    flops = ne * (move + el) + coul
+    return {"flops": float(flops), "exps": float(2 * ne * n_exp)}
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 5 + k and r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def cpu_reference(system, seconds, nthreads, step, seed=7):
+    """Reference algorithm on host cores; returns (walker-steps/s, tau, sample)."""
+    from oracle import cref
+    from oracle import gto_oracle as O
+    from omegaqmc_b200.sampler import init_walkers_gaussian
+    W = 256
+    X = np.ascontiguousarray(init_walkers_gaussian(system, W, 1.0, seed))
+    cref.run(system, X, 20, step, seed=seed, nthreads=nthreads)        # equilibrate
+    t0 = time.perf_counter()
+    ser, acc = cref.run(system, X, 10, step, seed=seed + 1, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    per_step = dt / 10
+    n = max(50, int(seconds / max(per_step, 1e-6)))
+    t0 = time.perf_counter()
+    ser, acc = cref.run(system, X, n, step, seed=seed + 2, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    rate = W * n / dt
+    _, _, _, kappa = O.binning_analysis(ser[:, 3])
+    return rate, kappa, acc, f"{W} walkers x {n} steps ({dt:.1f} s)", ser[:, 3]
+
+
+def run_reference(a):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    system = build_system(a.system)
+    step = a.step_size or STEP_DEFAULT.get(a.system, 0.3) * 1.0
+    cores = len(os.sched_getaffinity(0))
+    # the reference's all-electron move needs a smaller step than a sweep
+    ref_step = step * 0.5
+    rates, kappas = [], []
+    for _ in range(max(1, min(a.steps, 3))):
+        rate, kappa, acc, sample, _ = cpu_reference(system, a.cpu_seconds / 3, cores, ref_step)
+        rates.append(rate)
+        kappas.append(kappa)
+    rate = float(np.mean(rates))
+    kappa = float(np.mean(kappas))
+    value = rate / kappa
+    unit = "decorrelated samples/s"
+    line = {
+        "impl": "reference", "metric": "decorrelated samples/s (walker-steps/s / tau_int)",
+        "value": value, "unit": unit, "n_gpus": 0, "steps": a.steps, "warmup": a.warmup,
+        "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{a.system} cc-pVDZ-shaped, reference algorithm on host cores",
+                   "walkers_sample": 256, "move": "all-electron", "step": ref_step},
+        "walker_steps_per_s": rate, "tau_int": kappa, "acceptance": acc,
+        "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "vs_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+    from omegaqmc_b200 import _lib as L
+    from omegaqmc_b200.context import GTOContext
+    from omegaqmc_b200.sampler import WalkerEnsemble, init_walkers_gaussian, NSUM
+    from oracle import gto_oracle as O  # noqa: F401  (tau estimator is the oracle's restatement)
+
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    system = build_system(a.system)
+    ctx = GTOContext(system)
+    W = a.walkers
+    step = a.step_size or STEP_DEFAULT.get(a.system, 0.3)
+    X0 = init_walkers_gaussian(system, W, 1.0, seed=1000 + rank)
+    ens = WalkerEnsemble(ctx, X0, a.precision, seed=2024 + 7919 * rank,
+                         refresh_every=REFRESH_EVERY)
+    stream = torch.cuda.current_stream()
+
+    # warm-up (also equilibrates)
+    ens.run(max(a.warmup, 3), step)
+    torch.cuda.synchronize()
+
+    K = a.steps
+    sums = torch.zeros(K, NSUM, dtype=torch.float64, device=dev)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        ens.run(K, step, sums=sums)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    flags = ctx.flags()
+    s_np = sums.cpu().numpy()
+    series = s_np[:, 3] / np.maximum(s_np[:, 6], 1)
+    if K >= 1000:
+        tau_series = series
+        tau_src = f"timed series ({K} sweeps)"
+    else:
+        aux = ens.run(2000, step).cpu().numpy()
+        tau_series = aux[:, 3] / np.maximum(aux[:, 6], 1)
+        tau_src = "untimed 2000-sweep series"
+    e_mean, e_serr, e_sdev, kappa = O.binning_analysis(tau_series)
+    acc = float(s_np[:, 5].sum() / (K * W * system.n_e))
+
+    # kernel-level timing of the dominant kernel on its own stream: one chunk
+    # of REFRESH_EVERY sweeps = one k_sweeps launch; the refresh separately
+    chunk_sums = torch.zeros(REFRESH_EVERY, NSUM, dtype=torch.float64, device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e2 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.sweeps(ens.X, ens.state, ens.prec, REFRESH_EVERY, step, ens.seed, 10**7,
+               chunk_sums, stream=stream)
+    e1.record(stream)
+    ctx.refresh(ens.X, ens.state, ens.prec, stream=stream)
+    e2.record(stream)
+    torch.cuda.synchronize()
+    sweep_ms = e0.elapsed_time(e1)
+    refresh_ms = e1.elapsed_time(e2)
+
+    # e2e: host buffers through the public API
+    e2e = None
+    if not a.no_e2e:
+        Ke = min(K, 200)
+        hostX = torch.empty_like(ens.X, device="cpu").pin_memory()
+        hostX.copy_(ens.X)
+        host_sums = torch.empty(NSUM, dtype=torch.float64).pin_memory()
+        s1 = torch.zeros(Ke, NSUM, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for k in range(Ke):
+            ens.X.copy_(hostX, non_blocking=True)
+            ens.run(1, step, sums=s1[k:k + 1])
+            hostX.copy_(ens.X, non_blocking=True)
+            host_sums.copy_(s1[k], non_blocking=True)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ems = f0.elapsed_time(f1)
+        bi = ens.X.numel() * 8
+        e2e = {"ms_per_step": ems / Ke, "steps": Ke,
+               "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bi + NSUM * 8}
+
+    # max over ranks
+    t = torch.tensor([ms, e2e["ms_per_step"] if e2e else 0.0], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max, e2e_ms = float(t[0]), float(t[1])
+
+    wss = W * world * K / (ms_max * 1e-3)
+    value = wss / kappa
+    work = work_per_walker_sweep(system, acc)
+    peak_kind = 0 if a.precision == "fp64" else 1
+    rate = ctypes_peak(L, peak_kind)
+    achieved = work["flops"] * W * REFRESH_EVERY / (sweep_ms * 1e-3)
+    traffic = ncu_traffic(a.system, a.precision)
+    line = {
+        "metric": "decorrelated samples/s (walker-steps/s / tau_int) vs plain FP64, H2O 64k walkers",
+        "value": value, "unit": "decorrelated samples/s", "n_gpus": world, "steps": K,
+        "warmup": a.warmup, "ms_per_step": ms_max / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if a.precision == "mixed" else "f64",
+        "data": "synthetic",
+        "config": {"workload": f"{a.system} cc-pVDZ-shaped, {W} walkers/GPU, single-electron "
+                               f"sweeps + E_L every sweep, FP64 LU refresh every {REFRESH_EVERY}",
+                   "precision": a.precision, "walkers_per_gpu": W, "step": step,
+                   "parallelism": f"replicas x{world}",
+                   "l2": "walker state stays in shared memory for a whole launch; "
+                         "inputs 41 MB are re-read once per 50-sweep launch"},
+        "walker_sweeps_per_s": wss, "tau_int": kappa, "tau_source": tau_src,
+        "energy": {"mean": e_mean, "serr": e_serr}, "acceptance": acc, "kernel_flags": flags,
+        "gpu_launches": int(math.ceil(K / REFRESH_EVERY)) * 2,
+        "roofline": {"bound": "fp64" if peak_kind == 0 else "fp32",
+                     "achieved": achieved / 1e12, "peak": rate / 1e12, "unit": "TFLOP/s",
+                     "frac": achieved / rate if rate else None, "traffic": traffic,
+                     "kernel": "k_sweeps", "kernel_ms_per_launch": sweep_ms,
+                     "refresh_ms_per_launch": refresh_ms,
+                     "flops_per_walker_sweep": work["flops"],
+                     "peak_source": "own FMA microkernel (oqmc_measure_peak), of measured"},
+    }
+    if e2e:
+        line["e2e"] = {"value": W * world / (e2e_ms * 1e-3) / kappa,
+                       "unit": "decorrelated samples/s",
+                       "h2d_bytes_per_step": e2e["h2d_bytes_per_step"],
+                       "d2h_bytes_per_step": e2e["d2h_bytes_per_step"],
+                       "ms_per_step": e2e_ms}
+    if rank == 0 and not a.no_cpu and world == 1:
+        cores = len(os.sched_getaffinity(0))
+        r, kap, acc_c, sample, _ = cpu_reference(system, a.cpu_seconds, cores, step * 0.5)
+        line["cpu_baseline"] = {"value": r / kap, "unit": "decorrelated samples/s",
+                                "cores": cores, "kind": "port", "sample": sample,
+                                "walker_steps_per_s": r, "tau_int": kap}
+    with ClockSampler(local) as _:
+        pass
+    line["clocks"] = clk.summary()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def ctypes_peak(L, kind):
+    import ctypes
+    import torch
+    lib = L.load()
+    out = ctypes.c_double(0.0)
+    code = lib.oqmc_measure_peak(int(kind), ctypes.byref(out),
+                                 ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    return out.value if code == 0 else None
+
+
+def ncu_traffic(system, precision):
+    """DRAM bytes per k_sweeps launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return d.get(f"{system}/{precision}")
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -110,8 +110,15 @@ int oqmc_eval(oqmc_ctx* ctx, const double* walkers, int W, double* logpsi,
 int oqmc_log_psi(oqmc_ctx* ctx, const double* walkers, int W, double* logpsi,
                  void* stream);
 
-/* Bytes of sampler state for W walkers at a precision (inverse Slater
- * matrices and log|det|). */
+/* Occupied MO values (W, n_e, nocc) at every electron.  Replaces the
+ * mo_val output of get_psi_mo (OmegaQMC/psi/gto.py:1058-1070). */
+int oqmc_mo_values(oqmc_ctx* ctx, const double* walkers, int W, double* out,
+                   void* stream);
+
+/* Bytes of sampler state for W walkers at a precision: walker-minor
+ * positions, inverse Slater matrices and log|det|.  The state is derived
+ * from the walkers by oqmc_refresh; after changing walkers outside the
+ * library, refresh before the next sweep. */
 size_t oqmc_state_bytes(const oqmc_ctx* ctx, int W, int precision);
 
 /* Full FP64 LU refresh of the sampler state from positions (the periodic
@@ -135,6 +142,16 @@ int oqmc_sweeps(oqmc_ctx* ctx, double* walkers, int W, void* state,
                 double* el_trace, double* eparts_last, int walkers_per_block,
                 void* stream);
 
+/* n_steps basin relocations on every walker: one random electron is
+ * proposed at N(R_J, sigma^2) around a random nucleus J and accepted with
+ * the exact Metropolis-Hastings ratio including q(old)/q(new),
+ * q(x) = sum_J exp(-|x - R_J|^2 / 2 sigma^2).  acc_sum: optional device
+ * double that accumulates accepted moves.  Replaces basin_move_1w and
+ * _thermalize_basins (OmegaQMC/vmc_gto.py:925-957, 1036-1053). */
+int oqmc_basin(oqmc_ctx* ctx, double* walkers, int W, void* state, int precision,
+               int n_steps, double sigma, uint64_t seed, uint64_t step_base,
+               double* acc_sum, void* stream);
+
 /* Exponent threshold above which an exponent group is evaluated in FP64
  * near its nucleus in the mixed build (default 50.0; <= 0 disables). */
 int oqmc_set_split(oqmc_ctx* ctx, double tight_alpha);
@@ -142,6 +159,12 @@ int oqmc_set_split(oqmc_ctx* ctx, double tight_alpha);
 /* Synchronise `stream`, return the OR of kernel flag bits since the last
  * clear in *flags and optionally clear them. */
 int oqmc_get_flags(oqmc_ctx* ctx, unsigned* flags, int clear, void* stream);
+
+/* Measured arithmetic throughput of the current GPU, the roofline
+ * denominators of the CUDA-core kernels: kind 0 = FP64 FMA flop/s,
+ * 1 = FP32 FMA flop/s, 2 = FP32 exponentials/s (SFU).  A measurement
+ * utility with no counterpart in the reference. */
+int oqmc_measure_peak(int kind, double* out_rate, void* stream);
 
 #ifdef __cplusplus
 }

@@ -67,13 +67,17 @@ _SIGS = [
     ("oqmc_eval", c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
                           c_void_p, c_void_p]),
     ("oqmc_log_psi", c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    ("oqmc_mo_values", c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     ("oqmc_state_bytes", c_size_t, [c_void_p, c_int, c_int]),
     ("oqmc_refresh", c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p]),
     ("oqmc_sweeps", c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_int, c_int,
                             c_double, c_uint64, c_uint64, c_void_p, c_void_p, c_void_p,
                             c_int, c_void_p]),
+    ("oqmc_basin", c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_int, c_double,
+                           c_uint64, c_uint64, c_void_p, c_void_p]),
     ("oqmc_set_split", c_int, [c_void_p, c_double]),
     ("oqmc_get_flags", c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint), c_int, c_void_p]),
+    ("oqmc_measure_peak", c_int, [c_int, P_double, c_void_p]),
 ]
 
 EXPORTED = [s[0] for s in _SIGS]

@@ -167,6 +167,14 @@ class GTOContext:
                                           _stream_ptr(stream)))
         return out
 
+    def mo_values(self, X, stream=None):
+        X = self.walkers_tensor(X)
+        out = torch.empty(X.shape[0], self.n_e, self.nocc, dtype=torch.float64,
+                          device=self.device)
+        self._check(self.lib.oqmc_mo_values(self._h, _dptr(X), X.shape[0], _dptr(out),
+                                            _stream_ptr(stream)))
+        return out
+
     # -- sampler ------------------------------------------------------------
     def state_bytes(self, W, precision):
         return int(self.lib.oqmc_state_bytes(self._h, int(W), int(precision)))
@@ -187,6 +195,13 @@ class GTOContext:
             int(measure_every), float(step), ctypes.c_uint64(seed & (2**64 - 1)),
             ctypes.c_uint64(step_base), _dptr(sums), _dptr(el_trace), _dptr(eparts_last),
             int(walkers_per_block), _stream_ptr(stream)))
+
+    def basin(self, X, state, precision, n_steps, sigma, seed, step_base, acc_sum=None,
+              stream=None):
+        self._check(self.lib.oqmc_basin(
+            self._h, _dptr(X), X.shape[0], _dptr(state), int(precision), int(n_steps),
+            float(sigma), ctypes.c_uint64(seed & (2**64 - 1)), ctypes.c_uint64(step_base),
+            _dptr(acc_sum), _stream_ptr(stream)))
 
     def set_split(self, tight_alpha):
         self._check(self.lib.oqmc_set_split(self._h, float(tight_alpha)))

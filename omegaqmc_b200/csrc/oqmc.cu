@@ -274,43 +274,104 @@ int oqmc_log_psi(oqmc_ctx* ctx, const double* X, int W, double* logpsi, void* st
   return OQ_OK;
 }
 
-static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
-
-size_t oqmc_state_bytes(const oqmc_ctx* ctx, int W, int precision) {
-  if (!ctx || W < 0) return 0;
-  const size_t rs = precision == OQ_PREC_MIXED ? sizeof(float) : sizeof(double);
-  return align256((size_t)2 * ctx->nocc * ctx->nocc * W * rs) + align256((size_t)W * sizeof(double));
-}
-
-static void state_ptrs(const oqmc_ctx* ctx, void* state, int W, int precision, void** ainv,
-                       double** logdet) {
-  const size_t rs = precision == OQ_PREC_MIXED ? sizeof(float) : sizeof(double);
-  *ainv = state;
-  *logdet = reinterpret_cast<double*>(static_cast<char*>(state) +
-                                      align256((size_t)2 * ctx->nocc * ctx->nocc * W * rs));
-}
-
-int oqmc_refresh(oqmc_ctx* ctx, const double* X, int W, void* state, int precision,
-                 void* stream) {
+int oqmc_mo_values(oqmc_ctx* ctx, const double* X, int W, double* out, void* stream) {
   if (!ctx) return OQ_ERR_ARG;
-  if (W < 0 || (W > 0 && (!X || !state)) || (precision != OQ_PREC_FP64 && precision != OQ_PREC_MIXED))
-    return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
+  if (W < 0 || (W > 0 && (!X || !out))) return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
   if (W == 0) return OQ_OK;
-  void* ainv;
-  double* logdet;
-  state_ptrs(ctx, state, W, precision, &ainv, &logdet);
   const OqLaunch L = make_launch(ctx, stream, smem_sys_c64(ctx));
-  const int mixed = precision == OQ_PREC_MIXED;
   cudaError_t err = cudaSuccess;
-#define OQ_X(N) err = oq_refresh_##N(L, X, W, ainv, logdet, mixed)
+#define OQ_X(N) err = oq_movals_##N(L, X, W, out)
   OQ_SWITCH(ctx->nocc, OQ_X)
 #undef OQ_X
   OQ_CUDA(ctx, err);
   return OQ_OK;
 }
 
-static size_t sweep_smem(const oqmc_ctx* ctx, int wpb, int precision) {
-  const size_t rs = precision == OQ_PREC_MIXED ? sizeof(float) : sizeof(double);
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// Sampler state: [pos SoA 3*n_e*W doubles][ainv 2*nocc^2*W Real][logdet W doubles]
+struct OqStatePtrs {
+  double* pos;
+  void* ainv;
+  double* logdet;
+};
+
+static size_t real_size(int precision) {
+  return precision == OQ_PREC_MIXED ? sizeof(float) : sizeof(double);
+}
+
+size_t oqmc_state_bytes(const oqmc_ctx* ctx, int W, int precision) {
+  if (!ctx || W < 0) return 0;
+  return align256((size_t)3 * ctx->n_e * W * sizeof(double)) +
+         align256((size_t)2 * ctx->nocc * ctx->nocc * W * real_size(precision)) +
+         align256((size_t)W * sizeof(double));
+}
+
+static OqStatePtrs state_ptrs(const oqmc_ctx* ctx, void* state, int W, int precision) {
+  OqStatePtrs p;
+  char* b = static_cast<char*>(state);
+  p.pos = reinterpret_cast<double*>(b);
+  b += align256((size_t)3 * ctx->n_e * W * sizeof(double));
+  p.ainv = b;
+  b += align256((size_t)2 * ctx->nocc * ctx->nocc * W * real_size(precision));
+  p.logdet = reinterpret_cast<double*>(b);
+  return p;
+}
+
+// (W, n3) row-major <-> [n3][W]
+__global__ void k_aos_to_soa(const double* __restrict__ X, double* __restrict__ pos, int W,
+                             int n3) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)W * n3) return;
+  const int w = (int)(t / n3), k = (int)(t % n3);
+  pos[(size_t)k * W + w] = X[t];
+}
+
+__global__ void k_soa_to_aos(const double* __restrict__ pos, double* __restrict__ X, int W,
+                             int n3) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)W * n3) return;
+  const int w = (int)(t / n3), k = (int)(t % n3);
+  X[t] = pos[(size_t)k * W + w];
+}
+
+static cudaError_t to_soa(const oqmc_ctx* ctx, const double* X, double* pos, int W,
+                          cudaStream_t s) {
+  const long long n = (long long)W * 3 * ctx->n_e;
+  k_aos_to_soa<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(X, pos, W, 3 * ctx->n_e);
+  return cudaGetLastError();
+}
+
+static cudaError_t to_aos(const oqmc_ctx* ctx, const double* pos, double* X, int W,
+                          cudaStream_t s) {
+  const long long n = (long long)W * 3 * ctx->n_e;
+  k_soa_to_aos<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pos, X, W, 3 * ctx->n_e);
+  return cudaGetLastError();
+}
+
+static bool valid_prec(int p) { return p == OQ_PREC_FP64 || p == OQ_PREC_MIXED; }
+
+int oqmc_refresh(oqmc_ctx* ctx, const double* X, int W, void* state, int precision,
+                 void* stream) {
+  if (!ctx) return OQ_ERR_ARG;
+  if (W < 0 || (W > 0 && (!X || !state)) || !valid_prec(precision))
+    return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
+  if (W == 0) return OQ_OK;
+  const OqStatePtrs st = state_ptrs(ctx, state, W, precision);
+  cudaStream_t s = (cudaStream_t)stream;
+  OQ_CUDA(ctx, to_soa(ctx, X, st.pos, W, s));
+  const OqLaunch L = make_launch(ctx, stream, smem_sys_c64(ctx));
+  const int mixed = precision == OQ_PREC_MIXED;
+  cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_refresh_##N(L, st.pos, W, st.ainv, st.logdet, mixed)
+  OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+  OQ_CUDA(ctx, err);
+  return OQ_OK;
+}
+
+static size_t moves_smem(const oqmc_ctx* ctx, int wpb, int precision) {
+  const size_t rs = real_size(precision);
   size_t b = sizeof(OqSystem) + sizeof(OqSplit);
   b += ((size_t)ctx->nbf * ctx->nocc * rs + 15) & ~(size_t)15;
   b += (size_t)3 * ctx->n_e * wpb * sizeof(double);
@@ -318,38 +379,113 @@ static size_t sweep_smem(const oqmc_ctx* ctx, int wpb, int precision) {
   return b;
 }
 
+static size_t eloc_smem(const oqmc_ctx* ctx, int precision) {
+  size_t b = sizeof(OqSystem) + sizeof(OqSplit);
+  b += ((size_t)ctx->nbf * ctx->nocc * real_size(precision) + 15) & ~(size_t)15;
+  b += (size_t)ctx->n_e * 4 * 32 * sizeof(double);
+  return b;
+}
+
+static int pick_wpb(oqmc_ctx* ctx, int wpb, int precision, size_t* sm) {
+  if (wpb == 0) wpb = 128;
+  if (wpb != 32 && wpb != 64 && wpb != 128) return -1;
+  *sm = moves_smem(ctx, wpb, precision);
+  while (*sm > 227 * 1024 && wpb > 32) { wpb /= 2; *sm = moves_smem(ctx, wpb, precision); }
+  if (*sm > 227 * 1024) return -2;
+  return wpb;
+}
+
+static int launch_moves(oqmc_ctx* ctx, const OqMoveArgs& m, int wpb, size_t sm, int precision,
+                        void* stream) {
+  const OqLaunch L = make_launch(ctx, stream, sm);
+  const int mixed = precision == OQ_PREC_MIXED;
+  cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_moves_##N(L, m, wpb, mixed)
+  OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+  OQ_CUDA(ctx, err);
+  return OQ_OK;
+}
+
 int oqmc_sweeps(oqmc_ctx* ctx, double* X, int W, void* state, int precision, int n_sweeps,
                 int measure_every, double step, uint64_t seed, uint64_t step_base,
                 double* sums, double* el_trace, double* eparts_last, int wpb,
                 void* stream) {
   if (!ctx) return OQ_ERR_ARG;
-  if (W < 0 || n_sweeps < 0 || measure_every < 1 || !(step > 0.0) ||
-      (precision != OQ_PREC_FP64 && precision != OQ_PREC_MIXED))
+  if (W < 0 || n_sweeps < 0 || measure_every < 1 || !(step > 0.0) || !valid_prec(precision))
     return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
   if (W == 0 || n_sweeps == 0) return OQ_OK;
   if (!X || !state || (n_sweeps >= measure_every && !sums))
     return set_err(ctx, OQ_ERR_ARG, "null buffer%s");
-  if (wpb == 0) wpb = 128;
-  if (wpb != 32 && wpb != 64 && wpb != 128)
-    return set_err(ctx, OQ_ERR_ARG, "walkers_per_block must be 32, 64 or 128%s");
-  size_t sm = sweep_smem(ctx, wpb, precision);
-  while (sm > 227 * 1024 && wpb > 32) { wpb /= 2; sm = sweep_smem(ctx, wpb, precision); }
-  if (sm > 227 * 1024)
-    return set_err(ctx, OQ_ERR_UNSUPPORTED, "system too large for the shared-memory sweep kernel%s");
-  OqSweepArgs a;
-  memset(&a, 0, sizeof(a));
-  double* logdet;
-  state_ptrs(ctx, state, W, precision, &a.ainv, &logdet);
-  a.X = X; a.logdet = logdet; a.W = W; a.n_sweeps = n_sweeps; a.measure_every = measure_every;
-  a.step = step; a.seed = seed; a.step_base = step_base; a.sums = sums;
-  a.el_trace = el_trace; a.eparts_last = eparts_last; a.flags = ctx->d_flags;
-  const OqLaunch L = make_launch(ctx, stream, sm);
+  size_t sm;
+  wpb = pick_wpb(ctx, wpb, precision, &sm);
+  if (wpb == -1) return set_err(ctx, OQ_ERR_ARG, "walkers_per_block must be 32, 64 or 128%s");
+  if (wpb < 0)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED, "system too large for the shared-memory move kernel%s");
+  cudaStream_t s = (cudaStream_t)stream;
+  const OqStatePtrs st = state_ptrs(ctx, state, W, precision);
+  OQ_CUDA(ctx, to_soa(ctx, X, st.pos, W, s));
+  OqMoveArgs m;
+  memset(&m, 0, sizeof(m));
+  m.pos = st.pos; m.ainv = st.ainv; m.logdet = st.logdet; m.W = W; m.mode = 0;
+  m.step = step; m.seed = seed; m.flags = ctx->d_flags;
+  OqElocArgs el;
+  memset(&el, 0, sizeof(el));
+  el.pos = st.pos; el.ainv = st.ainv; el.W = W; el.flags = ctx->d_flags;
+  const OqLaunch Le = make_launch(ctx, stream, eloc_smem(ctx, precision));
   const int mixed = precision == OQ_PREC_MIXED;
-  cudaError_t err = cudaSuccess;
-#define OQ_X(N) err = oq_sweeps_##N(L, a, wpb, mixed)
-  OQ_SWITCH(ctx->nocc, OQ_X)
+  const int n_meas = n_sweeps / measure_every;
+  int done = 0;
+  for (int k = 0; k < n_meas; ++k) {
+    m.n_steps = measure_every;
+    m.step_base = step_base + done;
+    m.acc_sum = sums + (size_t)k * OQ_NSUM + 5;
+    int rc = launch_moves(ctx, m, wpb, sm, precision, stream);
+    if (rc != OQ_OK) return rc;
+    done += measure_every;
+    el.sums = sums + (size_t)k * OQ_NSUM;
+    el.el_trace = el_trace ? el_trace + (size_t)k * W : nullptr;
+    el.eparts = (k == n_meas - 1) ? eparts_last : nullptr;
+    cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_eloc_##N(Le, el, mixed)
+    OQ_SWITCH(ctx->nocc, OQ_X)
 #undef OQ_X
-  OQ_CUDA(ctx, err);
+    OQ_CUDA(ctx, err);
+  }
+  if (done < n_sweeps) {
+    m.n_steps = n_sweeps - done;
+    m.step_base = step_base + done;
+    m.acc_sum = nullptr;
+    int rc = launch_moves(ctx, m, wpb, sm, precision, stream);
+    if (rc != OQ_OK) return rc;
+  }
+  OQ_CUDA(ctx, to_aos(ctx, st.pos, X, W, s));
+  return OQ_OK;
+}
+
+int oqmc_basin(oqmc_ctx* ctx, double* X, int W, void* state, int precision, int n_steps,
+               double sigma, uint64_t seed, uint64_t step_base, double* acc_sum,
+               void* stream) {
+  if (!ctx) return OQ_ERR_ARG;
+  if (W < 0 || n_steps < 0 || !(sigma > 0.0) || !valid_prec(precision))
+    return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
+  if (W == 0 || n_steps == 0) return OQ_OK;
+  if (!X || !state) return set_err(ctx, OQ_ERR_ARG, "null buffer%s");
+  size_t sm;
+  const int wpb = pick_wpb(ctx, 0, precision, &sm);
+  if (wpb < 0)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED, "system too large for the shared-memory move kernel%s");
+  cudaStream_t s = (cudaStream_t)stream;
+  const OqStatePtrs st = state_ptrs(ctx, state, W, precision);
+  OQ_CUDA(ctx, to_soa(ctx, X, st.pos, W, s));
+  OqMoveArgs m;
+  memset(&m, 0, sizeof(m));
+  m.pos = st.pos; m.ainv = st.ainv; m.logdet = st.logdet; m.W = W; m.mode = 1;
+  m.n_steps = n_steps; m.step = sigma; m.seed = seed; m.step_base = step_base;
+  m.acc_sum = acc_sum; m.flags = ctx->d_flags;
+  int rc = launch_moves(ctx, m, wpb, sm, precision, stream);
+  if (rc != OQ_OK) return rc;
+  OQ_CUDA(ctx, to_aos(ctx, st.pos, X, W, s));
   return OQ_OK;
 }
 

@@ -115,16 +115,38 @@ __device__ __forceinline__ void oq_move_randoms(uint64_t seed, uint32_t walker,
   OqU4 r0 = oq_philox(c0, (uint32_t)seed, (uint32_t)(seed >> 32));
   OqU4 c1 = {walker, step, elec, 1u};
   OqU4 r1 = oq_philox(c1, (uint32_t)seed, (uint32_t)(seed >> 32));
-  double a = sqrt(-2.0 * log(oq_u01(r0.x)));
-  double s, c;
-  sincospi(2.0 * oq_u01(r0.y), &s, &c);
-  double b = sqrt(-2.0 * log(oq_u01(r0.z)));
-  double s2, c2;
-  sincospi(2.0 * oq_u01(r0.w), &s2, &c2);
-  n3[0] = a * c;
-  n3[1] = a * s;
-  n3[2] = b * c2;
-  u = oq_u01(r1.x) - 2.3283064365386963e-10;   // in [0, 1)
+  // Box-Muller in FP32: the deviates only set proposal widths, 24-bit
+  // resolution is ample and the FP32 transcendental units are cheap
+  const float k32 = 2.3283064365386963e-10f;
+  const float a = sqrtf(-2.0f * __logf(((float)r0.x + 1.0f) * k32));
+  const float b = sqrtf(-2.0f * __logf(((float)r0.z + 1.0f) * k32));
+  float s, c, s2, c2;
+  __sincosf(6.283185307179586f * ((float)r0.y * k32), &s, &c);
+  __sincosf(6.283185307179586f * ((float)r0.w * k32), &s2, &c2);
+  n3[0] = (double)(a * c);
+  n3[1] = (double)(a * s);
+  n3[2] = (double)(b * c2);
+  u = (double)r1.x * 2.3283064365386963e-10;   // in [0, 1)
+}
+
+// reciprocal / reciprocal square root in the working precision
+__device__ __forceinline__ double oq_rcp(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float oq_rcp(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double oq_rsqrt(double x) { return rsqrt(x); }
+__device__ __forceinline__ float oq_rsqrt(float x) { return rsqrtf(x); }
+
+// Padé u = a r / (1 + b r) from r and 1/r with one reciprocal:
+// q = 1/(1+br), u = a r q, u'/r = a q^2 / r, u'' + 2u'/r = -2ab q^3 + 2u'/r
+template <typename T>
+__device__ __forceinline__ T oq_pade_q(T a, T b, T r) {
+  return a * r * oq_rcp((T)1 + b * r);
+}
+template <typename T>
+__device__ __forceinline__ void oq_pade_vgl_q(T a, T b, T r, T rinv, T& up_r, T& lap) {
+  const T q = oq_rcp((T)1 + b * r);
+  const T aq2 = a * q * q;
+  up_r = aq2 * rinv;
+  lap = (T)-2 * b * aq2 * q + (T)2 * up_r;
 }
 
 // ---------------------------------------------------------------------------

@@ -215,3 +215,24 @@ k_logpsi(const OqSystem* __restrict__ gsys, const double* __restrict__ gC,
   logpsi[w] = ok ? l : -INFINITY;
   if (!ok) atomicOr(flags, OQ_FLAG_SINGULAR);
 }
+
+// Occupied MO values per (walker, electron): out[(w*n_e + e)*NOCC + m]
+// (get_psi_mo, OmegaQMC/psi/gto.py:1058-1070).  One thread per electron.
+template <int NOCC>
+__global__ void __launch_bounds__(128)
+k_mo_values(const OqSystem* __restrict__ gsys, const double* __restrict__ gC,
+            const double* __restrict__ X, int W, double* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  OqSystem& S = *reinterpret_cast<OqSystem*>(smem);
+  double* C = reinterpret_cast<double*>(smem + sizeof(OqSystem));
+  oq_load_system(&S, gsys);
+  for (int i = threadIdx.x; i < S.nbf * NOCC; i += blockDim.x) C[i] = gC[i];
+  __syncthreads();
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)W * 2 * NOCC) return;
+  const double* xp = X + 3 * t;
+  double mv[NOCC];
+  oq_mo_val<NOCC>(S, C, xp[0], xp[1], xp[2], mv);
+#pragma unroll
+  for (int m = 0; m < NOCC; ++m) out[t * NOCC + m] = mv[m];
+}

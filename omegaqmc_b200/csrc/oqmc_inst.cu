@@ -10,8 +10,13 @@
 #define OQ_CAT(a, b) OQ_CAT2(a, b)
 #define OQ_FN(name) OQ_CAT(name, OQ_N)
 
+// Dynamic shared memory above 48 KB needs an opt-in; every kernel also asks
+// for the largest shared-memory carveout so several CTAs fit per SM.
 template <typename K>
 static cudaError_t oq_smem_attr(K kernel, size_t smem) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
   if (smem > 48 * 1024)
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   return cudaSuccess;
@@ -35,35 +40,61 @@ cudaError_t OQ_FN(oq_logpsi)(const OqLaunch& L, const double* X, int W, double* 
   return cudaGetLastError();
 }
 
-cudaError_t OQ_FN(oq_refresh)(const OqLaunch& L, const double* X, int W, void* ainv,
+cudaError_t OQ_FN(oq_movals)(const OqLaunch& L, const double* X, int W, double* out) {
+  const int tpb = 128;
+  const long long n = (long long)W * 2 * OQ_N;
+  const int nb = (int)((n + tpb - 1) / tpb);
+  cudaError_t e = oq_smem_attr(k_mo_values<OQ_N>, L.smem);
+  if (e != cudaSuccess) return e;
+  k_mo_values<OQ_N><<<nb, tpb, L.smem, L.stream>>>(L.sys, L.C64, X, W, out);
+  return cudaGetLastError();
+}
+
+cudaError_t OQ_FN(oq_refresh)(const OqLaunch& L, const double* pos, int W, void* ainv,
                               double* logdet, int mixed) {
   const int tpb = 128, nb = (W + tpb - 1) / tpb;
   cudaError_t e;
   if (mixed) {
     e = oq_smem_attr(k_refresh<OQ_N, float>, L.smem);
     if (e != cudaSuccess) return e;
-    k_refresh<OQ_N, float><<<nb, tpb, L.smem, L.stream>>>(L.sys, L.C64, X, W, (float*)ainv,
+    k_refresh<OQ_N, float><<<nb, tpb, L.smem, L.stream>>>(L.sys, L.C64, pos, W, (float*)ainv,
                                                            logdet, L.flags);
   } else {
     e = oq_smem_attr(k_refresh<OQ_N, double>, L.smem);
     if (e != cudaSuccess) return e;
-    k_refresh<OQ_N, double><<<nb, tpb, L.smem, L.stream>>>(L.sys, L.C64, X, W, (double*)ainv,
-                                                            logdet, L.flags);
+    k_refresh<OQ_N, double><<<nb, tpb, L.smem, L.stream>>>(L.sys, L.C64, pos, W,
+                                                            (double*)ainv, logdet, L.flags);
   }
   return cudaGetLastError();
 }
 
-cudaError_t OQ_FN(oq_sweeps)(const OqLaunch& L, const OqSweepArgs& a, int wpb, int mixed) {
+cudaError_t OQ_FN(oq_moves)(const OqLaunch& L, const OqMoveArgs& a, int wpb, int mixed) {
   const int nb = (a.W + wpb - 1) / wpb;
   cudaError_t e;
   if (mixed) {
-    e = oq_smem_attr(k_sweeps<OQ_N, float, float>, L.smem);
+    e = oq_smem_attr(k_moves<OQ_N, float, float>, L.smem);
     if (e != cudaSuccess) return e;
-    k_sweeps<OQ_N, float, float><<<nb, wpb, L.smem, L.stream>>>(L.sys, L.split, L.C32, a);
+    k_moves<OQ_N, float, float><<<nb, wpb, L.smem, L.stream>>>(L.sys, L.split, L.C32, a);
   } else {
-    e = oq_smem_attr(k_sweeps<OQ_N, double, double>, L.smem);
+    e = oq_smem_attr(k_moves<OQ_N, double, double>, L.smem);
     if (e != cudaSuccess) return e;
-    k_sweeps<OQ_N, double, double><<<nb, wpb, L.smem, L.stream>>>(L.sys, L.split, L.C64, a);
+    k_moves<OQ_N, double, double><<<nb, wpb, L.smem, L.stream>>>(L.sys, L.split, L.C64, a);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t OQ_FN(oq_eloc)(const OqLaunch& L, const OqElocArgs& a, int mixed) {
+  const int nb = (a.W + 31) / 32;
+  const dim3 block(32, 2 * OQ_N);
+  cudaError_t e;
+  if (mixed) {
+    e = oq_smem_attr(k_eloc<OQ_N, float, float>, L.smem);
+    if (e != cudaSuccess) return e;
+    k_eloc<OQ_N, float, float><<<nb, block, L.smem, L.stream>>>(L.sys, L.split, L.C32, a);
+  } else {
+    e = oq_smem_attr(k_eloc<OQ_N, double, double>, L.smem);
+    if (e != cudaSuccess) return e;
+    k_eloc<OQ_N, double, double><<<nb, block, L.smem, L.stream>>>(L.sys, L.split, L.C64, a);
   }
   return cudaGetLastError();
 }

@@ -19,9 +19,11 @@ struct OqLaunch {
   cudaError_t oq_eval_##N(const OqLaunch& L, const double* X, int W, double* logpsi,  \
                           double* grad, double* lap, double* eparts);                 \
   cudaError_t oq_logpsi_##N(const OqLaunch& L, const double* X, int W, double* logpsi); \
-  cudaError_t oq_refresh_##N(const OqLaunch& L, const double* X, int W, void* ainv,   \
+  cudaError_t oq_movals_##N(const OqLaunch& L, const double* X, int W, double* out);  \
+  cudaError_t oq_refresh_##N(const OqLaunch& L, const double* pos, int W, void* ainv, \
                              double* logdet, int mixed);                              \
-  cudaError_t oq_sweeps_##N(const OqLaunch& L, const OqSweepArgs& a, int wpb, int mixed);
+  cudaError_t oq_moves_##N(const OqLaunch& L, const OqMoveArgs& a, int wpb, int mixed); \
+  cudaError_t oq_eloc_##N(const OqLaunch& L, const OqElocArgs& a, int mixed);
 
 #define OQ_NOCC_LIST(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(10) X(12) X(14) X(16)
 

@@ -201,13 +201,19 @@ __device__ __forceinline__ void oq_mo_vgl_t(const OqSystem& S, const OqSplit& SP
 }
 
 // ---------------------------------------------------------------------------
-// Refresh: FP64 Slater matrices from positions, Gauss-Jordan inverse,
-// stored as Real in the walker-minor state layout ainv[(s*N+m)*N+j][W].
+// Sampler state in global memory, walker-minor so consecutive threads
+// (walkers) touch consecutive words:
+//   pos    [3*NE][W] double        positions, pos[(3e+c)*W + w]
+//   ainv   [2*N*N][W] Real         ainv[((s*N + m)*N + j)*W + w] = (S_s^-1)[m][j]
+//   logdet [W] double              log|det up| + log|det down|
 // ---------------------------------------------------------------------------
+
+// Refresh: FP64 Slater matrices from positions, Gauss-Jordan inverse,
+// stored as Real.  One thread per walker.
 template <int NOCC, typename Real>
 __global__ void __launch_bounds__(128)
 k_refresh(const OqSystem* __restrict__ gsys, const double* __restrict__ gC,
-          const double* __restrict__ X, int W, Real* __restrict__ ainv,
+          const double* __restrict__ pos, int W, Real* __restrict__ ainv,
           double* __restrict__ logdet, unsigned* __restrict__ flags) {
   extern __shared__ __align__(16) unsigned char smem[];
   OqSystem& S = *reinterpret_cast<OqSystem*>(smem);
@@ -217,16 +223,15 @@ k_refresh(const OqSystem* __restrict__ gsys, const double* __restrict__ gC,
   __syncthreads();
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= W) return;
-  constexpr int NE = 2 * NOCC;
   double ld_tot = 0.0;
   bool ok = true;
   for (int s = 0; s < 2; ++s) {
     double Sm[NOCC][NOCC], Ai[NOCC][NOCC];
     for (int i = 0; i < NOCC; ++i) {
       const int e = 2 * i + s;
-      const double* xp = X + (size_t)w * 3 * NE + 3 * e;
       double mv[NOCC];
-      oq_mo_val<NOCC>(S, C, xp[0], xp[1], xp[2], mv);
+      oq_mo_val<NOCC>(S, C, pos[(size_t)(3 * e) * W + w], pos[(size_t)(3 * e + 1) * W + w],
+                      pos[(size_t)(3 * e + 2) * W + w], mv);
 #pragma unroll
       for (int m = 0; m < NOCC; ++m) Sm[i][m] = mv[m];
     }
@@ -243,29 +248,124 @@ k_refresh(const OqSystem* __restrict__ gsys, const double* __restrict__ gC,
 }
 
 // number of doubles reduced per measured sweep
-#define OQ_NSUM 8   // ee, en, ke, eloc, eloc^2, accepted moves, valid walkers, pad
+#define OQ_NSUM 8   // ee, en, ke, eloc, eloc^2, accepted moves, finite walkers, pad
 
-struct OqSweepArgs {
-  double* X;              // (W, n_e, 3) positions, in/out
-  void* ainv;             // Real, walker-minor inverse state
-  double* logdet;         // (W,) log|det up| + log|det down|
+struct OqMoveArgs {
+  double* pos;            // state positions (SoA)
+  void* ainv;             // state inverses (Real, SoA)
+  double* logdet;
   int W;
-  int n_sweeps;
-  int measure_every;      // local energy after every k-th sweep (k >= 1)
+  int n_steps;            // sweeps (mode 0) or basin relocations (mode 1)
+  int mode;               // 0: Gaussian single-electron sweeps; 1: basin relocation
   int pad;
-  double step;
+  double step;            // Gaussian width (mode 0) or blob width sigma (mode 1)
   uint64_t seed;
-  uint64_t step_base;     // global sweep counter of the first sweep (RNG)
-  double* sums;           // (n_meas, OQ_NSUM), accumulated with atomics
-  double* el_trace;       // (n_meas, W) local energies or null
-  double* eparts_last;    // (W, 4) ee, en, ke, eloc of the last measurement or null
+  uint64_t step_base;     // RNG counter of the first step
+  double* acc_sum;        // += accepted moves (may be null)
   unsigned* flags;
 };
 
+// One single-electron Metropolis move of electron e to (nx, ny, nz) against
+// shared-memory state; log_extra is the log proposal-density ratio
+// log q(old)/q(new) (0 for symmetric proposals).  Returns acceptance.
+template <int NOCC, typename T, typename Real>
+__device__ __forceinline__ bool oq_try_move(const OqSystem& S, const OqSplit& SP,
+                                            const Real* __restrict__ C, double* pos,
+                                            Real* Ai, int WPB, int tid, int e,
+                                            double nx, double ny, double nz,
+                                            double log_extra, double u, double& logdet) {
+  constexpr int NE = 2 * NOCC;
+  constexpr int NN = NOCC * NOCC;
+  const int s = e & 1, i = e >> 1;
+  const double thr2 = 1e-4 * 1e-4;
+  const double ox = pos[(3 * e) * WPB + tid], oy = pos[(3 * e + 1) * WPB + tid],
+               oz = pos[(3 * e + 2) * WPB + tid];
+  // Jastrow change (arithmetic in T) and the MIN_DIST_THRESHOLD test (FP64)
+  T dJ = (T)0;
+  bool valid = true;
+  for (int j = 0; j < NE; ++j) {
+    if (j == e) continue;
+    const double xj = pos[(3 * j) * WPB + tid], yj = pos[(3 * j + 1) * WPB + tid],
+                 zj = pos[(3 * j + 2) * WPB + tid];
+    const double ax = nx - xj, ay = ny - yj, az = nz - zj;
+    const double rn2 = ax * ax + ay * ay + az * az;
+    valid = valid && (rn2 >= thr2);
+    if (S.has_j2) {
+      const double bx = ox - xj, by = oy - yj, bz = oz - zj;
+      const T rn2t = (T)rn2, ro2t = (T)(bx * bx + by * by + bz * bz);
+      const int o = ((e & 1) == (j & 1)) ? 0 : 2;
+      const T pa = (T)S.j2[o], pb = (T)S.j2[o + 1];
+      dJ += oq_pade_q(pa, pb, rn2t * oq_rsqrt(rn2t)) - oq_pade_q(pa, pb, ro2t * oq_rsqrt(ro2t));
+    }
+  }
+  for (int I = 0; I < S.natm; ++I) {
+    const double ax = nx - S.nuc[I][0], ay = ny - S.nuc[I][1], az = nz - S.nuc[I][2];
+    const double rn2 = ax * ax + ay * ay + az * az;
+    valid = valid && (rn2 >= thr2);
+    if (S.has_j1) {
+      const double bx = ox - S.nuc[I][0], by = oy - S.nuc[I][1], bz = oz - S.nuc[I][2];
+      const T rn2t = (T)rn2, ro2t = (T)(bx * bx + by * by + bz * bz);
+      const T pa = (T)S.j1a[I], pb = (T)S.j1b[I];
+      dJ += oq_pade_q(pa, pb, rn2t * oq_rsqrt(rn2t)) - oq_pade_q(pa, pb, ro2t * oq_rsqrt(ro2t));
+    }
+  }
+  // new MO row and the ratio vector w_j = sum_m v_m A[m][j]; R = w_i
+  T v[NOCC];
+  oq_mo_val_t<NOCC, T, Real>(S, SP, C, nx, ny, nz, v);
+  Real* As = Ai + (size_t)s * NN * WPB;
+  T wv[NOCC];
+#pragma unroll
+  for (int j = 0; j < NOCC; ++j) {
+    T acc = (T)0;
+#pragma unroll
+    for (int m = 0; m < NOCC; ++m) acc += v[m] * (T)As[(m * NOCC + j) * WPB + tid];
+    wv[j] = acc;
+  }
+  T R = (T)0;
+#pragma unroll
+  for (int j = 0; j < NOCC; ++j) R = (j == i) ? wv[j] : R;
+  const double Rd = (double)R;
+  const double logp = 2.0 * log(fabs(Rd)) + 2.0 * (double)dJ + log_extra;
+  const bool acc = valid && (Rd != 0.0) && isfinite(logp) && (log(u) < logp);
+  if (acc) {
+    // Sherman-Morrison: A[k][j] -= A[k][i] (w_j - delta_ij) / R
+    const T rinv = (T)1 / R;
+    T coli[NOCC];
+#pragma unroll
+    for (int k = 0; k < NOCC; ++k) {
+      T c = (T)0;
+#pragma unroll
+      for (int j = 0; j < NOCC; ++j) c = (j == i) ? (T)As[(k * NOCC + j) * WPB + tid] : c;
+      coli[k] = c;
+    }
+#pragma unroll
+    for (int j = 0; j < NOCC; ++j) {
+      const T f = (wv[j] - (j == i ? (T)1 : (T)0)) * rinv;
+#pragma unroll
+      for (int k = 0; k < NOCC; ++k) {
+        Real& ref = As[(k * NOCC + j) * WPB + tid];
+        ref = (Real)((T)ref - coli[k] * f);
+      }
+    }
+    pos[(3 * e) * WPB + tid] = nx;
+    pos[(3 * e + 1) * WPB + tid] = ny;
+    pos[(3 * e + 2) * WPB + tid] = nz;
+    logdet += log(fabs(Rd));
+  }
+  return acc;
+}
+
+// Metropolis moves, one thread per walker, state resident in shared memory
+// for the whole launch.  mode 0: n_steps sweeps over all electrons with
+// Gaussian proposals (metropolis_move_1w, OmegaQMC/vmc_gto.py:841-905, as
+// single-electron moves).  mode 1: n_steps basin relocations: one random
+// electron proposed at N(R_J, sigma^2) around a random nucleus J, accepted
+// with the exact proposal ratio q(old)/q(new), q(x) = sum_J
+// exp(-|x-R_J|^2 / 2 sigma^2) (basin_move_1w, vmc_gto.py:925-957).
 template <int NOCC, typename T, typename Real>
 __global__ void __launch_bounds__(128)
-k_sweeps(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
-         const void* __restrict__ gC, OqSweepArgs a) {
+k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
+        const void* __restrict__ gC, OqMoveArgs a) {
   constexpr int NE = 2 * NOCC;
   constexpr int NN = NOCC * NOCC;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -292,186 +392,202 @@ k_sweeps(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
   const int w = blockIdx.x * WPB + tid;
   const bool live = w < a.W;
   const int W = a.W;
-  const Real* gA = reinterpret_cast<const Real*>(a.ainv);
+  Real* gA = reinterpret_cast<Real*>(a.ainv);
   if (live) {
-    for (int k = 0; k < 3 * NE; ++k) pos[k * WPB + tid] = a.X[(size_t)w * 3 * NE + k];
+    for (int k = 0; k < 3 * NE; ++k) pos[k * WPB + tid] = a.pos[(size_t)k * W + w];
     for (int k = 0; k < 2 * NN; ++k) Ai[k * WPB + tid] = gA[(size_t)k * W + w];
   }
   __syncthreads();
   double logdet = live ? a.logdet[w] : 0.0;
-  unsigned bad = 0;
-  const double thr2 = 1e-4 * 1e-4;
-  int meas = 0;
-
-  for (int sweep = 0; sweep < a.n_sweeps; ++sweep) {
-    int nacc = 0;
-    if (live) {
-      const uint32_t gstep = (uint32_t)(a.step_base + sweep);
+  int nacc = 0;
+  for (int t = 0; t < (live ? a.n_steps : 0); ++t) {
+    const uint32_t gstep = (uint32_t)(a.step_base + t);
+    if (a.mode == 0) {
       for (int e = 0; e < NE; ++e) {
-        const int s = e & 1, i = e >> 1;
         double n3[3], u;
         oq_move_randoms(a.seed, (uint32_t)w, gstep, (uint32_t)e, n3, u);
-        const double ox = pos[(3 * e) * WPB + tid], oy = pos[(3 * e + 1) * WPB + tid],
-                     oz = pos[(3 * e + 2) * WPB + tid];
-        const double nx = ox + a.step * n3[0], ny = oy + a.step * n3[1],
-                     nz = oz + a.step * n3[2];
-        // Jastrow change and singularity check
-        double dJ = 0.0;
-        bool valid = true;
-        for (int j = 0; j < NE; ++j) {
-          if (j == e) continue;
-          const double xj = pos[(3 * j) * WPB + tid], yj = pos[(3 * j + 1) * WPB + tid],
-                       zj = pos[(3 * j + 2) * WPB + tid];
-          const double ax = nx - xj, ay = ny - yj, az = nz - zj;
-          const double bx = ox - xj, by = oy - yj, bz = oz - zj;
-          const double rn2 = ax * ax + ay * ay + az * az;
-          valid = valid && (rn2 >= thr2);
-          if (S.has_j2) {
-            const int o = ((e & 1) == (j & 1)) ? 0 : 2;
-            dJ += oq_pade(S.j2[o], S.j2[o + 1], sqrt(rn2)) -
-                  oq_pade(S.j2[o], S.j2[o + 1], sqrt(bx * bx + by * by + bz * bz));
-          }
-        }
-        for (int I = 0; I < S.natm; ++I) {
-          const double ax = nx - S.nuc[I][0], ay = ny - S.nuc[I][1], az = nz - S.nuc[I][2];
-          const double rn2 = ax * ax + ay * ay + az * az;
-          valid = valid && (rn2 >= thr2);
-          if (S.has_j1) {
-            const double bx = ox - S.nuc[I][0], by = oy - S.nuc[I][1], bz = oz - S.nuc[I][2];
-            dJ += oq_pade(S.j1a[I], S.j1b[I], sqrt(rn2)) -
-                  oq_pade(S.j1a[I], S.j1b[I], sqrt(bx * bx + by * by + bz * bz));
-          }
-        }
-        // new MO row and determinant ratio against column i of the inverse
-        T v[NOCC];
-        oq_mo_val_t<NOCC, T, Real>(S, SP, C, nx, ny, nz, v);
-        const Real* As = Ai + (size_t)s * NN * WPB;
-        T wv[NOCC];
-#pragma unroll
-        for (int j = 0; j < NOCC; ++j) {
-          T acc = (T)0;
-#pragma unroll
-          for (int m = 0; m < NOCC; ++m) acc += v[m] * (T)As[(m * NOCC + j) * WPB + tid];
-          wv[j] = acc;
-        }
-        T R = (T)0;
-#pragma unroll
-        for (int j = 0; j < NOCC; ++j) R = (j == i) ? wv[j] : R;
-        const double Rd = (double)R;
-        const double prob = Rd * Rd * exp(2.0 * dJ);
-        const bool acc = valid && (u < prob) && (Rd != 0.0) && isfinite(prob);
-        if (acc) {
-          // Sherman-Morrison: A[k][j] -= A[k][i] (w_j - delta_ij) / R
-          const T rinv = (T)1 / R;
-          T coli[NOCC];
-          Real* Aw = Ai + (size_t)s * NN * WPB;
-#pragma unroll
-          for (int k = 0; k < NOCC; ++k) {
-            T c = (T)0;
-#pragma unroll
-            for (int j = 0; j < NOCC; ++j) c = (j == i) ? (T)Aw[(k * NOCC + j) * WPB + tid] : c;
-            coli[k] = c;
-          }
-#pragma unroll
-          for (int j = 0; j < NOCC; ++j) {
-            const T f = (wv[j] - (j == i ? (T)1 : (T)0)) * rinv;
-#pragma unroll
-            for (int k = 0; k < NOCC; ++k) {
-              Real& ref = Aw[(k * NOCC + j) * WPB + tid];
-              ref = (Real)((T)ref - coli[k] * f);
-            }
-          }
-          pos[(3 * e) * WPB + tid] = nx;
-          pos[(3 * e + 1) * WPB + tid] = ny;
-          pos[(3 * e + 2) * WPB + tid] = nz;
-          logdet += log(fabs(Rd));
-          ++nacc;
-        }
+        const double nx = pos[(3 * e) * WPB + tid] + a.step * n3[0];
+        const double ny = pos[(3 * e + 1) * WPB + tid] + a.step * n3[1];
+        const double nz = pos[(3 * e + 2) * WPB + tid] + a.step * n3[2];
+        nacc += oq_try_move<NOCC, T, Real>(S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz, 0.0, u,
+                                           logdet);
       }
-    }
-    // ---- local energy of this sweep ----
-    if (((sweep + 1) % a.measure_every) == 0) {
-      double ee = 0.0, en = 0.0, ke = 0.0, el = 0.0;
-      bool ok = live;
-      if (live) {
-        double lap_tot = 0.0, g2 = 0.0;
-        for (int e = 0; e < NE; ++e) {
-          const int s = e & 1, i = e >> 1;
-          const double xe = pos[(3 * e) * WPB + tid], ye = pos[(3 * e + 1) * WPB + tid],
-                       ze = pos[(3 * e + 2) * WPB + tid];
-          T mv[NOCC], mg[NOCC][3], ml[NOCC];
-          oq_mo_vgl_t<NOCC, T, Real>(S, SP, C, xe, ye, ze, mv, mg, ml);
-          const Real* As = Ai + (size_t)s * NN * WPB;
-          T gx = 0, gy = 0, gz = 0, lp = 0;
-#pragma unroll
-          for (int m = 0; m < NOCC; ++m) {
-            T am = (T)0;
-#pragma unroll
-            for (int j = 0; j < NOCC; ++j) am = (j == i) ? (T)As[(m * NOCC + j) * WPB + tid] : am;
-            gx += am * mg[m][0]; gy += am * mg[m][1]; gz += am * mg[m][2];
-            lp += am * ml[m];
-          }
-          double Gx = gx, Gy = gy, Gz = gz;
-          double L = (double)lp - (Gx * Gx + Gy * Gy + Gz * Gz);
-          for (int j = 0; j < NE; ++j) {
-            if (j == e) continue;
-            const double dx = xe - pos[(3 * j) * WPB + tid], dy = ye - pos[(3 * j + 1) * WPB + tid],
-                         dz = ze - pos[(3 * j + 2) * WPB + tid];
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            if (j > e) ee += 1.0 / sqrt(r2 + OQ_EPS);
-            if (S.has_j2) {
-              const int o = ((e & 1) == (j & 1)) ? 0 : 2;
-              double upr, l;
-              oq_pade_vgl(S.j2[o], S.j2[o + 1], sqrt(r2), upr, l);
-              Gx += upr * dx; Gy += upr * dy; Gz += upr * dz; L += l;
-            }
-          }
-          for (int I = 0; I < S.natm; ++I) {
-            const double dx = xe - S.nuc[I][0], dy = ye - S.nuc[I][1], dz = ze - S.nuc[I][2];
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            en -= S.Z[I] / sqrt(r2 + OQ_EPS);
-            if (S.has_j1) {
-              double upr, l;
-              oq_pade_vgl(S.j1a[I], S.j1b[I], sqrt(r2), upr, l);
-              Gx += upr * dx; Gy += upr * dy; Gz += upr * dz; L += l;
-            }
-          }
-          lap_tot += L;
-          g2 += Gx * Gx + Gy * Gy + Gz * Gz;
-        }
-        ke = -0.5 * (lap_tot + g2);
-        el = ee + en + ke + S.e_nn;
-        ok = isfinite(el);
-        if (!ok) bad |= OQ_FLAG_NAN;
-        if (a.el_trace) a.el_trace[(size_t)meas * W + w] = el;
-        if (a.eparts_last && meas * a.measure_every + a.measure_every >= a.n_sweeps) {
-          double* ep = a.eparts_last + (size_t)w * 4;
-          ep[0] = ee; ep[1] = en; ep[2] = ke; ep[3] = el;
-        }
+    } else {
+      double n3[3], u;
+      oq_move_randoms(a.seed, (uint32_t)w, gstep, 0xB0000000u, n3, u);
+      const OqU4 c = {(uint32_t)w, gstep, 0xB0000001u, 2u};
+      const OqU4 r = oq_philox(c, (uint32_t)a.seed, (uint32_t)(a.seed >> 32));
+      const int e = (int)(((uint64_t)r.x * NE) >> 32);
+      const int J = (int)(((uint64_t)r.y * S.natm) >> 32);
+      const double sg = a.step, inv2s2 = 1.0 / (2.0 * sg * sg);
+      const double nx = S.nuc[J][0] + sg * n3[0], ny = S.nuc[J][1] + sg * n3[1],
+                   nz = S.nuc[J][2] + sg * n3[2];
+      const double ox = pos[(3 * e) * WPB + tid], oy = pos[(3 * e + 1) * WPB + tid],
+                   oz = pos[(3 * e + 2) * WPB + tid];
+      // log q(x) = logsumexp_J(-|x - R_J|^2 / 2 sigma^2)
+      double mo = -INFINITY, mn = -INFINITY;
+      for (int I = 0; I < S.natm; ++I) {
+        const double dox = ox - S.nuc[I][0], doy = oy - S.nuc[I][1], doz = oz - S.nuc[I][2];
+        const double dnx = nx - S.nuc[I][0], dny = ny - S.nuc[I][1], dnz = nz - S.nuc[I][2];
+        mo = fmax(mo, -(dox * dox + doy * doy + doz * doz) * inv2s2);
+        mn = fmax(mn, -(dnx * dnx + dny * dny + dnz * dnz) * inv2s2);
       }
-      // fused walker reduction: warp shuffles, one atomic per warp and value
-      double vals[7] = {ok ? ee : 0.0, ok ? en : 0.0, ok ? ke : 0.0, ok ? el : 0.0,
-                        ok ? el * el : 0.0, (double)nacc, ok ? 1.0 : 0.0};
-#pragma unroll
-      for (int k = 0; k < 7; ++k) {
-        double v = vals[k];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        vals[k] = v;
+      double so = 0.0, sn = 0.0;
+      for (int I = 0; I < S.natm; ++I) {
+        const double dox = ox - S.nuc[I][0], doy = oy - S.nuc[I][1], doz = oz - S.nuc[I][2];
+        const double dnx = nx - S.nuc[I][0], dny = ny - S.nuc[I][1], dnz = nz - S.nuc[I][2];
+        so += exp(-(dox * dox + doy * doy + doz * doz) * inv2s2 - mo);
+        sn += exp(-(dnx * dnx + dny * dny + dnz * dnz) * inv2s2 - mn);
       }
-      if ((tid & 31) == 0) {
-        double* dst = a.sums + (size_t)meas * OQ_NSUM;
-#pragma unroll
-        for (int k = 0; k < 7; ++k) atomicAdd(dst + k, vals[k]);
-      }
-      ++meas;
+      const double log_qratio = (mo + log(so)) - (mn + log(sn));
+      nacc += oq_try_move<NOCC, T, Real>(S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
+                                         log_qratio, u, logdet);
     }
   }
   if (live) {
-    for (int k = 0; k < 3 * NE; ++k) a.X[(size_t)w * 3 * NE + k] = pos[k * WPB + tid];
-    Real* gAw = reinterpret_cast<Real*>(a.ainv);
-    for (int k = 0; k < 2 * NN; ++k) gAw[(size_t)k * W + w] = Ai[k * WPB + tid];
+    for (int k = 0; k < 3 * NE; ++k) a.pos[(size_t)k * W + w] = pos[k * WPB + tid];
+    for (int k = 0; k < 2 * NN; ++k) gA[(size_t)k * W + w] = Ai[k * WPB + tid];
     a.logdet[w] = logdet;
   }
-  if (bad) atomicOr(a.flags, bad);
+  if (a.acc_sum) {
+    double v = (double)nacc;   // every lane of the warp reaches here
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((tid & 31) == 0) atomicAdd(a.acc_sum, v);
+  }
+}
+
+struct OqElocArgs {
+  const double* pos;
+  const void* ainv;
+  int W;
+  int pad;
+  double* sums;           // OQ_NSUM slot of this measurement (accumulated)
+  double* el_trace;       // (W) local energies of this measurement, or null
+  double* eparts;         // (W, 4) ee, en, ke, E_L, or null
+  unsigned* flags;
+};
+
+// Local energy, one thread per (walker, electron): blockDim = (32, NE), lane
+// x = walker, y = electron.  Each thread forms its electron's MO VGL, the
+// Slater gradient/Laplacian against column i of the inverse
+// (_slater_det_assemble, gto.py:728-778), the Padé Jastrow VGL
+// (gto.py:1575-1649) and its Coulomb terms (gto.py:2406-2451); the CTA then
+// reduces over electrons (local_energy_ke, gto.py:2506-2579) and over
+// walkers (fused reduction of E, E^2 and the parts).
+template <int NOCC, typename T, typename Real>
+__global__ void __launch_bounds__(64 * NOCC, (NOCC <= 6) ? 2 : 1)
+k_eloc(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
+       const void* __restrict__ gC, OqElocArgs a) {
+  constexpr int NE = 2 * NOCC;
+  constexpr int NN = NOCC * NOCC;
+  extern __shared__ __align__(16) unsigned char smem[];
+  OqSystem& S = *reinterpret_cast<OqSystem*>(smem);
+  OqSplit& SP = *reinterpret_cast<OqSplit*>(smem + sizeof(OqSystem));
+  unsigned char* p = smem + sizeof(OqSystem) + sizeof(OqSplit);
+  Real* C = reinterpret_cast<Real*>(p);
+  const int nbf = gsys->nbf;
+  p += ((size_t)nbf * NOCC * sizeof(Real) + 15) & ~(size_t)15;
+  double* red = reinterpret_cast<double*>(p);          // [NE][4][32]
+  const int lane = threadIdx.x, e = threadIdx.y;
+  const int flat = e * 32 + lane, nthr = 32 * NE;
+  {
+    const int4* s4 = reinterpret_cast<const int4*>(gsys);
+    int4* d4 = reinterpret_cast<int4*>(&S);
+    for (int i = flat; i < (int)(sizeof(OqSystem) / 16); i += nthr) d4[i] = s4[i];
+    const double* src = reinterpret_cast<const double*>(gsplit);
+    double* dst = reinterpret_cast<double*>(&SP);
+    for (int i = flat; i < OQ_MAX_GROUP; i += nthr) dst[i] = src[i];
+    const Real* gc = reinterpret_cast<const Real*>(gC);
+    for (int i = flat; i < nbf * NOCC; i += nthr) C[i] = gc[i];
+  }
+  __syncthreads();
+  const int W = a.W;
+  const int w = blockIdx.x * 32 + lane;
+  const bool live = w < W;
+  double ee = 0.0, en = 0.0, lp_tot = 0.0, g2 = 0.0;
+  if (live) {
+    const int s = e & 1, i = e >> 1;
+    const double xe = a.pos[(size_t)(3 * e) * W + w], ye = a.pos[(size_t)(3 * e + 1) * W + w],
+                 ze = a.pos[(size_t)(3 * e + 2) * W + w];
+    T mv[NOCC], mg[NOCC][3], ml[NOCC];
+    oq_mo_vgl_t<NOCC, T, Real>(S, SP, C, xe, ye, ze, mv, mg, ml);
+    const Real* A = reinterpret_cast<const Real*>(a.ainv);
+    T gx = 0, gy = 0, gz = 0, lp = 0;
+#pragma unroll
+    for (int m = 0; m < NOCC; ++m) {
+      const T am = (T)A[(size_t)((s * NOCC + m) * NOCC + i) * W + w];
+      gx += am * mg[m][0]; gy += am * mg[m][1]; gz += am * mg[m][2];
+      lp += am * ml[m];
+    }
+    T jx = (T)0, jy = (T)0, jz = (T)0, jl = (T)0;
+    for (int j = 0; j < NE; ++j) {
+      if (j == e) continue;
+      const double dx = xe - a.pos[(size_t)(3 * j) * W + w],
+                   dy = ye - a.pos[(size_t)(3 * j + 1) * W + w],
+                   dz = ze - a.pos[(size_t)(3 * j + 2) * W + w];
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      if (j > e) ee += rsqrt(r2 + OQ_EPS);
+      if (S.has_j2) {
+        const int o = ((e & 1) == (j & 1)) ? 0 : 2;
+        const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
+        T upr, l;
+        oq_pade_vgl_q((T)S.j2[o], (T)S.j2[o + 1], r2t * rinv, rinv, upr, l);
+        jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
+      }
+    }
+    for (int I = 0; I < S.natm; ++I) {
+      const double dx = xe - S.nuc[I][0], dy = ye - S.nuc[I][1], dz = ze - S.nuc[I][2];
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      en -= S.Z[I] * rsqrt(r2 + OQ_EPS);
+      if (S.has_j1) {
+        const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
+        T upr, l;
+        oq_pade_vgl_q((T)S.j1a[I], (T)S.j1b[I], r2t * rinv, rinv, upr, l);
+        jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
+      }
+    }
+    const double sgx = (double)gx, sgy = (double)gy, sgz = (double)gz;
+    const double Gx = sgx + (double)jx, Gy = sgy + (double)jy, Gz = sgz + (double)jz;
+    lp_tot = (double)lp - (sgx * sgx + sgy * sgy + sgz * sgz) + (double)jl;
+    g2 = Gx * Gx + Gy * Gy + Gz * Gz;
+  }
+  red[(e * 4 + 0) * 32 + lane] = ee;
+  red[(e * 4 + 1) * 32 + lane] = en;
+  red[(e * 4 + 2) * 32 + lane] = lp_tot;
+  red[(e * 4 + 3) * 32 + lane] = g2;
+  __syncthreads();
+  if (e != 0) return;
+  double see = 0.0, sen = 0.0, slp = 0.0, sg2 = 0.0;
+  for (int k = 0; k < NE; ++k) {
+    see += red[(k * 4 + 0) * 32 + lane];
+    sen += red[(k * 4 + 1) * 32 + lane];
+    slp += red[(k * 4 + 2) * 32 + lane];
+    sg2 += red[(k * 4 + 3) * 32 + lane];
+  }
+  const double ke = -0.5 * (slp + sg2);
+  const double el = see + sen + ke + S.e_nn;
+  const bool ok = live && isfinite(el);
+  if (live) {
+    if (a.el_trace) a.el_trace[w] = el;
+    if (a.eparts) {
+      double* ep = a.eparts + (size_t)w * 4;
+      ep[0] = see; ep[1] = sen; ep[2] = ke; ep[3] = el;
+    }
+    if (!ok) atomicOr(a.flags, OQ_FLAG_NAN);
+  }
+  double vals[6] = {ok ? see : 0.0, ok ? sen : 0.0, ok ? ke : 0.0, ok ? el : 0.0,
+                    ok ? el * el : 0.0, ok ? 1.0 : 0.0};
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    double v = vals[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    vals[k] = v;
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) atomicAdd(a.sums + k, vals[k]);
+    atomicAdd(a.sums + 6, vals[5]);
+  }
 }

@@ -115,6 +115,16 @@ class WalkerEnsemble:
                 self.refresh(stream=stream)
         return sums
 
+    def basin(self, n_steps, sigma=1.5, stream=None):
+        """Basin relocation moves (``vmc_gto.py:925-957``); returns the mean
+        acceptance."""
+        acc = torch.zeros(1, dtype=torch.float64, device=self.X.device)
+        self.ctx.basin(self.X, self.state, self.prec, n_steps, sigma, self.seed ^ 0xBA5E,
+                       self.step_count, acc_sum=acc, stream=stream)
+        self.step_count += n_steps
+        self.refresh(stream=stream)
+        return float(acc.item()) / max(1, n_steps * self.W)
+
     def logdet(self):
         off = self.state.numel() - ((self.W * 8 + 255) // 256) * 256
         return self.state[off:off + self.W * 8].view(torch.float64)

@@ -109,3 +109,40 @@ def test_sampler_rejects_bad_arguments():
         ens.run(4, -1.0)
     with pytest.raises(ValueError):
         WalkerEnsemble(ctx, seeded_walkers(s, 8, 0.5, 0), "fp16")
+
+
+def test_basin_moves_keep_state_consistent():
+    s = _sys("H2O")
+    ctx = GTOContext(s)
+    W = 512
+    ens = WalkerEnsemble(ctx, seeded_walkers(s, W, 0.8, 3), "fp64", seed=5,
+                         refresh_every=10**9)
+    acc = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ctx.basin(ens.X, ens.state, ens.prec, 50, 1.5, 99, 0, acc_sum=acc)
+    torch.cuda.synchronize()
+    Xf = ens.X.cpu().numpy()
+    ld = ens.logdet().cpu().numpy()
+    ld_ref = O.log_slater(s, Xf)
+    assert np.max(np.abs(ld - ld_ref) / (np.abs(ld_ref) + 1)) < 1e-8
+    rate = float(acc.item()) / (50 * W)
+    assert 0.0005 < rate < 0.95, rate
+
+
+def test_basin_moves_sample_psi_squared_h2():
+    """Basin relocations alone are an exact MH chain for |psi|^2: the mean
+    local energy matches the oracle's reference-algorithm sampler."""
+    s = _sys("H2")
+    ctx = GTOContext(s)
+    ens = WalkerEnsemble(ctx, seeded_walkers(s, 4096, 0.5, 2), "fp64", seed=8,
+                         refresh_every=10**9)
+    ctx.basin(ens.X, ens.state, ens.prec, 200, 1.5, 17, 0)
+    series = []
+    for k in range(300):
+        ctx.basin(ens.X, ens.state, ens.prec, 4, 1.5, 17, 1000 + 4 * k)
+        series.append(float(ctx.evaluate(ens.X, want_grad=False, want_lap=False)["e_loc"].mean()))
+    m_b, se_b, _, _ = O.binning_analysis(np.array(series))
+    X0 = seeded_walkers(s, 512, 0.5, 1)
+    ser, _, _, _ = V.run_vmc(s, X0, 300, 3000, seed=3)
+    m_ref, se_ref, _, _ = O.binning_analysis(ser)
+    z = abs(m_b - m_ref) / np.hypot(se_b, se_ref)
+    assert z < 3.0, (m_b, se_b, m_ref, se_ref)
