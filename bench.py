@@ -38,6 +38,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 REFRESH_EVERY = 50
+EQUIL_SWEEPS = 3000
 
 
 def parse():
@@ -63,10 +64,7 @@ def build_system(name):
     from omegaqmc_b200 import molecules as M
     from omegaqmc_b200.system import build_system as bs
     mf = M.make_mf(name)
-    params = M.default_params_corr(mf.mol)
-    if name == "H2":
-        params = {"J2_pade": params["J2_pade"]}
-    return bs(mf, params)
+    return bs(mf, M.benchmark_params_corr(mf.mol))
 
 
 def work_per_walker_sweep(s, acc=0.5):
@@ -148,25 +146,40 @@ def dist_env():
     return rank, world, local
 
 
-def cpu_reference(system, seconds, nthreads, step, seed=7):
-    """Reference algorithm on host cores; returns (walker-steps/s, tau, sample)."""
+def cpu_reference(system, seconds, nthreads, step, seed=7, n_equil=300):
+    """Reference algorithm on host cores (OmegaQMC/vmc_gto.py:1338-1357 step
+    adaptation during equilibration, then fixed-step production); returns
+    (walker-steps/s, tau_int, acceptance, sample description, E_L series)."""
     from oracle import cref
     from oracle import gto_oracle as O
     from omegaqmc_b200.sampler import init_walkers_gaussian
     W = 256
     X = np.ascontiguousarray(init_walkers_gaussian(system, W, 1.0, seed))
-    cref.run(system, X, 20, step, seed=seed, nthreads=nthreads)        # equilibrate
+    for k in range(n_equil):
+        _, acc = cref.run(system, X, 1, step, seed=seed * 1000003 + k, nthreads=nthreads)
+        step = float(np.exp(np.log(step) + 0.05 * (acc - 0.4)))
     t0 = time.perf_counter()
-    ser, acc = cref.run(system, X, 10, step, seed=seed + 1, nthreads=nthreads)
-    dt = time.perf_counter() - t0
-    per_step = dt / 10
-    n = max(50, int(seconds / max(per_step, 1e-6)))
+    cref.run(system, X, 10, step, seed=seed + 1, nthreads=nthreads)
+    per_step = (time.perf_counter() - t0) / 10
+    n = max(200, int(seconds / max(per_step, 1e-6)))
     t0 = time.perf_counter()
     ser, acc = cref.run(system, X, n, step, seed=seed + 2, nthreads=nthreads)
     dt = time.perf_counter() - t0
     rate = W * n / dt
     _, _, _, kappa = O.binning_analysis(ser[:, 3])
-    return rate, kappa, acc, f"{W} walkers x {n} steps ({dt:.1f} s)", ser[:, 3]
+    return (rate, kappa, acc,
+            f"{W} walkers x {n} steps ({dt:.1f} s) after {n_equil} adaptive equilibration "
+            f"steps, step {step:.3f}", ser[:, 3])
+
+
+def adapt_step(ens, step, n_chunks=40, chunk=5, target=0.4):
+    """Equilibrate with the reference's rule log s += 0.05 (acc - target)
+    applied once per chunk of sweeps (OmegaQMC/vmc_gto.py:121-126)."""
+    for _ in range(n_chunks):
+        s = ens.run(chunk, step).cpu().numpy()
+        acc = s[:, 5].sum() / (chunk * ens.W * ens.ctx.n_e)
+        step = float(np.exp(np.log(step) + 0.05 * 5 * (acc - target)))
+    return step
 
 
 def run_reference(a):
@@ -176,8 +189,8 @@ def run_reference(a):
     system = build_system(a.system)
     step = a.step_size or STEP_DEFAULT.get(a.system, 0.3) * 1.0
     cores = len(os.sched_getaffinity(0))
-    # the reference's all-electron move needs a smaller step than a sweep
-    ref_step = step * 0.5
+    # initial step of the reference's adaptation (sqrt(3 * mc_timestep))
+    ref_step = (3 * 0.1) ** 0.5
     rates, kappas = [], []
     for _ in range(max(1, min(a.steps, 3))):
         rate, kappa, acc, sample, _ = cpu_reference(system, a.cpu_seconds / 3, cores, ref_step)
@@ -225,7 +238,11 @@ def run_ours(a):
                          refresh_every=REFRESH_EVERY)
     stream = torch.cuda.current_stream()
 
-    # warm-up (also equilibrates)
+    # set-up: step adaptation and a fixed equilibration (core electrons start
+    # far from their equilibrium density), then the W warm-up sweeps
+    if not a.step_size:
+        step = adapt_step(ens, step)
+    ens.run(EQUIL_SWEEPS, step)
     ens.run(max(a.warmup, 3), step)
     torch.cuda.synchronize()
 
@@ -256,6 +273,31 @@ def run_ours(a):
         tau_src = "untimed 2000-sweep series"
     e_mean, e_serr, e_sdev, kappa = O.binning_analysis(tau_series)
     acc = float(s_np[:, 5].sum() / (K * W * system.n_e))
+
+    # the comparison target: the plain FP64 sampler on the same walkers
+    plain = None
+    if a.precision != "fp64":
+        pe = WalkerEnsemble(ctx, ens.X, "fp64", seed=99 + rank, refresh_every=REFRESH_EVERY)
+        pe.run(20, step)
+        Kp = max(1000, min(K, 2000))
+        ps = torch.zeros(Kp, NSUM, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        pe.run(Kp, step, sums=ps)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        pms = p0.elapsed_time(p1)
+        pn = ps.cpu().numpy()
+        pser = pn[:, 3] / np.maximum(pn[:, 6], 1)
+        pm, pse, _, pk = O.binning_analysis(pser)
+        pw = W * Kp / (pms * 1e-3)
+        plain = {"value": pw * world / pk, "walker_sweeps_per_s": pw * world, "tau_int": pk,
+                 "ms_per_step": pms / Kp, "steps": Kp,
+                 "energy": {"mean": pm, "serr": pse},
+                 "energy_diff_sigma": abs(pm - e_mean) / max(np.hypot(pse, e_serr), 1e-300)}
+        del pe
 
     # kernel-level timing of the dominant kernel on its own stream: one chunk
     # of REFRESH_EVERY sweeps = one k_sweeps launch; the refresh separately
@@ -323,6 +365,8 @@ def run_ours(a):
                                f"sweeps + E_L every sweep, FP64 LU refresh every {REFRESH_EVERY}",
                    "precision": a.precision, "walkers_per_gpu": W, "step": step,
                    "parallelism": f"replicas x{world}",
+                   "trial": "RHF determinant + Pade J2 (b=3)",
+                   "equilibration_sweeps": EQUIL_SWEEPS + 200,
                    "l2": "walker state stays in shared memory for a whole launch; "
                          "inputs 41 MB are re-read once per 50-sweep launch"},
         "walker_sweeps_per_s": wss, "tau_int": kappa, "tau_source": tau_src,
@@ -331,11 +375,15 @@ def run_ours(a):
         "roofline": {"bound": "fp64" if peak_kind == 0 else "fp32",
                      "achieved": achieved / 1e12, "peak": rate / 1e12, "unit": "TFLOP/s",
                      "frac": achieved / rate if rate else None, "traffic": traffic,
-                     "kernel": "k_sweeps", "kernel_ms_per_launch": sweep_ms,
+                     "kernel": "k_moves+k_eloc (one 50-sweep oqmc_sweeps call)",
+                     "kernel_ms_per_launch": sweep_ms,
                      "refresh_ms_per_launch": refresh_ms,
                      "flops_per_walker_sweep": work["flops"],
                      "peak_source": "own FMA microkernel (oqmc_measure_peak), of measured"},
     }
+    if plain:
+        line["plain_fp64"] = plain
+        line["speedup_vs_plain_fp64"] = value / plain["value"]
     if e2e:
         line["e2e"] = {"value": W * world / (e2e_ms * 1e-3) / kappa,
                        "unit": "decorrelated samples/s",
@@ -344,12 +392,10 @@ def run_ours(a):
                        "ms_per_step": e2e_ms}
     if rank == 0 and not a.no_cpu and world == 1:
         cores = len(os.sched_getaffinity(0))
-        r, kap, acc_c, sample, _ = cpu_reference(system, a.cpu_seconds, cores, step * 0.5)
+        r, kap, acc_c, sample, _ = cpu_reference(system, a.cpu_seconds, cores, (3 * 0.1) ** 0.5)
         line["cpu_baseline"] = {"value": r / kap, "unit": "decorrelated samples/s",
                                 "cores": cores, "kind": "port", "sample": sample,
                                 "walker_steps_per_s": r, "tau_int": kap}
-    with ClockSampler(local) as _:
-        pass
     line["clocks"] = clk.summary()
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -86,6 +86,8 @@ def build(force=False, jobs=None, verbose=False):
     os.replace(tmp, LIB)
     with open(stamp, "w") as f:
         f.write(key)
+    from . import rhf
+    rhf._load()          # host integral library of the RHF front end
     return LIB
 
 

@@ -8,16 +8,15 @@ sets of the named systems are generated here:
 * ``ccpvdz_shaped(sym)`` is a *shape-matched synthetic* basis: the same
   angular momenta, number of basis entries, contraction depths and general
   contraction layout as cc-pVDZ (H: 2s1p = 5 functions; Li-Ne: 3s2p1d = 14
-  functions, the core s entry a two-column general contraction), with
-  exponents and coefficients from a deterministic even-tempered rule.  The
-  function counts (LiH 19, H2O 24, N2 28, (H2O)2 48) and the per-position
-  exponential counts therefore match the real basis; absolute energies do
-  not match literature values.
+  functions, the core s entry a two-column general contraction), built from
+  even-tempered primitives with contraction coefficients fitted to
+  Slater-type orbitals.  The function counts (LiH 19, H2O 24, N2 28,
+  (H2O)2 48) match the real basis; RHF energies are STO-3G-like
+  (H2O -74.80, N2 -107.67, LiH -7.88 hartree), not cc-pVDZ's.
 
-Occupied MO coefficients are seeded (``seeded_mo_coeff``): an aufbau-like
-choice of one dominant AO per occupied orbital plus a seeded admixture of
-all AOs, or, for H2, the symmetric bonding combination (which is the RHF
-orbital of a two-function homonuclear basis).
+Occupied orbitals come from this package's RHF (``omegaqmc_b200.rhf``) by
+default; ``seeded_mo_coeff`` gives reproducible non-SCF orbitals for parity
+tests (an aufbau-like dominant AO per orbital plus a seeded admixture).
 """
 from __future__ import annotations
 
@@ -26,7 +25,8 @@ import numpy as np
 from .system import Mole, MeanField, ELEMENT_Z, build_shells, ANG_TO_BOHR
 
 __all__ = ["sto3g_h", "ccpvdz_shaped", "named_system", "NAMED_SYSTEMS",
-           "seeded_mo_coeff", "default_params_corr", "synthetic_cusp_params"]
+           "seeded_mo_coeff", "default_params_corr", "benchmark_params_corr",
+           "synthetic_cusp_params", "make_mf"]
 
 
 def sto3g_h():
@@ -39,35 +39,64 @@ def _even_tempered(a_max, ratio, n):
     return a_max / ratio ** np.arange(n)
 
 
+# Slater's-rules orbital exponents (zeta of the 1s and of the 2s/2p shells);
+# hydrogen uses the molecular value 1.24.
+_SLATER = {"H": (1.24, None), "He": (1.69, None), "Li": (2.69, 0.65), "Be": (3.69, 0.975),
+           "B": (4.68, 1.3), "C": (5.67, 1.625), "N": (6.67, 1.95), "O": (7.66, 2.275),
+           "F": (8.65, 2.6), "Ne": (9.64, 2.925)}
+# polarisation exponents of the single d (first row) or p (H, He) function
+_POL = {"H": 0.73, "He": 1.2, "Li": 0.2, "Be": 0.26, "B": 0.4, "C": 0.55, "N": 0.82,
+        "O": 1.2, "F": 1.6, "Ne": 2.0}
+
+
+def _sto_fit(alphas, zeta, n, l):
+    """Least-squares Gaussian expansion of the Slater function r^(n-1) e^(-zeta r)
+    with primitives r^l e^(-alpha r^2), in the r^2-weighted L2 norm; returns the
+    coefficients of the unnormalised primitives (read_shell normalises)."""
+    r = np.linspace(1e-4, 30.0 / zeta, 6000)
+    w = r ** 2
+    target = r ** (n - 1) * np.exp(-zeta * r)
+    target = target / np.sqrt(np.sum(w * target * target))
+    G = r[:, None] ** l * np.exp(-alphas[None, :] * r[:, None] ** 2)
+    cn = (2 * alphas / np.pi) ** 0.75 * (4 * alphas) ** (l / 2)   # primitive norms
+    A = (G * cn[None, :]) * np.sqrt(w)[:, None]
+    c, *_ = np.linalg.lstsq(A, target * np.sqrt(w), rcond=None)
+    return c
+
+
 def ccpvdz_shaped(sym):
-    """Synthetic basis with cc-pVDZ's shape for ``sym`` (PySCF format)."""
-    Z = ELEMENT_Z[sym]
-    if Z <= 2:
-        s_exp = _even_tempered(10.0 * Z ** 2, 4.6, 3)
-        s_cof = np.array([0.03, 0.20, 0.55])
+    """Synthetic basis with cc-pVDZ's shape for ``sym`` (PySCF format).
+
+    Contractions are least-squares fits to Slater-type orbitals (1s; 2s, 2p
+    with Slater's-rules exponents) over even-tempered primitives, the way
+    STO-nG sets are built; the uncontracted diffuse and polarisation
+    functions follow cc-pVDZ's layout."""
+    z1, z2 = _SLATER[sym]
+    if z2 is None:
+        s_exp = _even_tempered(18.0 * z1 ** 2, 5.2, 3)
+        s_cof = _sto_fit(s_exp, z1, 1, 0)
         return [
-            [0] + [[a, c] for a, c in zip(s_exp, s_cof)],
-            [0, [0.14 * Z, 1.0]],
-            [1, [0.8 * Z, 1.0]],
+            [0] + [[float(a), float(c)] for a, c in zip(s_exp, s_cof)],
+            [0, [float(0.08 * z1 ** 2), 1.0]],
+            [1, [_POL[sym], 1.0]],
         ]
-    # first row: 9-primitive s general contraction with two columns
-    n_s = 9 if Z >= 5 else 8
-    a_max = 1500.0 * Z ** 1.5
-    s_exp = _even_tempered(a_max, 3.55, n_s)
-    x = np.arange(n_s) / (n_s - 1)
-    core = np.exp(-((x - 0.62) / 0.22) ** 2)
-    core[-1] *= -0.1
-    val = -0.45 * np.exp(-((x - 0.6) / 0.2) ** 2)
-    val[-2:] = [0.55, 0.60]
-    s_entry = [0] + [[a, c1, c2] for a, c1, c2 in zip(s_exp, core, val)]
-    p_exp = _even_tempered(2.2 * Z, 4.3, 3)
-    p_entry = [1] + [[a, c] for a, c in zip(p_exp, [0.05, 0.25, 0.55])]
+    n_s = 9 if ELEMENT_Z[sym] >= 5 else 8
+    a_max = 220.0 * z1 ** 2
+    a_min = 0.09 * z2 ** 2
+    ratio = (a_max / a_min) ** (1.0 / (n_s - 1))
+    s_exp = _even_tempered(a_max, ratio, n_s)
+    c1 = _sto_fit(s_exp, z1, 1, 0)
+    c2 = _sto_fit(s_exp, z2, 2, 0)
+    s_entry = [0] + [[float(a), float(x), float(y)] for a, x, y in zip(s_exp, c1, c2)]
+    p_exp = _even_tempered(6.0 * z2 ** 2, 4.2, 3)
+    p_cof = _sto_fit(p_exp, z2, 2, 1)
+    p_entry = [1] + [[float(a), float(c)] for a, c in zip(p_exp, p_cof)]
     return [
         s_entry,
-        [0, [0.038 * Z, 1.0]],
+        [0, [float(0.05 * z2 ** 2), 1.0]],
         p_entry,
-        [1, [0.034 * Z, 1.0]],
-        [2, [0.15 * Z, 1.0]],
+        [1, [float(0.055 * z2 ** 2), 1.0]],
+        [2, [_POL[sym], 1.0]],
     ]
 
 
@@ -163,17 +192,28 @@ def seeded_mo_coeff(mol, seed=0, mix=0.08):
     return C
 
 
-def default_params_corr(mol, cusp=False):
-    """Padé Jastrow parameters used by the benchmarks.
+def default_params_corr(mol, cusp=False, j1=True):
+    """Padé Jastrow parameters.
 
-    J2 satisfies the e-e cusp (like 0.25, unlike 0.5) with b = 1.0; J1 is
-    ``b = 1.0`` per element (``a = -Z`` implied without cusp correction)."""
-    j1 = {}
-    for s in set(mol.elements):
-        j1[s] = np.array([-0.05, 1.0]) if cusp else np.array(1.0)
-    return {"J1_pade": j1,
-            "J2_pade": {"like": np.array([0.25, 1.0]),
-                        "unlike": np.array([0.5, 1.0])}}
+    J2 satisfies the e-e cusp (like 0.25, unlike 0.5) with b = 1.0.  With
+    ``j1``, J1 is ``b = 1.0`` per element (``a = -Z`` implied without cusp
+    correction) or ``[-0.05, 1.0]`` with it."""
+    out = {"J2_pade": {"like": np.array([0.25, 1.0]),
+                       "unlike": np.array([0.5, 1.0])}}
+    if j1:
+        out["J1_pade"] = {s: (np.array([-0.05, 1.0]) if cusp else np.array(1.0))
+                          for s in set(mol.elements)}
+    return out
+
+
+def benchmark_params_corr(mol):
+    """Jastrow of the benchmark trial: Padé J2 (cusp a = 0.25 / 0.5, b = 3).
+
+    With Gaussian orbitals that already fit the 1s shape, the cusp-free J1
+    (a = -Z) counts the nuclear cusp twice and raises the local-energy
+    variance of H2O from about 90 to several thousand hartree^2; among
+    J2-only trials b = 3 gave the lowest variance (85 hartree^2)."""
+    return {"J2_pade": {"like": np.array([0.25, 3.0]), "unlike": np.array([0.5, 3.0])}}
 
 
 def synthetic_cusp_params(mol, seed=3):
@@ -190,6 +230,17 @@ def synthetic_cusp_params(mol, seed=3):
     return out
 
 
-def make_mf(name, seed=0):
+_RHF_CACHE = {}
+
+
+def make_mf(name, mos="rhf", seed=0):
+    """Mean-field object of a named system: RHF orbitals (``mos="rhf"``)
+    or seeded non-SCF orbitals (``mos="seeded"``)."""
     mol = named_system(name)
-    return MeanField(mol, seeded_mo_coeff(mol, seed=seed))
+    if mos == "seeded":
+        return MeanField(mol, seeded_mo_coeff(mol, seed=seed))
+    if name not in _RHF_CACHE:
+        from .rhf import run_rhf
+        _RHF_CACHE[name] = run_rhf(mol)
+    mf = _RHF_CACHE[name]
+    return MeanField(mol, mf.mo_coeff, mf.mo_occ)
