@@ -152,6 +152,27 @@ int oqmc_basin(oqmc_ctx* ctx, double* walkers, int W, void* state, int precision
                int n_steps, double sigma, uint64_t seed, uint64_t step_base,
                double* acc_sum, void* stream);
 
+/* Size of the device array behind oqmc_sweeps_noalloc (every GPU that
+ * loads the library holds it until the library is unloaded). */
+#define OQ_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* Allocation-free sampling, for callers that cannot allocate device memory
+ * (their device memory belongs to another allocator's arena or budget, or
+ * a cudaMalloc would synchronise the device on their path).  No counterpart
+ * in the reference.  Runs oqmc_refresh + oqmc_sweeps with the walker state
+ * in a library-owned 16 MiB device array instead of a caller buffer: every
+ * call refreshes the state from `walkers`, then runs the sweeps; the other
+ * arguments mean what they mean for oqmc_sweeps.  W is limited to
+ * oqmc_state_bytes(ctx, W, precision) <= OQ_NOALLOC_SCRATCH_BYTES (about
+ * 25,000 FP64 H2O walkers); larger W returns OQ_ERR_ARG.  Allocates
+ * nothing.  The first call on a device looks up the array's device address;
+ * make it before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race, so serialise them. */
+int oqmc_sweeps_noalloc(oqmc_ctx* ctx, double* walkers, int W, int precision,
+                        int n_sweeps, int measure_every, double step,
+                        uint64_t seed, uint64_t step_base, double* sums,
+                        double* el_trace, double* eparts_last, void* stream);
+
 /* Exponent threshold above which an exponent group is evaluated in FP64
  * near its nucleus in the mixed build (default 50.0; <= 0 disables). */
 int oqmc_set_split(oqmc_ctx* ctx, double tight_alpha);

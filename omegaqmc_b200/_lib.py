@@ -75,6 +75,9 @@ _SIGS = [
                             c_int, c_void_p]),
     ("oqmc_basin", c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_int, c_double,
                            c_uint64, c_uint64, c_void_p, c_void_p]),
+    ("oqmc_sweeps_noalloc", c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int,
+                                    c_double, c_uint64, c_uint64, c_void_p, c_void_p,
+                                    c_void_p, c_void_p]),
     ("oqmc_set_split", c_int, [c_void_p, c_double]),
     ("oqmc_get_flags", c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint), c_int, c_void_p]),
     ("oqmc_measure_peak", c_int, [c_int, P_double, c_void_p]),

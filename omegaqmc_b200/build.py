@@ -64,7 +64,8 @@ def build(force=False, jobs=None, verbose=False):
         return LIB
     jobs = jobs or max(1, min(len(NOCC_LIST) + 1, os.cpu_count() or 4))
     units = [(os.path.join(CSRC, "oqmc.cu"), os.path.join(BUILD, "oqmc.o"), []),
-             (os.path.join(CSRC, "oqmc_peak.cu"), os.path.join(BUILD, "oqmc_peak.o"), [])]
+             (os.path.join(CSRC, "oqmc_peak.cu"), os.path.join(BUILD, "oqmc_peak.o"), []),
+             (os.path.join(CSRC, "oqmc_noalloc.cu"), os.path.join(BUILD, "oqmc_noalloc.o"), [])]
     for n in NOCC_LIST:
         units.append((os.path.join(CSRC, "oqmc_inst.cu"),
                       os.path.join(BUILD, f"oqmc_inst_{n}.o"), [f"-DOQ_N={n}"]))

@@ -131,6 +131,11 @@ static void compute_split(oqmc_ctx* ctx) {
   }
 }
 
+// Record an error on a context (used by entry points in other files).
+int oq_ctx_set_error(oqmc_ctx* ctx, int code, const char* msg) {
+  return set_err(ctx, code, "%s", msg);
+}
+
 extern "C" {
 
 const char* oqmc_version(void) { return "oqmc_b200 0.1.0 (sm_100a)"; }
