@@ -39,6 +39,7 @@ sys.path.insert(0, ROOT)
 
 REFRESH_EVERY = 50
 EQUIL_SWEEPS = 3000
+SCALED_R0, SCALED_FMIN = 1.0, 0.05
 
 
 def parse():
@@ -54,6 +55,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--proposal", default="scaled", choices=["scaled", "plain"])
     return ap.parse_args()
 
 
@@ -231,6 +233,8 @@ def run_ours(a):
     dev = torch.device("cuda", local)
     system = build_system(a.system)
     ctx = GTOContext(system)
+    if a.proposal == "scaled":
+        ctx.set_proposal(1, SCALED_R0, SCALED_FMIN)
     W = a.walkers
     step = a.step_size or STEP_DEFAULT.get(a.system, 0.3)
     X0 = init_walkers_gaussian(system, W, 1.0, seed=1000 + rank)
@@ -276,16 +280,18 @@ def run_ours(a):
 
     # the comparison target: the plain FP64 sampler on the same walkers
     plain = None
-    if a.precision != "fp64":
-        pe = WalkerEnsemble(ctx, ens.X, "fp64", seed=99 + rank, refresh_every=REFRESH_EVERY)
-        pe.run(20, step)
-        Kp = max(1000, min(K, 2000))
+    if a.precision != "fp64" or a.proposal != "plain":
+        pctx = GTOContext(system)            # fixed-width Gaussian proposal
+        pe = WalkerEnsemble(pctx, ens.X, "fp64", seed=99 + rank, refresh_every=REFRESH_EVERY)
+        pstep = adapt_step(pe, STEP_DEFAULT.get(a.system, 0.3))
+        pe.run(500, pstep)
+        Kp = 4000
         ps = torch.zeros(Kp, NSUM, dtype=torch.float64, device=dev)
         torch.cuda.synchronize()
         p0 = torch.cuda.Event(enable_timing=True)
         p1 = torch.cuda.Event(enable_timing=True)
         p0.record(stream)
-        pe.run(Kp, step, sums=ps)
+        pe.run(Kp, pstep, sums=ps)
         p1.record(stream)
         torch.cuda.synchronize()
         pms = p0.elapsed_time(p1)
@@ -294,6 +300,7 @@ def run_ours(a):
         pm, pse, _, pk = O.binning_analysis(pser)
         pw = W * Kp / (pms * 1e-3)
         plain = {"value": pw * world / pk, "walker_sweeps_per_s": pw * world, "tau_int": pk,
+                 "proposal": "fixed-width Gaussian", "step": pstep,
                  "ms_per_step": pms / Kp, "steps": Kp,
                  "energy": {"mean": pm, "serr": pse},
                  "energy_diff_sigma": abs(pm - e_mean) / max(np.hypot(pse, e_serr), 1e-300)}
@@ -366,6 +373,8 @@ def run_ours(a):
                    "precision": a.precision, "walkers_per_gpu": W, "step": step,
                    "parallelism": f"replicas x{world}",
                    "trial": "RHF determinant + Pade J2 (b=3)",
+                   "proposal": (f"nucleus-scaled Gaussian (r0={SCALED_R0}, fmin={SCALED_FMIN}), "
+                                "exact MH" if a.proposal == "scaled" else "fixed-width Gaussian"),
                    "equilibration_sweeps": EQUIL_SWEEPS + 200,
                    "l2": "walker state stays in shared memory for a whole launch; "
                          "inputs 41 MB are re-read once per 50-sweep launch"},

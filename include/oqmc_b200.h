@@ -173,6 +173,15 @@ int oqmc_sweeps_noalloc(oqmc_ctx* ctx, double* walkers, int W, int precision,
                         uint64_t seed, uint64_t step_base, double* sums,
                         double* el_trace, double* eparts_last, void* stream);
 
+/* Proposal of the single-electron moves of oqmc_sweeps: kind 0 (default)
+ * is the reference's fixed-width Gaussian (metropolis_move_alle,
+ * OmegaQMC/vmc_gto.py:815-839, applied per electron); kind 1 scales the width
+ * with the distance to the nearest nucleus, sigma(x) = step *
+ * clamp(r_near(x) / r0, fmin_frac, 1), and corrects the acceptance with the
+ * exact proposal-density ratio, so the stationary distribution is unchanged
+ * while core electrons move with core-sized steps. */
+int oqmc_set_proposal(oqmc_ctx* ctx, int kind, double r0, double fmin_frac);
+
 /* Exponent threshold above which an exponent group is evaluated in FP64
  * near its nucleus in the mixed build (default 50.0; <= 0 disables). */
 int oqmc_set_split(oqmc_ctx* ctx, double tight_alpha);

@@ -78,6 +78,7 @@ _SIGS = [
     ("oqmc_sweeps_noalloc", c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int,
                                     c_double, c_uint64, c_uint64, c_void_p, c_void_p,
                                     c_void_p, c_void_p]),
+    ("oqmc_set_proposal", c_int, [c_void_p, c_int, c_double, c_double]),
     ("oqmc_set_split", c_int, [c_void_p, c_double]),
     ("oqmc_get_flags", c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint), c_int, c_void_p]),
     ("oqmc_measure_peak", c_int, [c_int, P_double, c_void_p]),

@@ -203,5 +203,9 @@ class GTOContext:
             float(sigma), ctypes.c_uint64(seed & (2**64 - 1)), ctypes.c_uint64(step_base),
             _dptr(acc_sum), _stream_ptr(stream)))
 
+    def set_proposal(self, kind, r0=1.0, fmin_frac=0.05):
+        """0: fixed-width Gaussian (reference); 1: nucleus-scaled width."""
+        self._check(self.lib.oqmc_set_proposal(self._h, int(kind), float(r0), float(fmin_frac)))
+
     def set_split(self, tight_alpha):
         self._check(self.lib.oqmc_set_split(self._h, float(tight_alpha)))

@@ -21,6 +21,8 @@ struct oqmc_ctx {
   float* d_C32;
   unsigned* d_flags;
   double tight_alpha;
+  int proposal;           // 0 fixed-width Gaussian, 1 nucleus-scaled width
+  double scale_r0, scale_fmin;
   char err[512];
 };
 
@@ -204,6 +206,9 @@ int oqmc_create(oqmc_ctx** out, const oqmc_system_desc* d) {
   }
   ctx->nocc = d->nocc; ctx->n_e = d->n_e; ctx->nbf = d->nbf; ctx->natm = d->natm;
   ctx->tight_alpha = 50.0;
+  ctx->proposal = 0;
+  ctx->scale_r0 = 1.0;
+  ctx->scale_fmin = 0.05;
   compute_split(ctx);
   cudaGetDevice(&ctx->device);
   build_harm_table(S.harm);
@@ -237,6 +242,15 @@ int oqmc_destroy(oqmc_ctx* ctx) {
   cudaFree(ctx->d_C32);
   cudaFree(ctx->d_flags);
   delete ctx;
+  return OQ_OK;
+}
+
+int oqmc_set_proposal(oqmc_ctx* ctx, int kind, double r0, double fmin_frac) {
+  if (!ctx) return OQ_ERR_ARG;
+  if (kind < 0 || kind > 1 || (kind == 1 && (!(r0 > 0.0) || !(fmin_frac > 0.0) || fmin_frac > 1.0)))
+    return set_err(ctx, OQ_ERR_ARG, "bad proposal parameters%s");
+  ctx->proposal = kind;
+  if (kind == 1) { ctx->scale_r0 = r0; ctx->scale_fmin = fmin_frac; }
   return OQ_OK;
 }
 
@@ -434,6 +448,7 @@ int oqmc_sweeps(oqmc_ctx* ctx, double* X, int W, void* state, int precision, int
   memset(&m, 0, sizeof(m));
   m.pos = st.pos; m.ainv = st.ainv; m.logdet = st.logdet; m.W = W; m.mode = 0;
   m.step = step; m.seed = seed; m.flags = ctx->d_flags;
+  m.proposal = ctx->proposal; m.scale_r0 = ctx->scale_r0; m.scale_fmin = ctx->scale_fmin;
   OqElocArgs el;
   memset(&el, 0, sizeof(el));
   el.pos = st.pos; el.ainv = st.ainv; el.W = W; el.flags = ctx->d_flags;

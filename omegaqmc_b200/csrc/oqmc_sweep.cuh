@@ -257,13 +257,28 @@ struct OqMoveArgs {
   int W;
   int n_steps;            // sweeps (mode 0) or basin relocations (mode 1)
   int mode;               // 0: Gaussian single-electron sweeps; 1: basin relocation
-  int pad;
+  int proposal;           // mode 0: 0 = fixed width, 1 = nucleus-scaled width
   double step;            // Gaussian width (mode 0) or blob width sigma (mode 1)
+  double scale_r0;        // nucleus-scaled width: sigma = step * clamp(r_near/r0, fmin, 1)
+  double scale_fmin;
   uint64_t seed;
   uint64_t step_base;     // RNG counter of the first step
   double* acc_sum;        // += accepted moves (may be null)
   unsigned* flags;
 };
+
+// Proposal width at x for the nucleus-scaled Gaussian move.
+__device__ __forceinline__ double oq_scaled_width(const OqSystem& S, double x, double y,
+                                                  double z, double step, double r0,
+                                                  double fmn) {
+  double r2 = 1e300;
+  for (int I = 0; I < S.natm; ++I) {
+    const double dx = x - S.nuc[I][0], dy = y - S.nuc[I][1], dz = z - S.nuc[I][2];
+    r2 = fmin(r2, dx * dx + dy * dy + dz * dz);
+  }
+  const double f = sqrt(r2) / r0;
+  return step * fmin(1.0, fmax(fmn, f));
+}
 
 // One single-electron Metropolis move of electron e to (nx, ny, nz) against
 // shared-memory state; log_extra is the log proposal-density ratio
@@ -402,7 +417,7 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
   int nacc = 0;
   for (int t = 0; t < (live ? a.n_steps : 0); ++t) {
     const uint32_t gstep = (uint32_t)(a.step_base + t);
-    if (a.mode == 0) {
+    if (a.mode == 0 && a.proposal == 0) {
       for (int e = 0; e < NE; ++e) {
         double n3[3], u;
         oq_move_randoms(a.seed, (uint32_t)w, gstep, (uint32_t)e, n3, u);
@@ -411,6 +426,23 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
         const double nz = pos[(3 * e + 2) * WPB + tid] + a.step * n3[2];
         nacc += oq_try_move<NOCC, T, Real>(S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz, 0.0, u,
                                            logdet);
+      }
+    } else if (a.mode == 0) {
+      // nucleus-scaled Gaussian: sigma(x) = step * clamp(r_near(x)/r0, fmin, 1);
+      // exact MH with log q(x|x') - log q(x'|x) for the asymmetric proposal
+      for (int e = 0; e < NE; ++e) {
+        double n3[3], u;
+        oq_move_randoms(a.seed, (uint32_t)w, gstep, (uint32_t)e, n3, u);
+        const double ox = pos[(3 * e) * WPB + tid], oy = pos[(3 * e + 1) * WPB + tid],
+                     oz = pos[(3 * e + 2) * WPB + tid];
+        const double so = oq_scaled_width(S, ox, oy, oz, a.step, a.scale_r0, a.scale_fmin);
+        const double nx = ox + so * n3[0], ny = oy + so * n3[1], nz = oz + so * n3[2];
+        const double sn = oq_scaled_width(S, nx, ny, nz, a.step, a.scale_r0, a.scale_fmin);
+        const double d2 = (nx - ox) * (nx - ox) + (ny - oy) * (ny - oy) + (nz - oz) * (nz - oz);
+        const double log_extra =
+            3.0 * log(so / sn) + 0.5 * d2 * (1.0 / (so * so) - 1.0 / (sn * sn));
+        nacc += oq_try_move<NOCC, T, Real>(S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
+                                           log_extra, u, logdet);
       }
     } else {
       double n3[3], u;

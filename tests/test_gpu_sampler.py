@@ -146,3 +146,22 @@ def test_basin_moves_sample_psi_squared_h2():
     m_ref, se_ref, _, _ = O.binning_analysis(ser)
     z = abs(m_b - m_ref) / np.hypot(se_b, se_ref)
     assert z < 3.0, (m_b, se_b, m_ref, se_ref)
+
+
+@pytest.mark.parametrize("name", ["LiH", "H2O"])
+def test_scaled_proposal_preserves_distribution(name):
+    """The nucleus-scaled proposal with its exact MH correction samples the
+    same |psi|^2: energies agree with the fixed-width sampler."""
+    mf = M.make_mf(name)
+    s = build_system(mf, M.benchmark_params_corr(mf.mol))
+    res = {}
+    for kind in (0, 1):
+        ctx = GTOContext(s)
+        ctx.set_proposal(kind, 1.0, 0.05)
+        ens = WalkerEnsemble(ctx, seeded_walkers(s, 16384, 0.8, 4), "fp64", seed=21 + kind)
+        ens.run(1500, 0.5)
+        sums = ens.run(1500, 0.5).cpu().numpy()
+        res[kind] = O.binning_analysis(sums[:, 3] / sums[:, 6])
+        assert ctx.flags() == 0
+    z = abs(res[0][0] - res[1][0]) / np.hypot(res[0][1], res[1][1])
+    assert z < 3.0, res
