@@ -233,6 +233,9 @@ def run_ours(a):
     dev = torch.device("cuda", local)
     system = build_system(a.system)
     ctx = GTOContext(system)
+    t_spec = time.perf_counter()
+    ctx.specialize()                 # NVRTC-compiled kernels for this molecule
+    t_spec = time.perf_counter() - t_spec
     if a.proposal == "scaled":
         ctx.set_proposal(1, SCALED_R0, SCALED_FMIN)
     W = a.walkers
@@ -282,6 +285,7 @@ def run_ours(a):
     plain = None
     if a.precision != "fp64" or a.proposal != "plain":
         pctx = GTOContext(system)            # fixed-width Gaussian proposal
+        pctx.specialize()
         pe = WalkerEnsemble(pctx, ens.X, "fp64", seed=99 + rank, refresh_every=REFRESH_EVERY)
         pstep = adapt_step(pe, STEP_DEFAULT.get(a.system, 0.3))
         pe.run(500, pstep)
@@ -373,6 +377,7 @@ def run_ours(a):
                    "precision": a.precision, "walkers_per_gpu": W, "step": step,
                    "parallelism": f"replicas x{world}",
                    "trial": "RHF determinant + Pade J2 (b=3)",
+                   "kernels": f"NVRTC-specialised to the molecule (compile {t_spec:.1f} s, untimed)",
                    "proposal": (f"nucleus-scaled Gaussian (r0={SCALED_R0}, fmin={SCALED_FMIN}), "
                                 "exact MH" if a.proposal == "scaled" else "fixed-width Gaussian"),
                    "equilibration_sweeps": EQUIL_SWEEPS + 200,

@@ -182,6 +182,21 @@ int oqmc_sweeps_noalloc(oqmc_ctx* ctx, double* walkers, int W, int precision,
  * while core electrons move with core-sized steps. */
 int oqmc_set_proposal(oqmc_ctx* ctx, int kind, double r0, double fmin_frac);
 
+/* Per-system specialisation (no counterpart in the reference, whose jit
+ * unrolls the shell loop at trace time, OmegaQMC/psi/gto.py:1012-1186):
+ * generate the AO->MO evaluation of this molecule as straight-line code with
+ * exponents and coefficients compiled in, compile the move and local-energy
+ * kernels with NVRTC for sm_100a and use them from then on (enable = 0
+ * returns to the table-driven kernels).  Takes a few seconds; returns
+ * OQ_ERR_UNSUPPORTED when NVRTC is not available. */
+int oqmc_specialize(oqmc_ctx* ctx, int enable);
+
+/* The generated specialisation source (of a context, or of a descriptor
+ * without any device work): writes at most len-1 chars plus NUL into buf
+ * and returns the full length (or a negative OQ_ERR_* code). */
+int oqmc_spec_source(const oqmc_ctx* ctx, char* buf, size_t len);
+int oqmc_spec_source_desc(const oqmc_system_desc* desc, char* buf, size_t len);
+
 /* Exponent threshold above which an exponent group is evaluated in FP64
  * near its nucleus in the mixed build (default 50.0; <= 0 disables). */
 int oqmc_set_split(oqmc_ctx* ctx, double tight_alpha);

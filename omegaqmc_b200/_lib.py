@@ -79,6 +79,9 @@ _SIGS = [
                                     c_double, c_uint64, c_uint64, c_void_p, c_void_p,
                                     c_void_p, c_void_p]),
     ("oqmc_set_proposal", c_int, [c_void_p, c_int, c_double, c_double]),
+    ("oqmc_specialize", c_int, [c_void_p, c_int]),
+    ("oqmc_spec_source", c_int, [c_void_p, ctypes.c_char_p, c_size_t]),
+    ("oqmc_spec_source_desc", c_int, [ctypes.POINTER(SystemDesc), ctypes.c_char_p, c_size_t]),
     ("oqmc_set_split", c_int, [c_void_p, c_double]),
     ("oqmc_get_flags", c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint), c_int, c_void_p]),
     ("oqmc_measure_peak", c_int, [c_int, P_double, c_void_p]),

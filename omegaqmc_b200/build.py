@@ -53,6 +53,29 @@ def _run(cmd):
     return r
 
 
+RTC_HEADERS = ("oqmc_common.cuh", "oqmc_ao.cuh", "oqmc_eval.cuh", "oqmc_sweep.cuh")
+
+
+def _embed_headers():
+    """Write _build/oqmc_rtc_src.inc: the kernel headers as string literals for
+    the run-time (NVRTC) specialisation."""
+    out = ["// generated by omegaqmc_b200/build.py from csrc/*.cuh", "#pragma once",
+           f"static const int kOqRtcCount = {len(RTC_HEADERS)};",
+           "static const char* const kOqRtcNames[] = {" +
+           ", ".join(f'"{h}"' for h in RTC_HEADERS) + "};",
+           "static const char* const kOqRtcSrcs[] = {"]
+    for h in RTC_HEADERS:
+        txt = open(os.path.join(CSRC, h)).read()
+        assert ")OQRTC\"" not in txt
+        out.append('R"OQRTC(' + txt + ')OQRTC",')
+    out.append("};")
+    path = os.path.join(BUILD, "oqmc_rtc_src.inc")
+    new = "\n".join(out) + "\n"
+    if not os.path.exists(path) or open(path).read() != new:
+        with open(path, "w") as f:
+            f.write(new)
+
+
 def build(force=False, jobs=None, verbose=False):
     """Compile and link the library; returns its path."""
     nvcc = _nvcc()
@@ -63,9 +86,12 @@ def build(force=False, jobs=None, verbose=False):
             and open(stamp).read().strip() == key):
         return LIB
     jobs = jobs or max(1, min(len(NOCC_LIST) + 1, os.cpu_count() or 4))
+    _embed_headers()
     units = [(os.path.join(CSRC, "oqmc.cu"), os.path.join(BUILD, "oqmc.o"), []),
              (os.path.join(CSRC, "oqmc_peak.cu"), os.path.join(BUILD, "oqmc_peak.o"), []),
-             (os.path.join(CSRC, "oqmc_noalloc.cu"), os.path.join(BUILD, "oqmc_noalloc.o"), [])]
+             (os.path.join(CSRC, "oqmc_noalloc.cu"), os.path.join(BUILD, "oqmc_noalloc.o"), []),
+             (os.path.join(CSRC, "oqmc_rtc.cu"), os.path.join(BUILD, "oqmc_rtc.o"),
+              ["-I" + BUILD])]
     for n in NOCC_LIST:
         units.append((os.path.join(CSRC, "oqmc_inst.cu"),
                       os.path.join(BUILD, f"oqmc_inst_{n}.o"), [f"-DOQ_N={n}"]))
@@ -83,7 +109,7 @@ def build(force=False, jobs=None, verbose=False):
         for r in results:
             print(r.stderr)
     tmp = LIB + ".tmp"
-    _run([nvcc] + ARCH + ["-shared", "-o", tmp] + [u[1] for u in units] + ["-lcudart"])
+    _run([nvcc] + ARCH + ["-shared", "-o", tmp] + [u[1] for u in units] + ["-lcudart", "-ldl"])
     os.replace(tmp, LIB)
     with open(stamp, "w") as f:
         f.write(key)

@@ -203,6 +203,11 @@ class GTOContext:
             float(sigma), ctypes.c_uint64(seed & (2**64 - 1)), ctypes.c_uint64(step_base),
             _dptr(acc_sum), _stream_ptr(stream)))
 
+    def specialize(self, enable=True):
+        """Compile (NVRTC) and use kernels specialised to this system's basis
+        and orbitals; raises NotImplementedError where NVRTC is unavailable."""
+        self._check(self.lib.oqmc_specialize(self._h, int(enable)))
+
     def set_proposal(self, kind, r0=1.0, fmin_frac=0.05):
         """0: fixed-width Gaussian (reference); 1: nucleus-scaled width."""
         self._check(self.lib.oqmc_set_proposal(self._h, int(kind), float(r0), float(fmin_frac)))

@@ -4,10 +4,12 @@
 #include <cstdlib>
 #include <cstring>
 #include <cmath>
+#include <string>
 #include <vector>
 #include <cuda_runtime.h>
 
 #include "oqmc_launch.h"
+#include "oqmc_rtc.h"
 #include "../../include/oqmc_b200.h"
 
 struct oqmc_ctx {
@@ -22,6 +24,8 @@ struct oqmc_ctx {
   unsigned* d_flags;
   double tight_alpha;
   int proposal;           // 0 fixed-width Gaussian, 1 nucleus-scaled width
+  OqSpecModule* spec;     // run-time specialised kernels, or null
+  double* h_C;            // host copy of the MO coefficients (for specialisation)
   double scale_r0, scale_fmin;
   char err[512];
 };
@@ -144,9 +148,9 @@ const char* oqmc_version(void) { return "oqmc_b200 0.1.0 (sm_100a)"; }
 
 const char* oqmc_last_error(const oqmc_ctx* ctx) { return ctx ? ctx->err : g_create_err; }
 
-int oqmc_create(oqmc_ctx** out, const oqmc_system_desc* d) {
-  if (!out || !d) return set_err(nullptr, OQ_ERR_ARG, "null argument%s");
-  *out = nullptr;
+// Validate a descriptor and fill the device system tables (host side only).
+static int fill_system(const oqmc_system_desc* d, OqSystem& S) {
+  if (!d) return set_err(nullptr, OQ_ERR_ARG, "null argument%s");
   if (d->natm < 1 || d->natm > OQ_MAX_NUC)
     return set_err(nullptr, OQ_ERR_UNSUPPORTED, "natm out of range (1..16)%s");
   if (d->n_e != 2 * d->nocc)
@@ -158,10 +162,7 @@ int oqmc_create(oqmc_ctx** out, const oqmc_system_desc* d) {
     return set_err(nullptr, OQ_ERR_UNSUPPORTED, "nbf out of range%s");
   if (d->ngroup < 1 || d->ngroup > OQ_MAX_GROUP)
     return set_err(nullptr, OQ_ERR_UNSUPPORTED, "too many exponent groups%s");
-  oqmc_ctx* ctx = new (std::nothrow) oqmc_ctx();
-  if (!ctx) return set_err(nullptr, OQ_ERR_NOMEM, "out of host memory%s");
-  memset(&ctx->hsys, 0, sizeof(OqSystem));
-  OqSystem& S = ctx->hsys;
+  memset(&S, 0, sizeof(OqSystem));
   S.natm = d->natm; S.nbf = d->nbf; S.nocc = d->nocc; S.n_e = d->n_e;
   S.ngroup = d->ngroup; S.has_j1 = d->has_j1; S.has_j2 = d->has_j2; S.cusp = d->cusp;
   S.e_nn = d->e_nn;
@@ -180,10 +181,8 @@ int oqmc_create(oqmc_ctx** out, const oqmc_system_desc* d) {
     const int np = d->group_nprim[g], nc = d->group_ncol[g], am = d->group_am[g];
     const int ia = d->group_atom[g];
     if (np < 1 || nc < 1 || nc > OQ_MAX_COL || am < 0 || am > 4 || ia < 0 || ia >= d->natm ||
-        prim + np > OQ_MAX_PRIM || shell + nc > OQ_MAX_SHELL || normo + np * nc > OQ_MAX_NORM) {
-      delete ctx;
+        prim + np > OQ_MAX_PRIM || shell + nc > OQ_MAX_SHELL || normo + np * nc > OQ_MAX_NORM)
       return set_err(nullptr, OQ_ERR_UNSUPPORTED, "basis group out of supported range%s");
-    }
     S.g_iat[g] = ia; S.g_off[g] = prim; S.g_n[g] = np; S.g_shell0[g] = shell;
     S.g_ncol[g] = nc; S.g_am[g] = am;
     for (int p = 0; p < np; ++p) S.alpha[prim + p] = d->alpha[prim + p];
@@ -200,18 +199,61 @@ int oqmc_create(oqmc_ctx** out, const oqmc_system_desc* d) {
   }
   S.nshell = shell;
   S.nprim_total = prim;
-  if (ao != d->nbf) {
-    delete ctx;
-    return set_err(nullptr, OQ_ERR_ARG, "group table does not add up to nbf AOs%s");
+  if (ao != d->nbf) return set_err(nullptr, OQ_ERR_ARG, "group table does not add up to nbf AOs%s");
+  build_harm_table(S.harm);
+  return OQ_OK;
+}
+
+static void split_for(const OqSystem& S, double tight_alpha, OqSplit& sp) {
+  for (int g = 0; g < OQ_MAX_GROUP; ++g) sp.r2[g] = 0.0;
+  if (!(tight_alpha > 0.0)) return;
+  for (int g = 0; g < S.ngroup; ++g) {
+    double r2 = 0.0;
+    for (int p = 0; p < S.g_n[g]; ++p) {
+      const double a = S.alpha[S.g_off[g] + p];
+      if (a > tight_alpha) r2 = fmax(r2, 25.0 / a);
+    }
+    sp.r2[g] = r2;
   }
+}
+
+extern "C" int oqmc_spec_source_desc(const oqmc_system_desc* d, char* buf, size_t len) {
+  OqSystem* S = new (std::nothrow) OqSystem();
+  if (!S) return OQ_ERR_NOMEM;
+  int rc = fill_system(d, *S);
+  if (rc != OQ_OK) { delete S; return rc; }
+  OqSplit sp;
+  split_for(*S, 50.0, sp);
+  const std::string src = oq_spec_source(*S, sp, d->C, d->nocc);
+  delete S;
+  if (buf && len) {
+    const size_t n = src.size() < len - 1 ? src.size() : len - 1;
+    memcpy(buf, src.data(), n);
+    buf[n] = 0;
+  }
+  return (int)src.size();
+}
+
+extern "C" int oqmc_create(oqmc_ctx** out, const oqmc_system_desc* d) {
+  if (!out || !d) return set_err(nullptr, OQ_ERR_ARG, "null argument%s");
+  *out = nullptr;
+  oqmc_ctx* ctx = new (std::nothrow) oqmc_ctx();
+  if (!ctx) return set_err(nullptr, OQ_ERR_NOMEM, "out of host memory%s");
+  {
+    const int rc = fill_system(d, ctx->hsys);
+    if (rc != OQ_OK) { delete ctx; return rc; }
+  }
+  OqSystem& S = ctx->hsys;
   ctx->nocc = d->nocc; ctx->n_e = d->n_e; ctx->nbf = d->nbf; ctx->natm = d->natm;
   ctx->tight_alpha = 50.0;
   ctx->proposal = 0;
+  ctx->spec = nullptr;
+  ctx->h_C = new double[(size_t)d->nbf * d->nocc];
+  memcpy(ctx->h_C, d->C, sizeof(double) * (size_t)d->nbf * d->nocc);
   ctx->scale_r0 = 1.0;
   ctx->scale_fmin = 0.05;
   compute_split(ctx);
   cudaGetDevice(&ctx->device);
-  build_harm_table(S.harm);
   std::vector<float> c32((size_t)d->nbf * d->nocc);
   for (size_t i = 0; i < c32.size(); ++i) c32[i] = (float)d->C[i];
   cudaError_t e = cudaSuccess;
@@ -236,6 +278,8 @@ int oqmc_create(oqmc_ctx** out, const oqmc_system_desc* d) {
 
 int oqmc_destroy(oqmc_ctx* ctx) {
   if (!ctx) return OQ_OK;
+  oq_spec_destroy(ctx->spec);
+  delete[] ctx->h_C;
   cudaFree(ctx->d_sys);
   cudaFree(ctx->d_split);
   cudaFree(ctx->d_C64);
@@ -254,10 +298,38 @@ int oqmc_set_proposal(oqmc_ctx* ctx, int kind, double r0, double fmin_frac) {
   return OQ_OK;
 }
 
+int oqmc_specialize(oqmc_ctx* ctx, int enable) {
+  if (!ctx) return OQ_ERR_ARG;
+  oq_spec_destroy(ctx->spec);
+  ctx->spec = nullptr;
+  if (!enable) return OQ_OK;
+  std::string err;
+  OqSpecModule* m = nullptr;
+  if (oq_spec_build(ctx->hsys, ctx->hsplit, ctx->h_C, ctx->nocc, &m, &err) != 0)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED, "specialisation unavailable: %s", err.c_str());
+  ctx->spec = m;
+  return OQ_OK;
+}
+
+int oqmc_spec_source(const oqmc_ctx* ctx, char* buf, size_t len) {
+  if (!ctx) return OQ_ERR_ARG;
+  const std::string s = oq_spec_source(ctx->hsys, ctx->hsplit, ctx->h_C, ctx->nocc);
+  if (buf && len) {
+    const size_t n = s.size() < len - 1 ? s.size() : len - 1;
+    memcpy(buf, s.data(), n);
+    buf[n] = 0;
+  }
+  return (int)s.size();
+}
+
 int oqmc_set_split(oqmc_ctx* ctx, double tight_alpha) {
   if (!ctx) return OQ_ERR_ARG;
   ctx->tight_alpha = tight_alpha;
   compute_split(ctx);
+  if (ctx->spec) {   // the specialised kernels carry the split radii as literals
+    const int rc = oqmc_specialize(ctx, 1);
+    if (rc != OQ_OK) return rc;
+  }
   OQ_CUDA(ctx, cudaMemcpy(ctx->d_split, &ctx->hsplit, sizeof(OqSplit), cudaMemcpyHostToDevice));
   return OQ_OK;
 }
@@ -418,6 +490,15 @@ static int launch_moves(oqmc_ctx* ctx, const OqMoveArgs& m, int wpb, size_t sm, 
                         void* stream) {
   const OqLaunch L = make_launch(ctx, stream, sm);
   const int mixed = precision == OQ_PREC_MIXED;
+  if (ctx->spec) {
+    OqMoveArgs mm = m;
+    const void* C = mixed ? (const void*)ctx->d_C32 : (const void*)ctx->d_C64;
+    void* args[4] = {(void*)&L.sys, (void*)&L.split, (void*)&C, (void*)&mm};
+    if (oq_spec_launch(ctx->spec, mixed ? 1 : 0, dim3((m.W + wpb - 1) / wpb), dim3(wpb), sm,
+                       L.stream, args) != 0)
+      return set_err(ctx, OQ_ERR_CUDA, "specialised move kernel launch failed%s");
+    return OQ_OK;
+  }
   cudaError_t err = cudaSuccess;
 #define OQ_X(N) err = oq_moves_##N(L, m, wpb, mixed)
   OQ_SWITCH(ctx->nocc, OQ_X)
@@ -466,6 +547,15 @@ int oqmc_sweeps(oqmc_ctx* ctx, double* X, int W, void* state, int precision, int
     el.sums = sums + (size_t)k * OQ_NSUM;
     el.el_trace = el_trace ? el_trace + (size_t)k * W : nullptr;
     el.eparts = (k == n_meas - 1) ? eparts_last : nullptr;
+    if (ctx->spec) {
+      OqElocArgs ee = el;
+      const void* C = mixed ? (const void*)ctx->d_C32 : (const void*)ctx->d_C64;
+      void* args[4] = {(void*)&Le.sys, (void*)&Le.split, (void*)&C, (void*)&ee};
+      if (oq_spec_launch(ctx->spec, mixed ? 3 : 2, dim3((W + 31) / 32), dim3(32, ctx->n_e),
+                         Le.smem, Le.stream, args) != 0)
+        return set_err(ctx, OQ_ERR_CUDA, "specialised local-energy kernel launch failed%s");
+      continue;
+    }
     cudaError_t err = cudaSuccess;
 #define OQ_X(N) err = oq_eloc_##N(Le, el, mixed)
     OQ_SWITCH(ctx->nocc, OQ_X)

@@ -6,8 +6,17 @@
 // laid out walker-minor ("structure of arrays") wherever consecutive threads
 // handle consecutive walkers, so global accesses coalesce.
 #pragma once
+#ifdef __CUDACC_RTC__
+// run-time compilation (NVRTC): no host headers
+typedef unsigned int uint32_t;
+typedef unsigned long long uint64_t;
+#ifndef INFINITY
+#define INFINITY __longlong_as_double(0x7ff0000000000000ULL)
+#endif
+#else
 #include <cstdint>
 #include <cuda_runtime.h>
+#endif
 
 #define OQ_MAX_NUC 16
 #define OQ_MAX_GROUP 96

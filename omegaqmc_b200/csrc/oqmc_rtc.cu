@@ -1,0 +1,388 @@
+// Per-system kernel specialisation.
+//
+// oqmc_specialize() writes a basis policy for the context's molecule as
+// straight-line CUDA: one displacement per nucleus, every exponential of every
+// exponent group, the contraction sums and the MO accumulation with the
+// exponents, normalised contraction coefficients and MO coefficients as
+// literals (zero MO coefficients dropped).  NVRTC compiles the move and
+// local-energy kernels with that policy for sm_100a and the driver API loads
+// them; the sweep entry points then launch these instead of the table-driven
+// kernels.  NVRTC and the driver library are opened with dlopen, so the
+// library loads (and runs its table-driven kernels) where NVRTC is absent.
+#include <cstdio>
+#include <cstring>
+#include <dlfcn.h>
+#include <mutex>
+#include <string>
+#include <vector>
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <nvrtc.h>
+
+#include "oqmc_rtc.h"
+#include "oqmc_rtc_src.inc"   // generated: the kernel headers as strings
+
+namespace {
+
+struct Api {
+  bool ok = false;
+  std::string err;
+  nvrtcResult (*CreateProgram)(nvrtcProgram*, const char*, const char*, int, const char* const*,
+                               const char* const*);
+  nvrtcResult (*AddNameExpression)(nvrtcProgram, const char*);
+  nvrtcResult (*CompileProgram)(nvrtcProgram, int, const char* const*);
+  nvrtcResult (*GetProgramLogSize)(nvrtcProgram, size_t*);
+  nvrtcResult (*GetProgramLog)(nvrtcProgram, char*);
+  nvrtcResult (*GetCUBINSize)(nvrtcProgram, size_t*);
+  nvrtcResult (*GetCUBIN)(nvrtcProgram, char*);
+  nvrtcResult (*GetLoweredName)(nvrtcProgram, const char*, const char**);
+  nvrtcResult (*DestroyProgram)(nvrtcProgram*);
+  CUresult (*ModuleLoadData)(CUmodule*, const void*);
+  CUresult (*ModuleGetFunction)(CUfunction*, CUmodule, const char*);
+  CUresult (*ModuleUnload)(CUmodule);
+  CUresult (*FuncSetAttribute)(CUfunction, CUfunction_attribute, int);
+  CUresult (*LaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned,
+                           unsigned, unsigned, CUstream, void**, void**);
+};
+
+Api g_api;
+std::once_flag g_api_once;
+
+template <typename F>
+bool sym(void* h, const char* name, F& f) {
+  f = reinterpret_cast<F>(dlsym(h, name));
+  return f != nullptr;
+}
+
+void load_api() {
+  const char* nv_names[] = {"libnvrtc.so.12", "libnvrtc.so", "/usr/local/cuda/lib64/libnvrtc.so.12",
+                            "/usr/local/cuda/lib64/libnvrtc.so"};
+  void* nv = nullptr;
+  for (const char* n : nv_names)
+    if ((nv = dlopen(n, RTLD_NOW | RTLD_LOCAL))) break;
+  void* cu = dlopen("libcuda.so.1", RTLD_NOW | RTLD_LOCAL);
+  if (!nv || !cu) {
+    g_api.err = !nv ? "NVRTC (libnvrtc.so.12) not found" : "libcuda.so.1 not found";
+    return;
+  }
+  Api& a = g_api;
+  bool ok = sym(nv, "nvrtcCreateProgram", a.CreateProgram) &&
+            sym(nv, "nvrtcAddNameExpression", a.AddNameExpression) &&
+            sym(nv, "nvrtcCompileProgram", a.CompileProgram) &&
+            sym(nv, "nvrtcGetProgramLogSize", a.GetProgramLogSize) &&
+            sym(nv, "nvrtcGetProgramLog", a.GetProgramLog) &&
+            sym(nv, "nvrtcGetCUBINSize", a.GetCUBINSize) &&
+            sym(nv, "nvrtcGetCUBIN", a.GetCUBIN) &&
+            sym(nv, "nvrtcGetLoweredName", a.GetLoweredName) &&
+            sym(nv, "nvrtcDestroyProgram", a.DestroyProgram) &&
+            sym(cu, "cuModuleLoadData", a.ModuleLoadData) &&
+            sym(cu, "cuModuleGetFunction", a.ModuleGetFunction) &&
+            sym(cu, "cuModuleUnload", a.ModuleUnload) &&
+            sym(cu, "cuFuncSetAttribute", a.FuncSetAttribute) &&
+            sym(cu, "cuLaunchKernel", a.LaunchKernel);
+  if (!ok) {
+    a.err = "missing NVRTC or driver symbol";
+    return;
+  }
+  a.ok = true;
+}
+
+// ---------------------------------------------------------------------------
+// source generation
+// ---------------------------------------------------------------------------
+struct Gen {
+  const OqSystem& S;
+  const OqSplit& SP;
+  const double* C;     // nbf x nocc
+  int nocc;
+  std::string o;
+  void add(const std::string& s) { o += s; }
+
+  static std::string num(double v) {
+    char b[40];
+    snprintf(b, sizeof b, "%.17g", v);
+    std::string s(b);
+    if (s.find_first_of(".eEn") == std::string::npos) s += ".0";
+    return s;
+  }
+
+  // declare R<k> (and Rp<k>, Rl<k>) of type ty and accumulate group g
+  void radial(int g, bool vgl, const std::string& ty, const char* r2) {
+    const int np = S.g_n[g], nc = S.g_ncol[g], off = S.g_off[g], sh0 = S.g_shell0[g];
+    for (int k = 0; k < nc; ++k) {
+      const std::string ks = std::to_string(k);
+      add("      " + ty + " R" + ks + " = 0");
+      if (vgl) add(", Rp" + ks + " = 0, Rl" + ks + " = 0");
+      add(";\n");
+    }
+    const std::string ex = (ty == "double") ? "exp" : "oq_exp<T>";
+    for (int p = 0; p < np; ++p) {
+      const std::string al = "((" + ty + ")" + num(S.alpha[off + p]) + ")";
+      add("      { const " + ty + " e = " + ex + "(-" + al + " * " + r2 + ");\n");
+      if (vgl) {
+        add("        const " + ty + " fp = (" + ty + ")-2 * " + al + " * e;\n");
+        add("        const " + ty + " fl = ((" + ty + ")4 * " + al + " * " + al + " * " + r2 +
+            " - (" + ty + ")6 * " + al + ") * e;\n");
+      }
+      for (int k = 0; k < nc; ++k) {
+        const std::string nl = "((" + ty + ")" + num(S.norm[S.s_norm[sh0 + k] + p]) + ")";
+        const std::string ks = std::to_string(k);
+        add("        R" + ks + " += " + nl + " * e;");
+        if (vgl) add(" Rp" + ks + " += " + nl + " * fp; Rl" + ks + " += " + nl + " * fl;");
+        add("\n");
+      }
+      add("      }\n");
+    }
+  }
+
+  // accumulate one AO into the MOs (value expression v; grad g[3], lap l)
+  void accum(int ao, const std::string& v, const std::string* g, const std::string* l) {
+    for (int m = 0; m < nocc; ++m) {
+      const double c = C[ao * nocc + m];
+      if (c == 0.0) continue;
+      const std::string cl = "(T)(" + num(c) + ")", ms = std::to_string(m);
+      add("      mv[" + ms + "] += " + cl + " * " + v + ";\n");
+      if (g) {
+        add("      mg[" + ms + "][0] += " + cl + " * " + g[0] + "; mg[" + ms + "][1] += " + cl +
+            " * " + g[1] + "; mg[" + ms + "][2] += " + cl + " * " + g[2] + ";\n");
+        add("      ml[" + ms + "] += " + cl + " * " + *l + ";\n");
+      }
+    }
+  }
+
+  // angular factors of column k of group g; radial names R, Rp, Rl
+  void angular(int g, int k, bool vgl, const std::string& R, const std::string& Rp,
+               const std::string& Rl) {
+    const int am = S.g_am[g];
+    const int ao = S.s_ao[S.g_shell0[g] + k];
+    add("    {\n");
+    if (am == 0) {
+      if (!vgl) {
+        accum(ao, R, nullptr, nullptr);
+      } else {
+        std::string gg[3] = {"(" + Rp + " * dx)", "(" + Rp + " * dy)", "(" + Rp + " * dz)"};
+        accum(ao, R, gg, &Rl);
+      }
+    } else {
+      if (vgl) add("      const T lfac = " + Rl + " + (T)" + std::to_string(2 * am) + " * " + Rp + ";\n");
+      if (am == 2) add("      T Y[5], dY[5][3]; oq_harm_d<T>(dx, dy, dz, Y, dY);\n");
+      for (int c = 0; c < 2 * am + 1; ++c) {
+        const std::string cs = std::to_string(c);
+        std::string Y, d0, d1, d2;
+        if (am == 1) {
+          Y = c == 0 ? "dx" : c == 1 ? "dy" : "dz";
+          d0 = c == 0 ? "(T)1" : "(T)0"; d1 = c == 1 ? "(T)1" : "(T)0"; d2 = c == 2 ? "(T)1" : "(T)0";
+        } else if (am == 2) {
+          Y = "Y[" + cs + "]"; d0 = "dY[" + cs + "][0]"; d1 = "dY[" + cs + "][1]"; d2 = "dY[" + cs + "][2]";
+        } else {
+          add("      T Y" + cs + ", dY" + cs + "[3]; oq_harm_table<T>(S.harm, " + std::to_string(am) +
+              ", " + cs + ", dx, dy, dz, Y" + cs + ", dY" + cs + ");\n");
+          Y = "Y" + cs; d0 = "dY" + cs + "[0]"; d1 = "dY" + cs + "[1]"; d2 = "dY" + cs + "[2]";
+        }
+        if (!vgl) {
+          accum(ao + c, "(" + R + " * " + Y + ")", nullptr, nullptr);
+        } else {
+          std::string gg[3] = {"(" + Rp + " * dx * " + Y + " + " + R + " * " + d0 + ")",
+                               "(" + Rp + " * dy * " + Y + " + " + R + " * " + d1 + ")",
+                               "(" + Rp + " * dz * " + Y + " + " + R + " * " + d2 + ")"};
+          std::string ll = "(lfac * " + Y + ")";
+          accum(ao + c, "(" + R + " * " + Y + ")", gg, &ll);
+        }
+      }
+    }
+    add("    }\n");
+  }
+
+  void body(bool vgl) {
+    for (int m = 0; m < nocc; ++m) {
+      const std::string ms = std::to_string(m);
+      add("  mv[" + ms + "] = (T)0;");
+      if (vgl)
+        add(" mg[" + ms + "][0] = (T)0; mg[" + ms + "][1] = (T)0; mg[" + ms + "][2] = (T)0; ml[" +
+            ms + "] = (T)0;");
+      add("\n");
+    }
+    for (int ia = 0; ia < S.natm; ++ia) {
+      bool any = false;
+      for (int g = 0; g < S.ngroup; ++g) any = any || S.g_iat[g] == ia;
+      if (!any) continue;
+      add("  {\n  const double dxd = x - (" + num(S.nuc[ia][0]) + "), dyd = y - (" +
+          num(S.nuc[ia][1]) + "), dzd = z - (" + num(S.nuc[ia][2]) + ");\n"
+          "  const double r2d = dxd * dxd + dyd * dyd + dzd * dzd;\n"
+          "  const T dx = (T)dxd, dy = (T)dyd, dz = (T)dzd, r2 = (T)r2d;\n  (void)r2;\n");
+      for (int g = 0; g < S.ngroup; ++g) {
+        if (S.g_iat[g] != ia) continue;
+        const int nc = S.g_ncol[g], sh0 = S.g_shell0[g];
+        const bool s_shell = S.g_am[g] == 0;
+        add("  {\n");
+        if (!vgl) {
+          radial(g, false, "T", "r2");
+          for (int k = 0; k < nc; ++k)
+            if (s_shell && S.s_cusp[sh0 + k])
+              add("    R" + std::to_string(k) + " = (T)oq_cusp_val(S, " + std::to_string(ia) +
+                  ", sqrt(r2d), (double)R" + std::to_string(k) + ");\n");
+          for (int k = 0; k < nc; ++k) {
+            const std::string ks = std::to_string(k);
+            angular(g, k, false, "R" + ks, "", "");
+          }
+        } else {
+          bool cusp = false;
+          for (int k = 0; k < nc; ++k) cusp = cusp || (s_shell && S.s_cusp[sh0 + k]);
+          for (int k = 0; k < nc; ++k) {
+            const std::string ks = std::to_string(k);
+            add("    T RT" + ks + ", RpT" + ks + ", RlT" + ks + ";\n");
+          }
+          add("    if (sizeof(T) == 8 || r2d < " + num(SP.r2[g]) + (cusp ? " || true" : "") +
+              ") {\n      {\n");
+          radial(g, true, "double", "r2d");
+          for (int k = 0; k < nc; ++k) {
+            const std::string ks = std::to_string(k);
+            if (s_shell && S.s_cusp[sh0 + k])
+              add("      oq_cusp_vgl(S, " + std::to_string(ia) + ", sqrt(r2d), R" + ks + ", Rp" + ks +
+                  ", Rl" + ks + ");\n");
+            add("      RT" + ks + " = (T)R" + ks + "; RpT" + ks + " = (T)Rp" + ks + "; RlT" + ks +
+                " = (T)Rl" + ks + ";\n");
+          }
+          add("      }\n    } else {\n      {\n");
+          radial(g, true, "T", "r2");
+          for (int k = 0; k < nc; ++k) {
+            const std::string ks = std::to_string(k);
+            add("      RT" + ks + " = R" + ks + "; RpT" + ks + " = Rp" + ks + "; RlT" + ks + " = Rl" +
+                ks + ";\n");
+          }
+          add("      }\n    }\n");
+          for (int k = 0; k < nc; ++k) {
+            const std::string ks = std::to_string(k);
+            angular(g, k, true, "RT" + ks, "RpT" + ks, "RlT" + ks);
+          }
+        }
+        add("  }\n");
+      }
+      add("  }\n");
+    }
+  }
+};
+
+std::string generate(const OqSystem& S, const OqSplit& SP, const double* C, int nocc) {
+  std::string src = "#include \"oqmc_sweep.cuh\"\n\nstruct OqSpecBasis {\n";
+  {
+    Gen g{S, SP, C, nocc, ""};
+    g.body(false);
+    src += "  template <typename T, typename TC>\n"
+           "  __device__ static __forceinline__ void mo_val(const OqSystem& S, const OqSplit& SP,\n"
+           "      const TC* __restrict__ C, double x, double y, double z, T* mv) {\n"
+           "  (void)SP; (void)C;\n";
+    src += g.o + "  }\n\n";
+  }
+  {
+    Gen g{S, SP, C, nocc, ""};
+    g.body(true);
+    std::string b = g.o;
+    src += "  template <typename T, typename TC>\n"
+           "  __device__ static __forceinline__ void mo_vgl(const OqSystem& S, const OqSplit& SP,\n"
+           "      const TC* __restrict__ C, double x, double y, double z, T* mv, T (*mg)[3],\n"
+           "      T* ml) {\n  (void)SP; (void)C;\n";
+    src += b + "  }\n";
+  }
+  src += "};\n";
+  return src;
+}
+
+}  // namespace
+
+struct OqSpecModule {
+  CUmodule mod = nullptr;
+  CUfunction fn[4] = {nullptr, nullptr, nullptr, nullptr};  // moves d/f, eloc d/f
+};
+
+int oq_spec_build(const OqSystem& S, const OqSplit& SP, const double* C, int nocc,
+                  OqSpecModule** out, std::string* err) {
+  std::call_once(g_api_once, load_api);
+  if (!g_api.ok) {
+    *err = g_api.err;
+    return -1;
+  }
+  const Api& A = g_api;
+  std::string src = generate(S, SP, C, nocc);
+  std::vector<const char*> hdr_src, hdr_name;
+  for (int i = 0; i < kOqRtcCount; ++i) {
+    hdr_src.push_back(kOqRtcSrcs[i]);
+    hdr_name.push_back(kOqRtcNames[i]);
+  }
+  nvrtcProgram prog;
+  if (A.CreateProgram(&prog, src.c_str(), "oqmc_spec.cu", kOqRtcCount, hdr_src.data(),
+                      hdr_name.data()) != NVRTC_SUCCESS) {
+    *err = "nvrtcCreateProgram failed";
+    return -1;
+  }
+  char names[4][128];
+  snprintf(names[0], 128, "k_moves<%d, double, double, OqSpecBasis>", nocc);
+  snprintf(names[1], 128, "k_moves<%d, float, float, OqSpecBasis>", nocc);
+  snprintf(names[2], 128, "k_eloc<%d, double, double, OqSpecBasis>", nocc);
+  snprintf(names[3], 128, "k_eloc<%d, float, float, OqSpecBasis>", nocc);
+  for (auto& n : names) A.AddNameExpression(prog, n);
+  const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-lineinfo",
+                        "--device-as-default-execution-space"};
+  const nvrtcResult rc = A.CompileProgram(prog, 4, opts);
+  if (rc != NVRTC_SUCCESS) {
+    size_t n = 0;
+    A.GetProgramLogSize(prog, &n);
+    std::string log(n, '\0');
+    A.GetProgramLog(prog, &log[0]);
+    *err = "NVRTC compile failed: " + log.substr(0, 2000);
+    A.DestroyProgram(&prog);
+    return -1;
+  }
+  size_t nb = 0;
+  A.GetCUBINSize(prog, &nb);
+  std::vector<char> cubin(nb);
+  A.GetCUBIN(prog, cubin.data());
+  std::string lowered[4];
+  for (int i = 0; i < 4; ++i) {
+    const char* ln = nullptr;
+    A.GetLoweredName(prog, names[i], &ln);
+    lowered[i] = ln ? ln : "";
+  }
+  A.DestroyProgram(&prog);
+  OqSpecModule* m = new OqSpecModule();
+  if (A.ModuleLoadData(&m->mod, cubin.data()) != CUDA_SUCCESS) {
+    delete m;
+    *err = "cuModuleLoadData failed";
+    return -1;
+  }
+  for (int i = 0; i < 4; ++i) {
+    if (A.ModuleGetFunction(&m->fn[i], m->mod, lowered[i].c_str()) != CUDA_SUCCESS) {
+      A.ModuleUnload(m->mod);
+      delete m;
+      *err = "cuModuleGetFunction failed";
+      return -1;
+    }
+    A.FuncSetAttribute(m->fn[i], CU_FUNC_ATTRIBUTE_PREFERRED_SHARED_MEMORY_CARVEOUT, 100);
+  }
+  *out = m;
+  return 0;
+}
+
+void oq_spec_destroy(OqSpecModule* m) {
+  if (!m) return;
+  if (g_api.ok && m->mod) g_api.ModuleUnload(m->mod);
+  delete m;
+}
+
+int oq_spec_launch(OqSpecModule* m, int which, dim3 grid, dim3 block, size_t smem,
+                   cudaStream_t stream, void** args) {
+  const Api& A = g_api;
+  CUfunction f = m->fn[which];
+  if (smem > 48 * 1024 &&
+      A.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem) !=
+          CUDA_SUCCESS)
+    return -1;
+  return A.LaunchKernel(f, grid.x, grid.y, grid.z, block.x, block.y, block.z, (unsigned)smem,
+                        (CUstream)stream, args, nullptr) == CUDA_SUCCESS
+             ? 0
+             : -1;
+}
+
+std::string oq_spec_source(const OqSystem& S, const OqSplit& SP, const double* C, int nocc) {
+  return generate(S, SP, C, nocc);
+}

@@ -1,0 +1,17 @@
+// Run-time specialised kernels (see oqmc_rtc.cu).
+#pragma once
+#include <string>
+#include <cuda_runtime.h>
+#include "oqmc_sweep.cuh"
+
+struct OqSpecModule;
+
+// Generate, compile (NVRTC, sm_100a) and load the specialised move and
+// local-energy kernels of one system.  Returns 0 or -1 with *err set.
+int oq_spec_build(const OqSystem& S, const OqSplit& SP, const double* C, int nocc,
+                  OqSpecModule** out, std::string* err);
+void oq_spec_destroy(OqSpecModule* m);
+// which: 0 = moves FP64, 1 = moves mixed, 2 = local energy FP64, 3 = mixed
+int oq_spec_launch(OqSpecModule* m, int which, dim3 grid, dim3 block, size_t smem,
+                   cudaStream_t stream, void** args);
+std::string oq_spec_source(const OqSystem& S, const OqSplit& SP, const double* C, int nocc);

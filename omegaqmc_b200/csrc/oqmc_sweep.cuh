@@ -200,6 +200,26 @@ __device__ __forceinline__ void oq_mo_vgl_t(const OqSystem& S, const OqSplit& SP
   }
 }
 
+// Basis policy: how a kernel evaluates the occupied MOs at one position.
+// OqBasisTable reads the system tables (any molecule); a per-system policy
+// generated at run time (oqmc_specialize) has the same two members with the
+// exponents and coefficients compiled in.
+template <int NOCC>
+struct OqBasisTable {
+  template <typename T, typename TC>
+  __device__ static __forceinline__ void mo_val(const OqSystem& S, const OqSplit& SP,
+                                                const TC* __restrict__ C, double x, double y,
+                                                double z, T* mv) {
+    oq_mo_val_t<NOCC, T, TC>(S, SP, C, x, y, z, mv);
+  }
+  template <typename T, typename TC>
+  __device__ static __forceinline__ void mo_vgl(const OqSystem& S, const OqSplit& SP,
+                                                const TC* __restrict__ C, double x, double y,
+                                                double z, T* mv, T (*mg)[3], T* ml) {
+    oq_mo_vgl_t<NOCC, T, TC>(S, SP, C, x, y, z, mv, mg, ml);
+  }
+};
+
 // ---------------------------------------------------------------------------
 // Sampler state in global memory, walker-minor so consecutive threads
 // (walkers) touch consecutive words:
@@ -283,7 +303,7 @@ __device__ __forceinline__ double oq_scaled_width(const OqSystem& S, double x, d
 // One single-electron Metropolis move of electron e to (nx, ny, nz) against
 // shared-memory state; log_extra is the log proposal-density ratio
 // log q(old)/q(new) (0 for symmetric proposals).  Returns acceptance.
-template <int NOCC, typename T, typename Real>
+template <int NOCC, typename T, typename Real, class B>
 __device__ __forceinline__ bool oq_try_move(const OqSystem& S, const OqSplit& SP,
                                             const Real* __restrict__ C, double* pos,
                                             Real* Ai, int WPB, int tid, int e,
@@ -326,7 +346,7 @@ __device__ __forceinline__ bool oq_try_move(const OqSystem& S, const OqSplit& SP
   }
   // new MO row and the ratio vector w_j = sum_m v_m A[m][j]; R = w_i
   T v[NOCC];
-  oq_mo_val_t<NOCC, T, Real>(S, SP, C, nx, ny, nz, v);
+  B::template mo_val<T, Real>(S, SP, C, nx, ny, nz, v);
   Real* As = Ai + (size_t)s * NN * WPB;
   T wv[NOCC];
 #pragma unroll
@@ -377,7 +397,7 @@ __device__ __forceinline__ bool oq_try_move(const OqSystem& S, const OqSplit& SP
 // electron proposed at N(R_J, sigma^2) around a random nucleus J, accepted
 // with the exact proposal ratio q(old)/q(new), q(x) = sum_J
 // exp(-|x-R_J|^2 / 2 sigma^2) (basin_move_1w, vmc_gto.py:925-957).
-template <int NOCC, typename T, typename Real>
+template <int NOCC, typename T, typename Real, class B = OqBasisTable<NOCC>>
 __global__ void __launch_bounds__(128)
 k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
         const void* __restrict__ gC, OqMoveArgs a) {
@@ -424,7 +444,7 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
         const double nx = pos[(3 * e) * WPB + tid] + a.step * n3[0];
         const double ny = pos[(3 * e + 1) * WPB + tid] + a.step * n3[1];
         const double nz = pos[(3 * e + 2) * WPB + tid] + a.step * n3[2];
-        nacc += oq_try_move<NOCC, T, Real>(S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz, 0.0, u,
+        nacc += oq_try_move<NOCC, T, Real, B>(S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz, 0.0, u,
                                            logdet);
       }
     } else if (a.mode == 0) {
@@ -441,7 +461,7 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
         const double d2 = (nx - ox) * (nx - ox) + (ny - oy) * (ny - oy) + (nz - oz) * (nz - oz);
         const double log_extra =
             3.0 * log(so / sn) + 0.5 * d2 * (1.0 / (so * so) - 1.0 / (sn * sn));
-        nacc += oq_try_move<NOCC, T, Real>(S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
+        nacc += oq_try_move<NOCC, T, Real, B>(S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
                                            log_extra, u, logdet);
       }
     } else {
@@ -472,7 +492,7 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
         sn += exp(-(dnx * dnx + dny * dny + dnz * dnz) * inv2s2 - mn);
       }
       const double log_qratio = (mo + log(so)) - (mn + log(sn));
-      nacc += oq_try_move<NOCC, T, Real>(S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
+      nacc += oq_try_move<NOCC, T, Real, B>(S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
                                          log_qratio, u, logdet);
     }
   }
@@ -507,7 +527,7 @@ struct OqElocArgs {
 // (gto.py:1575-1649) and its Coulomb terms (gto.py:2406-2451); the CTA then
 // reduces over electrons (local_energy_ke, gto.py:2506-2579) and over
 // walkers (fused reduction of E, E^2 and the parts).
-template <int NOCC, typename T, typename Real>
+template <int NOCC, typename T, typename Real, class B = OqBasisTable<NOCC>>
 __global__ void __launch_bounds__(64 * NOCC, (NOCC <= 6) ? 2 : 1)
 k_eloc(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
        const void* __restrict__ gC, OqElocArgs a) {
@@ -543,7 +563,7 @@ k_eloc(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
     const double xe = a.pos[(size_t)(3 * e) * W + w], ye = a.pos[(size_t)(3 * e + 1) * W + w],
                  ze = a.pos[(size_t)(3 * e + 2) * W + w];
     T mv[NOCC], mg[NOCC][3], ml[NOCC];
-    oq_mo_vgl_t<NOCC, T, Real>(S, SP, C, xe, ye, ze, mv, mg, ml);
+    B::template mo_vgl<T, Real>(S, SP, C, xe, ye, ze, mv, mg, ml);
     const Real* A = reinterpret_cast<const Real*>(a.ainv);
     T gx = 0, gy = 0, gz = 0, lp = 0;
 #pragma unroll

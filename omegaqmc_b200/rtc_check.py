@@ -1,0 +1,66 @@
+"""Compile the run-time specialised kernels of a system with NVRTC on the
+host (no GPU needed): the same source and options the library uses in
+``oqmc_specialize``, for checking and inspection."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from . import _lib as L
+from .context import pack_system
+
+CSRC = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc")
+HEADERS = ("oqmc_common.cuh", "oqmc_ao.cuh", "oqmc_eval.cuh", "oqmc_sweep.cuh")
+
+
+def spec_source(system):
+    """The generated specialisation source of ``system``."""
+    lib = L.load()
+    d, keep = pack_system(system)
+    n = lib.oqmc_spec_source_desc(ctypes.byref(d), None, 0)
+    L.check(min(n, 0), None)
+    buf = ctypes.create_string_buffer(n + 1)
+    lib.oqmc_spec_source_desc(ctypes.byref(d), buf, n + 1)
+    return buf.value.decode()
+
+
+def _nvrtc():
+    for n in ("libnvrtc.so.12", "libnvrtc.so", "/usr/local/cuda/lib64/libnvrtc.so.12"):
+        try:
+            return ctypes.CDLL(n)
+        except OSError:
+            continue
+    raise OSError("libnvrtc not found")
+
+
+def compile_spec(system):
+    """NVRTC-compile the specialised kernels; returns (ok, log, cubin bytes)."""
+    nv = _nvrtc()
+    src = spec_source(system)
+    hs = [open(os.path.join(CSRC, h), "rb").read() for h in HEADERS]
+    prog = ctypes.c_void_p()
+    arr_s = (ctypes.c_char_p * len(hs))(*hs)
+    arr_n = (ctypes.c_char_p * len(hs))(*[h.encode() for h in HEADERS])
+    rc = nv.nvrtcCreateProgram(ctypes.byref(prog), src.encode(), b"oqmc_spec.cu", len(hs),
+                               arr_s, arr_n)
+    if rc:
+        return False, f"nvrtcCreateProgram {rc}", b""
+    nocc = system.nocc
+    for k in ("k_moves", "k_eloc"):
+        for t in ("double, double", "float, float"):
+            nv.nvrtcAddNameExpression(prog, f"{k}<{nocc}, {t}, OqSpecBasis>".encode())
+    opts = [b"--gpu-architecture=sm_100a", b"--std=c++17", b"-lineinfo",
+            b"--device-as-default-execution-space"]
+    rc = nv.nvrtcCompileProgram(prog, len(opts), (ctypes.c_char_p * len(opts))(*opts))
+    n = ctypes.c_size_t()
+    nv.nvrtcGetProgramLogSize(prog, ctypes.byref(n))
+    log = ctypes.create_string_buffer(n.value + 1)
+    nv.nvrtcGetProgramLog(prog, log)
+    cubin = b""
+    if rc == 0:
+        nv.nvrtcGetCUBINSize(prog, ctypes.byref(n))
+        cb = ctypes.create_string_buffer(n.value)
+        nv.nvrtcGetCUBIN(prog, cb)
+        cubin = cb.raw
+    nv.nvrtcDestroyProgram(ctypes.byref(prog))
+    return rc == 0, log.value.decode(errors="replace"), cubin
