@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--proposal", default="scaled", choices=["scaled", "plain"])
+    ap.add_argument("--quick", action="store_true",
+                    help="profiling mode: no equilibration, comparison, e2e or CPU legs")
     return ap.parse_args()
 
 
@@ -247,9 +249,13 @@ def run_ours(a):
 
     # set-up: step adaptation and a fixed equilibration (core electrons start
     # far from their equilibrium density), then the W warm-up sweeps
-    if not a.step_size:
-        step = adapt_step(ens, step)
-    ens.run(EQUIL_SWEEPS, step)
+    if a.quick:
+        a.no_e2e = a.no_cpu = True
+        step = a.step_size or 0.8
+    else:
+        if not a.step_size:
+            step = adapt_step(ens, step)
+        ens.run(EQUIL_SWEEPS, step)
     ens.run(max(a.warmup, 3), step)
     torch.cuda.synchronize()
 
@@ -271,7 +277,7 @@ def run_ours(a):
     flags = ctx.flags()
     s_np = sums.cpu().numpy()
     series = s_np[:, 3] / np.maximum(s_np[:, 6], 1)
-    if K >= 1000:
+    if K >= 1000 or a.quick:
         tau_series = series
         tau_src = f"timed series ({K} sweeps)"
     else:
@@ -283,7 +289,7 @@ def run_ours(a):
 
     # the comparison target: the plain FP64 sampler on the same walkers
     plain = None
-    if a.precision != "fp64" or a.proposal != "plain":
+    if not a.quick and (a.precision != "fp64" or a.proposal != "plain"):
         pctx = GTOContext(system)            # fixed-width Gaussian proposal
         pctx.specialize()
         pe = WalkerEnsemble(pctx, ens.X, "fp64", seed=99 + rank, refresh_every=REFRESH_EVERY)

@@ -490,11 +490,12 @@ static int launch_moves(oqmc_ctx* ctx, const OqMoveArgs& m, int wpb, size_t sm, 
                         void* stream) {
   const OqLaunch L = make_launch(ctx, stream, sm);
   const int mixed = precision == OQ_PREC_MIXED;
-  if (ctx->spec) {
+  if (ctx->spec && m.mode == 0) {
     OqMoveArgs mm = m;
     const void* C = mixed ? (const void*)ctx->d_C32 : (const void*)ctx->d_C64;
     void* args[4] = {(void*)&L.sys, (void*)&L.split, (void*)&C, (void*)&mm};
-    if (oq_spec_launch(ctx->spec, mixed ? 1 : 0, dim3((m.W + wpb - 1) / wpb), dim3(wpb), sm,
+    const int which = (m.proposal == 1 ? 4 : 0) + (mixed ? 1 : 0);
+    if (oq_spec_launch(ctx->spec, which, dim3((m.W + wpb - 1) / wpb), dim3(wpb), sm,
                        L.stream, args) != 0)
       return set_err(ctx, OQ_ERR_CUDA, "specialised move kernel launch failed%s");
     return OQ_OK;

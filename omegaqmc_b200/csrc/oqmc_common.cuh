@@ -140,7 +140,7 @@ __device__ __forceinline__ void oq_move_randoms(uint64_t seed, uint32_t walker,
 
 // reciprocal / reciprocal square root in the working precision
 __device__ __forceinline__ double oq_rcp(double x) { return __drcp_rn(x); }
-__device__ __forceinline__ float oq_rcp(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ float oq_rcp(float x) { return __fdividef(1.0f, x); }
 __device__ __forceinline__ double oq_rsqrt(double x) { return rsqrt(x); }
 __device__ __forceinline__ float oq_rsqrt(float x) { return rsqrtf(x); }
 

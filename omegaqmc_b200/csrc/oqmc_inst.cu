@@ -68,19 +68,26 @@ cudaError_t OQ_FN(oq_refresh)(const OqLaunch& L, const double* pos, int W, void*
   return cudaGetLastError();
 }
 
-cudaError_t OQ_FN(oq_moves)(const OqLaunch& L, const OqMoveArgs& a, int wpb, int mixed) {
+template <int PROP>
+static cudaError_t moves_prop(const OqLaunch& L, const OqMoveArgs& a, int wpb, int mixed) {
   const int nb = (a.W + wpb - 1) / wpb;
   cudaError_t e;
   if (mixed) {
-    e = oq_smem_attr(k_moves<OQ_N, float, float>, L.smem);
+    e = oq_smem_attr(k_moves<OQ_N, float, float, PROP>, L.smem);
     if (e != cudaSuccess) return e;
-    k_moves<OQ_N, float, float><<<nb, wpb, L.smem, L.stream>>>(L.sys, L.split, L.C32, a);
+    k_moves<OQ_N, float, float, PROP><<<nb, wpb, L.smem, L.stream>>>(L.sys, L.split, L.C32, a);
   } else {
-    e = oq_smem_attr(k_moves<OQ_N, double, double>, L.smem);
+    e = oq_smem_attr(k_moves<OQ_N, double, double, PROP>, L.smem);
     if (e != cudaSuccess) return e;
-    k_moves<OQ_N, double, double><<<nb, wpb, L.smem, L.stream>>>(L.sys, L.split, L.C64, a);
+    k_moves<OQ_N, double, double, PROP><<<nb, wpb, L.smem, L.stream>>>(L.sys, L.split, L.C64, a);
   }
   return cudaGetLastError();
+}
+
+cudaError_t OQ_FN(oq_moves)(const OqLaunch& L, const OqMoveArgs& a, int wpb, int mixed) {
+  if (a.mode == 1) return moves_prop<2>(L, a, wpb, mixed);
+  if (a.proposal == 1) return moves_prop<1>(L, a, wpb, mixed);
+  return moves_prop<0>(L, a, wpb, mixed);
 }
 
 cudaError_t OQ_FN(oq_eloc)(const OqLaunch& L, const OqElocArgs& a, int mixed) {

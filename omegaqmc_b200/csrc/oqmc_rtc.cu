@@ -292,7 +292,8 @@ std::string generate(const OqSystem& S, const OqSplit& SP, const double* C, int 
 
 struct OqSpecModule {
   CUmodule mod = nullptr;
-  CUfunction fn[4] = {nullptr, nullptr, nullptr, nullptr};  // moves d/f, eloc d/f
+  // moves fixed-width d/f, eloc d/f, moves nucleus-scaled d/f
+  CUfunction fn[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 int oq_spec_build(const OqSystem& S, const OqSplit& SP, const double* C, int nocc,
@@ -315,11 +316,13 @@ int oq_spec_build(const OqSystem& S, const OqSplit& SP, const double* C, int noc
     *err = "nvrtcCreateProgram failed";
     return -1;
   }
-  char names[4][128];
-  snprintf(names[0], 128, "k_moves<%d, double, double, OqSpecBasis>", nocc);
-  snprintf(names[1], 128, "k_moves<%d, float, float, OqSpecBasis>", nocc);
+  char names[6][128];
+  snprintf(names[0], 128, "k_moves<%d, double, double, 0, OqSpecBasis>", nocc);
+  snprintf(names[1], 128, "k_moves<%d, float, float, 0, OqSpecBasis>", nocc);
   snprintf(names[2], 128, "k_eloc<%d, double, double, OqSpecBasis>", nocc);
   snprintf(names[3], 128, "k_eloc<%d, float, float, OqSpecBasis>", nocc);
+  snprintf(names[4], 128, "k_moves<%d, double, double, 1, OqSpecBasis>", nocc);
+  snprintf(names[5], 128, "k_moves<%d, float, float, 1, OqSpecBasis>", nocc);
   for (auto& n : names) A.AddNameExpression(prog, n);
   const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-lineinfo",
                         "--device-as-default-execution-space"};
@@ -337,8 +340,8 @@ int oq_spec_build(const OqSystem& S, const OqSplit& SP, const double* C, int noc
   A.GetCUBINSize(prog, &nb);
   std::vector<char> cubin(nb);
   A.GetCUBIN(prog, cubin.data());
-  std::string lowered[4];
-  for (int i = 0; i < 4; ++i) {
+  std::string lowered[6];
+  for (int i = 0; i < 6; ++i) {
     const char* ln = nullptr;
     A.GetLoweredName(prog, names[i], &ln);
     lowered[i] = ln ? ln : "";
@@ -350,7 +353,7 @@ int oq_spec_build(const OqSystem& S, const OqSplit& SP, const double* C, int noc
     *err = "cuModuleLoadData failed";
     return -1;
   }
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < 6; ++i) {
     if (A.ModuleGetFunction(&m->fn[i], m->mod, lowered[i].c_str()) != CUDA_SUCCESS) {
       A.ModuleUnload(m->mod);
       delete m;

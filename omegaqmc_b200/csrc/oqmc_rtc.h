@@ -11,7 +11,8 @@ struct OqSpecModule;
 int oq_spec_build(const OqSystem& S, const OqSplit& SP, const double* C, int nocc,
                   OqSpecModule** out, std::string* err);
 void oq_spec_destroy(OqSpecModule* m);
-// which: 0 = moves FP64, 1 = moves mixed, 2 = local energy FP64, 3 = mixed
+// which: 0/1 = fixed-width moves FP64/mixed, 2/3 = local energy FP64/mixed,
+// 4/5 = nucleus-scaled moves FP64/mixed
 int oq_spec_launch(OqSpecModule* m, int which, dim3 grid, dim3 block, size_t smem,
                    cudaStream_t stream, void** args);
 std::string oq_spec_source(const OqSystem& S, const OqSplit& SP, const double* C, int nocc);

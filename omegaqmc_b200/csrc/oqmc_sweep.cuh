@@ -391,14 +391,15 @@ __device__ __forceinline__ bool oq_try_move(const OqSystem& S, const OqSplit& SP
 }
 
 // Metropolis moves, one thread per walker, state resident in shared memory
-// for the whole launch.  mode 0: n_steps sweeps over all electrons with
+// for the whole launch.  PROP (compile time) selects the proposal: 0 fixed-
+// width Gaussian, 1 nucleus-scaled Gaussian, 2 basin relocation.  mode 0: n_steps sweeps over all electrons with
 // Gaussian proposals (metropolis_move_1w, OmegaQMC/vmc_gto.py:841-905, as
 // single-electron moves).  mode 1: n_steps basin relocations: one random
 // electron proposed at N(R_J, sigma^2) around a random nucleus J, accepted
 // with the exact proposal ratio q(old)/q(new), q(x) = sum_J
 // exp(-|x-R_J|^2 / 2 sigma^2) (basin_move_1w, vmc_gto.py:925-957).
-template <int NOCC, typename T, typename Real, class B = OqBasisTable<NOCC>>
-__global__ void __launch_bounds__(128)
+template <int NOCC, typename T, typename Real, int PROP, class B = OqBasisTable<NOCC>>
+__global__ void __launch_bounds__(128, 4)
 k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
         const void* __restrict__ gC, OqMoveArgs a) {
   constexpr int NE = 2 * NOCC;
@@ -437,7 +438,7 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
   int nacc = 0;
   for (int t = 0; t < (live ? a.n_steps : 0); ++t) {
     const uint32_t gstep = (uint32_t)(a.step_base + t);
-    if (a.mode == 0 && a.proposal == 0) {
+    if (PROP == 0) {
       for (int e = 0; e < NE; ++e) {
         double n3[3], u;
         oq_move_randoms(a.seed, (uint32_t)w, gstep, (uint32_t)e, n3, u);
@@ -447,7 +448,7 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
         nacc += oq_try_move<NOCC, T, Real, B>(S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz, 0.0, u,
                                            logdet);
       }
-    } else if (a.mode == 0) {
+    } else if (PROP == 1) {
       // nucleus-scaled Gaussian: sigma(x) = step * clamp(r_near(x)/r0, fmin, 1);
       // exact MH with log q(x|x') - log q(x'|x) for the asymmetric proposal
       for (int e = 0; e < NE; ++e) {

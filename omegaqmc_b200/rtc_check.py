@@ -46,9 +46,10 @@ def compile_spec(system):
     if rc:
         return False, f"nvrtcCreateProgram {rc}", b""
     nocc = system.nocc
-    for k in ("k_moves", "k_eloc"):
-        for t in ("double, double", "float, float"):
-            nv.nvrtcAddNameExpression(prog, f"{k}<{nocc}, {t}, OqSpecBasis>".encode())
+    for t in ("double, double", "float, float"):
+        nv.nvrtcAddNameExpression(prog, f"k_eloc<{nocc}, {t}, OqSpecBasis>".encode())
+        for prop in (0, 1):
+            nv.nvrtcAddNameExpression(prog, f"k_moves<{nocc}, {t}, {prop}, OqSpecBasis>".encode())
     opts = [b"--gpu-architecture=sm_100a", b"--std=c++17", b"-lineinfo",
             b"--device-as-default-execution-space"]
     rc = nv.nvrtcCompileProgram(prog, len(opts), (ctypes.c_char_p * len(opts))(*opts))
