@@ -1,0 +1,56 @@
+"""B200-native GTO variational Monte Carlo hot path of ΩQMC (myung-group/OmegaQMC).
+
+Public surface mirrors the reference's: :func:`get_psi_fun`,
+:func:`get_vmc_gto_func`, :class:`VMCTrialState` and
+:func:`generate_molecular_orbitals` (here backed by this package's RHF).
+The arithmetic runs in ``liboqmc_b200.so`` (sm_100a CUDA, C ABI in
+``include/oqmc_b200.h``)."""
+from __future__ import annotations
+
+from .system import Mole, MeanField, build_system, read_shell  # noqa: F401
+
+__version__ = "0.1.0"
+
+__all__ = ["get_psi_fun", "get_vmc_gto_func", "VMCTrialState", "generate_molecular_orbitals",
+           "Mole", "MeanField", "build_system", "read_shell"]
+
+
+def get_psi_fun(*a, **k):
+    from .psi import get_psi_fun as f
+    return f(*a, **k)
+
+
+def get_vmc_gto_func(*a, **k):
+    from .vmc import get_vmc_gto_func as f
+    return f(*a, **k)
+
+
+def __getattr__(name):
+    if name == "VMCTrialState":
+        from .psi import VMCTrialState
+        return VMCTrialState
+    raise AttributeError(name)
+
+
+def generate_molecular_orbitals(astr, units="Bohr", basis="cc-pvdz-shaped", spin=0,
+                                charge=0, **kw):
+    """RHF mean-field object for ``astr`` (``OmegaQMC/vmc_gto.py:217-452`` runs
+    PySCF; here the package's own RHF).  ``basis`` is a PySCF-format dict
+    ``{element: [[am, [alpha, c...], ...], ...]}`` or one of the generated
+    sets ``"cc-pvdz-shaped"`` / ``"sto-3g"`` (H only)."""
+    from . import molecules as M
+    from .rhf import run_rhf
+    if spin != 0:
+        raise NotImplementedError("only closed-shell RHF is supported")
+    if isinstance(basis, str):
+        name = basis.lower()
+        atoms = Mole(astr, {s: [] for s in M.ELEMENT_Z}, unit=units)._atom
+        syms = sorted({s for s, _ in atoms})
+        if name == "cc-pvdz-shaped":
+            basis = {s: M.ccpvdz_shaped(s) for s in syms}
+        elif name == "sto-3g" and syms == ["H"]:
+            basis = {"H": M.sto3g_h()}
+        else:
+            raise ValueError(f"unknown basis {basis!r}; pass a PySCF-format dict")
+    mol = Mole(astr, basis, unit=units, charge=charge, basis_name="gen")
+    return run_rhf(mol, **kw)
