@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--proposal", default="scaled", choices=["scaled", "plain"])
+    ap.add_argument("--eloc", default="cc", choices=["cc", "tc"],
+                    help="local energy on CUDA cores (specialised) or tensor cores (tcgen05)")
     ap.add_argument("--quick", action="store_true",
                     help="profiling mode: no equilibration, comparison, e2e or CPU legs")
     return ap.parse_args()
@@ -240,6 +242,8 @@ def run_ours(a):
     t_spec = time.perf_counter() - t_spec
     if a.proposal == "scaled":
         ctx.set_proposal(1, SCALED_R0, SCALED_FMIN)
+    if a.eloc == "tc" and a.precision == "mixed":
+        ctx.use_tensor_cores(True)
     W = a.walkers
     step = a.step_size or STEP_DEFAULT.get(a.system, 0.3)
     X0 = init_walkers_gaussian(system, W, 1.0, seed=1000 + rank)
@@ -384,6 +388,8 @@ def run_ours(a):
                    "parallelism": f"replicas x{world}",
                    "trial": "RHF determinant + Pade J2 (b=3)",
                    "kernels": f"NVRTC-specialised to the molecule (compile {t_spec:.1f} s, untimed)",
+                   "local_energy": "tcgen05 tensor cores (split TF32/BF16)" if a.eloc == "tc"
+                                   else "CUDA cores",
                    "proposal": (f"nucleus-scaled Gaussian (r0={SCALED_R0}, fmin={SCALED_FMIN}), "
                                 "exact MH" if a.proposal == "scaled" else "fixed-width Gaussian"),
                    "equilibration_sweeps": EQUIL_SWEEPS + 200,

@@ -182,6 +182,13 @@ int oqmc_sweeps_noalloc(oqmc_ctx* ctx, double* walkers, int W, int precision,
  * while core electrons move with core-sized steps. */
 int oqmc_set_proposal(oqmc_ctx* ctx, int kind, double r0, double fmin_frac);
 
+/* Mixed-precision local energy with the MO contraction (the GEMM
+ * AO(5 components) x C of get_psi_mo_vgl, OmegaQMC/psi/gto.py:1188-1214) on
+ * the tcgen05 tensor cores: 128 (walker, electron) rows per CTA, split
+ * TF32/BF16 operands for near-FP32 accuracy, FP32 accumulators in TMEM.
+ * enable = 0 returns to the CUDA-core local-energy kernel. */
+int oqmc_use_tensor_cores(oqmc_ctx* ctx, int enable);
+
 /* Per-system specialisation (no counterpart in the reference, whose jit
  * unrolls the shell loop at trace time, OmegaQMC/psi/gto.py:1012-1186):
  * generate the AO->MO evaluation of this molecule as straight-line code with

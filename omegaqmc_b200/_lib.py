@@ -80,6 +80,7 @@ _SIGS = [
                                     c_void_p, c_void_p]),
     ("oqmc_set_proposal", c_int, [c_void_p, c_int, c_double, c_double]),
     ("oqmc_specialize", c_int, [c_void_p, c_int]),
+    ("oqmc_use_tensor_cores", c_int, [c_void_p, c_int]),
     ("oqmc_spec_source", c_int, [c_void_p, ctypes.c_char_p, c_size_t]),
     ("oqmc_spec_source_desc", c_int, [ctypes.POINTER(SystemDesc), ctypes.c_char_p, c_size_t]),
     ("oqmc_set_split", c_int, [c_void_p, c_double]),

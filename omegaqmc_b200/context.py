@@ -208,6 +208,10 @@ class GTOContext:
         and orbitals; raises NotImplementedError where NVRTC is unavailable."""
         self._check(self.lib.oqmc_specialize(self._h, int(enable)))
 
+    def use_tensor_cores(self, enable=True):
+        """Mixed-precision local energy with the MO contraction on tcgen05."""
+        self._check(self.lib.oqmc_use_tensor_cores(self._h, int(enable)))
+
     def set_proposal(self, kind, r0=1.0, fmin_frac=0.05):
         """0: fixed-width Gaussian (reference); 1: nucleus-scaled width."""
         self._check(self.lib.oqmc_set_proposal(self._h, int(kind), float(r0), float(fmin_frac)))

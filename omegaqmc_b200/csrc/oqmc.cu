@@ -25,6 +25,8 @@ struct oqmc_ctx {
   double tight_alpha;
   int proposal;           // 0 fixed-width Gaussian, 1 nucleus-scaled width
   OqSpecModule* spec;     // run-time specialised kernels, or null
+  int use_tc;             // mixed local energy on the tensor cores
+  unsigned char* d_Btc;   // split MO-coefficient operands of k_eloc_tc
   double* h_C;            // host copy of the MO coefficients (for specialisation)
   double scale_r0, scale_fmin;
   char err[512];
@@ -248,6 +250,8 @@ extern "C" int oqmc_create(oqmc_ctx** out, const oqmc_system_desc* d) {
   ctx->tight_alpha = 50.0;
   ctx->proposal = 0;
   ctx->spec = nullptr;
+  ctx->use_tc = 0;
+  ctx->d_Btc = nullptr;
   ctx->h_C = new double[(size_t)d->nbf * d->nocc];
   memcpy(ctx->h_C, d->C, sizeof(double) * (size_t)d->nbf * d->nocc);
   ctx->scale_r0 = 1.0;
@@ -279,6 +283,7 @@ extern "C" int oqmc_create(oqmc_ctx** out, const oqmc_system_desc* d) {
 int oqmc_destroy(oqmc_ctx* ctx) {
   if (!ctx) return OQ_OK;
   oq_spec_destroy(ctx->spec);
+  cudaFree(ctx->d_Btc);
   delete[] ctx->h_C;
   cudaFree(ctx->d_sys);
   cudaFree(ctx->d_split);
@@ -295,6 +300,49 @@ int oqmc_set_proposal(oqmc_ctx* ctx, int kind, double r0, double fmin_frac) {
     return set_err(ctx, OQ_ERR_ARG, "bad proposal parameters%s");
   ctx->proposal = kind;
   if (kind == 1) { ctx->scale_r0 = r0; ctx->scale_fmin = fmin_frac; }
+  return OQ_OK;
+}
+
+// TF32 rounding as cvt.rna (nearest, ties away from zero) and BF16 (nearest even)
+static float host_tf32(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  u = (u + 0x1000u) & 0xFFFFE000u;
+  memcpy(&f, &u, 4);
+  return f;
+}
+static uint16_t host_bf16(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  return (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
+}
+
+int oqmc_use_tensor_cores(oqmc_ctx* ctx, int enable) {
+  if (!ctx) return OQ_ERR_ARG;
+  if (!enable) { ctx->use_tc = 0; return OQ_OK; }
+  if (ctx->nocc > 16 || 128 / ctx->n_e < 1)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED, "tensor-core local energy needs n_occ <= 16%s");
+  const OqTcPlan P = oq_tc_plan(ctx->nbf);
+  if (P.total > 227u * 1024u)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED, "basis too large for the tensor-core tile%s");
+  if (!ctx->d_Btc) {
+    std::vector<unsigned char> h(P.b_end - P.b_hi, 0);
+    const int KC4 = (int)(P.K4 >> 2), KC2 = (int)(P.K2 >> 3);
+    for (int n = 0; n < 16; ++n)
+      for (int k = 0; k < ctx->nbf; ++k) {
+        const float c = n < ctx->nocc ? (float)ctx->h_C[(size_t)k * ctx->nocc + n] : 0.0f;
+        const float hi = host_tf32(c), lo = c - hi;
+        const uint32_t o4 = (uint32_t)(((n >> 3) * KC4 + (k >> 2)) << 7) + ((n & 7) << 4) + ((k & 3) << 2);
+        const uint32_t o2 = (uint32_t)(((n >> 3) * KC2 + (k >> 3)) << 7) + ((n & 7) << 4) + ((k & 7) << 1);
+        memcpy(&h[(P.b_hi - P.b_hi) + o4], &hi, 4);
+        memcpy(&h[(P.b_lo - P.b_hi) + o4], &lo, 4);
+        const uint16_t bf = host_bf16(hi);
+        memcpy(&h[(P.b_bf - P.b_hi) + o2], &bf, 2);
+      }
+    OQ_CUDA(ctx, cudaMalloc(&ctx->d_Btc, h.size()));
+    OQ_CUDA(ctx, cudaMemcpy(ctx->d_Btc, h.data(), h.size(), cudaMemcpyHostToDevice));
+  }
+  ctx->use_tc = 1;
   return OQ_OK;
 }
 
@@ -548,6 +596,14 @@ int oqmc_sweeps(oqmc_ctx* ctx, double* X, int W, void* state, int precision, int
     el.sums = sums + (size_t)k * OQ_NSUM;
     el.el_trace = el_trace ? el_trace + (size_t)k * W : nullptr;
     el.eparts = (k == n_meas - 1) ? eparts_last : nullptr;
+    if (mixed && ctx->use_tc) {
+      cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_eloc_tc_##N(Le, el, ctx->d_Btc, ctx->nbf)
+      OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+      OQ_CUDA(ctx, err);
+      continue;
+    }
     if (ctx->spec) {
       OqElocArgs ee = el;
       const void* C = mixed ? (const void*)ctx->d_C32 : (const void*)ctx->d_C64;

@@ -73,6 +73,7 @@ enum OqStatus {
 // Device flag bits written by kernels (OR-ed into a per-launch word).
 #define OQ_FLAG_NAN 1u
 #define OQ_FLAG_SINGULAR 2u
+#define OQ_FLAG_TIMEOUT 4u
 
 
 // ---------------------------------------------------------------------------

@@ -105,3 +105,14 @@ cudaError_t OQ_FN(oq_eloc)(const OqLaunch& L, const OqElocArgs& a, int mixed) {
   }
   return cudaGetLastError();
 }
+
+cudaError_t OQ_FN(oq_eloc_tc)(const OqLaunch& L, const OqElocArgs& a, const void* Bpack, int nbf) {
+  constexpr int WB = 128 / (2 * OQ_N);
+  const int nb = (a.W + WB - 1) / WB;
+  const size_t smem = oq_tc_plan(nbf).total;
+  cudaError_t e = oq_smem_attr(k_eloc_tc<OQ_N>, smem);
+  if (e != cudaSuccess) return e;
+  k_eloc_tc<OQ_N><<<nb, 128, smem, L.stream>>>(L.sys, L.split,
+                                                static_cast<const unsigned char*>(Bpack), a);
+  return cudaGetLastError();
+}

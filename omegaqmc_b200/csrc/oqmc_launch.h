@@ -3,7 +3,7 @@
 // template instantiations build in parallel.
 #pragma once
 #include <cuda_runtime.h>
-#include "oqmc_sweep.cuh"
+#include "oqmc_eloc_tc.cuh"
 
 struct OqLaunch {
   const OqSystem* sys;
@@ -23,7 +23,9 @@ struct OqLaunch {
   cudaError_t oq_refresh_##N(const OqLaunch& L, const double* pos, int W, void* ainv, \
                              double* logdet, int mixed);                              \
   cudaError_t oq_moves_##N(const OqLaunch& L, const OqMoveArgs& a, int wpb, int mixed); \
-  cudaError_t oq_eloc_##N(const OqLaunch& L, const OqElocArgs& a, int mixed);
+  cudaError_t oq_eloc_##N(const OqLaunch& L, const OqElocArgs& a, int mixed);           \
+  cudaError_t oq_eloc_tc_##N(const OqLaunch& L, const OqElocArgs& a, const void* Bpack, \
+                             int nbf);
 
 #define OQ_NOCC_LIST(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(10) X(12) X(14) X(16)
 
