@@ -218,6 +218,66 @@ int oqmc_get_flags(oqmc_ctx* ctx, unsigned* flags, int clear, void* stream);
  * utility with no counterpart in the reference. */
 int oqmc_measure_peak(int kind, double* out_rate, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Batched sampling: several molecules (contexts) of different electron and
+ * basis counts share one persistent launch.  No counterpart in the
+ * reference, whose driver samples one molecule per run
+ * (OmegaQMC/vmc_gto.py:1233-1617 VMCDriverGTO.__call__); per system a launch
+ * does what oqmc_refresh followed by oqmc_sweeps does here
+ * (_make_production_step, vmc_gto.py:985-1034, as single-electron sweeps),
+ * with the same random-number counters, so the walkers it leaves are those
+ * of the per-system path.
+ * ---------------------------------------------------------------------- */
+typedef struct oqmc_batch oqmc_batch;
+
+/* One system of a batch. */
+typedef struct {
+  double* walkers;       /* (W, n_e, 3) device positions, updated in place */
+  int W;
+  int proposal;          /* 0 fixed-width Gaussian, 1 nucleus-scaled */
+  double step;           /* Gaussian width (scale s of the scaled proposal) */
+  double scale_r0;       /* nucleus-scaled width: step*clamp(r_near/r0, fmin, 1) */
+  double scale_fmin;
+  double* sums;          /* [cap][8] device measurement sums (as oqmc_sweeps),
+                            accumulated; slot = measurement index since reset */
+  int cap;
+} oqmc_batch_system;
+
+/* Generate and compile (NVRTC, sm_100a) the batch kernel for n contexts on
+ * one device at a precision (tens of seconds for five cc-pVDZ molecules).
+ * OQ_ERR_UNSUPPORTED without NVRTC. */
+int oqmc_batch_create(oqmc_batch** out, oqmc_ctx* const* ctxs, int n, int precision);
+int oqmc_batch_destroy(oqmc_batch* b);
+const char* oqmc_batch_last_error(const oqmc_batch* b);
+/* Attach walkers and proposal settings (n entries) and plan the tiles. */
+int oqmc_batch_bind(oqmc_batch* b, const oqmc_batch_system* sys);
+/* Tile shape: threads per CTA, walkers per tile of each system (multiples
+ * of 32 dividing threads) and register variant (0: <= 255 registers per
+ * thread, 1: <= 168 with at most 128 threads, 2: <= 128). */
+int oqmc_batch_configure(oqmc_batch* b, int threads, const int* walkers_per_tile, int variant);
+int oqmc_batch_get_config(const oqmc_batch* b, int* threads, int* walkers_per_tile,
+                          int* variant, int* grid, size_t* smem, int* regs, int* local_bytes);
+/* Autotune the tile shape by timing short batched runs (moves the walkers,
+ * accumulates nothing); *best_ms = time of n_sweeps sweeps with the winner. */
+int oqmc_batch_tune(oqmc_batch* b, int n_sweeps, uint64_t seed, void* stream, float* best_ms);
+/* Sweep counter of the next launch = step_base, measurement slot = 0, tile
+ * timers cleared (synchronises stream). */
+int oqmc_batch_reset(oqmc_batch* b, uint64_t step_base, void* stream);
+/* One persistent launch: FP64 refresh, then n_sweeps sweeps with a
+ * measurement every measure_every sweeps, for every system. */
+int oqmc_batch_run(oqmc_batch* b, int n_sweeps, int measure_every, uint64_t seed, void* stream);
+/* Capture n_launches consecutive launches in a CUDA graph (the counters
+ * advance on the device between them); oqmc_batch_replay launches it. */
+int oqmc_batch_capture(oqmc_batch* b, int n_launches, int n_sweeps, int measure_every,
+                       uint64_t seed);
+int oqmc_batch_replay(oqmc_batch* b, void* stream);
+/* Per-system sum of tile durations (ns) since the last reset (synchronises). */
+int oqmc_batch_busy(oqmc_batch* b, unsigned long long* busy_ns, void* stream);
+int oqmc_batch_get_flags(oqmc_batch* b, unsigned* flags, int clear, void* stream);
+/* Generated batch source for descriptors (host only). */
+int oqmc_batch_source_desc(const oqmc_system_desc* descs, int n, char* buf, size_t cap,
+                           size_t* len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -48,6 +48,15 @@ class SystemDesc(ctypes.Structure):
     ]
 
 
+class BatchSystem(ctypes.Structure):
+    """Mirror of ``oqmc_batch_system``."""
+    _fields_ = [
+        ("walkers", c_void_p), ("W", c_int), ("proposal", c_int),
+        ("step", c_double), ("scale_r0", c_double), ("scale_fmin", c_double),
+        ("sums", c_void_p), ("cap", c_int),
+    ]
+
+
 class OqmcError(RuntimeError):
     """A liboqmc_b200 call failed; ``code`` is the OQ_ERR_* status."""
 
@@ -86,6 +95,24 @@ _SIGS = [
     ("oqmc_set_split", c_int, [c_void_p, c_double]),
     ("oqmc_get_flags", c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint), c_int, c_void_p]),
     ("oqmc_measure_peak", c_int, [c_int, P_double, c_void_p]),
+    ("oqmc_batch_create", c_int, [ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), c_int,
+                                  c_int]),
+    ("oqmc_batch_destroy", c_int, [c_void_p]),
+    ("oqmc_batch_last_error", ctypes.c_char_p, [c_void_p]),
+    ("oqmc_batch_bind", c_int, [c_void_p, ctypes.POINTER(BatchSystem)]),
+    ("oqmc_batch_configure", c_int, [c_void_p, c_int, P_int, c_int]),
+    ("oqmc_batch_get_config", c_int, [c_void_p, P_int, P_int, P_int, P_int,
+                                      ctypes.POINTER(c_size_t), P_int, P_int]),
+    ("oqmc_batch_tune", c_int, [c_void_p, c_int, c_uint64, c_void_p,
+                                ctypes.POINTER(ctypes.c_float)]),
+    ("oqmc_batch_reset", c_int, [c_void_p, c_uint64, c_void_p]),
+    ("oqmc_batch_run", c_int, [c_void_p, c_int, c_int, c_uint64, c_void_p]),
+    ("oqmc_batch_capture", c_int, [c_void_p, c_int, c_int, c_int, c_uint64]),
+    ("oqmc_batch_replay", c_int, [c_void_p, c_void_p]),
+    ("oqmc_batch_busy", c_int, [c_void_p, ctypes.POINTER(ctypes.c_ulonglong), c_void_p]),
+    ("oqmc_batch_get_flags", c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint), c_int, c_void_p]),
+    ("oqmc_batch_source_desc", c_int, [ctypes.POINTER(SystemDesc), c_int, ctypes.c_char_p,
+                                       c_size_t, ctypes.POINTER(c_size_t)]),
 ]
 
 EXPORTED = [s[0] for s in _SIGS]
@@ -110,11 +137,14 @@ def load(path=None):
     return lib
 
 
-def check(code, ctx=None):
-    """Raise for a negative status, with the library's message."""
+def check(code, ctx=None, batch=False):
+    """Raise for a negative status, with the library's message (of a context,
+    or of a batch handle when ``batch`` is true)."""
     if code == OQ_OK:
         return
-    msg = load().oqmc_last_error(ctx).decode(errors="replace")
+    lib = load()
+    msg = (lib.oqmc_batch_last_error(ctx) if batch else lib.oqmc_last_error(ctx))
+    msg = msg.decode(errors="replace")
     if code == OQ_ERR_ARG:
         raise ValueError(msg)
     if code == OQ_ERR_UNSUPPORTED:

@@ -53,7 +53,8 @@ def _run(cmd):
     return r
 
 
-RTC_HEADERS = ("oqmc_common.cuh", "oqmc_ao.cuh", "oqmc_eval.cuh", "oqmc_sweep.cuh")
+RTC_HEADERS = ("oqmc_common.cuh", "oqmc_ao.cuh", "oqmc_eval.cuh", "oqmc_sweep.cuh",
+               "oqmc_batch.cuh")
 
 
 def _embed_headers():
@@ -91,7 +92,8 @@ def build(force=False, jobs=None, verbose=False):
              (os.path.join(CSRC, "oqmc_peak.cu"), os.path.join(BUILD, "oqmc_peak.o"), []),
              (os.path.join(CSRC, "oqmc_noalloc.cu"), os.path.join(BUILD, "oqmc_noalloc.o"), []),
              (os.path.join(CSRC, "oqmc_rtc.cu"), os.path.join(BUILD, "oqmc_rtc.o"),
-              ["-I" + BUILD])]
+              ["-I" + BUILD]),
+             (os.path.join(CSRC, "oqmc_batch.cu"), os.path.join(BUILD, "oqmc_batch.o"), [])]
     for n in NOCC_LIST:
         units.append((os.path.join(CSRC, "oqmc_inst.cu"),
                       os.path.join(BUILD, f"oqmc_inst_{n}.o"), [f"-DOQ_N={n}"]))

@@ -12,25 +12,7 @@
 #include "oqmc_rtc.h"
 #include "../../include/oqmc_b200.h"
 
-struct oqmc_ctx {
-  int device;
-  int nocc, n_e, nbf, natm;
-  OqSystem hsys;
-  OqSplit hsplit;
-  OqSystem* d_sys;
-  OqSplit* d_split;
-  double* d_C64;
-  float* d_C32;
-  unsigned* d_flags;
-  double tight_alpha;
-  int proposal;           // 0 fixed-width Gaussian, 1 nucleus-scaled width
-  OqSpecModule* spec;     // run-time specialised kernels, or null
-  int use_tc;             // mixed local energy on the tensor cores
-  unsigned char* d_Btc;   // split MO-coefficient operands of k_eloc_tc
-  double* h_C;            // host copy of the MO coefficients (for specialisation)
-  double scale_r0, scale_fmin;
-  char err[512];
-};
+#include "oqmc_ctx.h"
 
 static thread_local char g_create_err[512] = "";
 
@@ -218,6 +200,24 @@ static void split_for(const OqSystem& S, double tight_alpha, OqSplit& sp) {
     sp.r2[g] = r2;
   }
 }
+
+}  // extern "C"
+
+// Host-side system tables and split radii for a descriptor (used by the
+// batch source generator); err receives the validation message.
+int oq_fill_system_desc(const oqmc_system_desc* d, OqSystem* S, OqSplit* SP, int* nocc,
+                        std::string* err) {
+  const int rc = fill_system(d, *S);
+  if (rc != OQ_OK) {
+    *err = g_create_err;
+    return rc;
+  }
+  split_for(*S, 50.0, *SP);
+  *nocc = d->nocc;
+  return OQ_OK;
+}
+
+extern "C" {
 
 extern "C" int oqmc_spec_source_desc(const oqmc_system_desc* d, char* buf, size_t len) {
   OqSystem* S = new (std::nothrow) OqSystem();

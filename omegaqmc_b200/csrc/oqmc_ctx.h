@@ -1,0 +1,29 @@
+// Internal: the context object behind the opaque oqmc_ctx handle, shared by
+// the library's translation units (not part of the public ABI).
+#pragma once
+#include "oqmc_sweep.cuh"
+
+struct OqSpecModule;
+
+struct oqmc_ctx {
+  int device;
+  int nocc, n_e, nbf, natm;
+  OqSystem hsys;
+  OqSplit hsplit;
+  OqSystem* d_sys;
+  OqSplit* d_split;
+  double* d_C64;
+  float* d_C32;
+  unsigned* d_flags;
+  double tight_alpha;
+  int proposal;           // 0 fixed-width Gaussian, 1 nucleus-scaled width
+  OqSpecModule* spec;     // run-time specialised kernels, or null
+  int use_tc;             // mixed local energy on the tensor cores
+  unsigned char* d_Btc;   // split MO-coefficient operands of k_eloc_tc
+  double* h_C;            // host copy of the MO coefficients (for specialisation)
+  double scale_r0, scale_fmin;
+  char err[512];
+};
+
+// Record an error message on a context and return code.
+int oq_ctx_set_error(oqmc_ctx* ctx, int code, const char* msg);

@@ -43,6 +43,8 @@ struct Api {
   CUresult (*FuncSetAttribute)(CUfunction, CUfunction_attribute, int);
   CUresult (*LaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned,
                            unsigned, unsigned, CUstream, void**, void**);
+  CUresult (*Occupancy)(int*, CUfunction, int, size_t);
+  CUresult (*FuncGetAttribute)(int*, CUfunction_attribute, CUfunction);
 };
 
 Api g_api;
@@ -79,7 +81,9 @@ void load_api() {
             sym(cu, "cuModuleGetFunction", a.ModuleGetFunction) &&
             sym(cu, "cuModuleUnload", a.ModuleUnload) &&
             sym(cu, "cuFuncSetAttribute", a.FuncSetAttribute) &&
-            sym(cu, "cuLaunchKernel", a.LaunchKernel);
+            sym(cu, "cuLaunchKernel", a.LaunchKernel) &&
+            sym(cu, "cuOccupancyMaxActiveBlocksPerMultiprocessor", a.Occupancy) &&
+            sym(cu, "cuFuncGetAttribute", a.FuncGetAttribute);
   if (!ok) {
     a.err = "missing NVRTC or driver symbol";
     return;
@@ -263,8 +267,10 @@ struct Gen {
   }
 };
 
-std::string generate(const OqSystem& S, const OqSplit& SP, const double* C, int nocc) {
-  std::string src = "#include \"oqmc_sweep.cuh\"\n\nstruct OqSpecBasis {\n";
+// The basis policy of one system as a struct named `name`.
+std::string generate_basis(const OqSystem& S, const OqSplit& SP, const double* C, int nocc,
+                           const std::string& name) {
+  std::string src = "struct " + name + " {\n";
   {
     Gen g{S, SP, C, nocc, ""};
     g.body(false);
@@ -288,42 +294,44 @@ std::string generate(const OqSystem& S, const OqSplit& SP, const double* C, int 
   return src;
 }
 
+std::string generate(const OqSystem& S, const OqSplit& SP, const double* C, int nocc) {
+  return "#include \"oqmc_sweep.cuh\"\n\n" + generate_basis(S, SP, C, nocc, "OqSpecBasis");
+}
+
 }  // namespace
 
-struct OqSpecModule {
-  CUmodule mod = nullptr;
-  // moves fixed-width d/f, eloc d/f, moves nucleus-scaled d/f
-  CUfunction fn[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-};
+std::string oq_spec_basis_source(const OqSystem& S, const OqSplit& SP, const double* C, int nocc,
+                                 const std::string& name) {
+  return generate_basis(S, SP, C, nocc, name);
+}
 
-int oq_spec_build(const OqSystem& S, const OqSplit& SP, const double* C, int nocc,
-                  OqSpecModule** out, std::string* err) {
+int oq_rtc_available(std::string* err) {
+  std::call_once(g_api_once, load_api);
+  if (!g_api.ok && err) *err = g_api.err;
+  return g_api.ok ? 1 : 0;
+}
+
+int oq_rtc_compile(const std::string& src, const std::vector<std::string>& names,
+                   std::vector<char>* cubin, std::vector<std::string>* lowered,
+                   std::string* err) {
   std::call_once(g_api_once, load_api);
   if (!g_api.ok) {
     *err = g_api.err;
     return -1;
   }
   const Api& A = g_api;
-  std::string src = generate(S, SP, C, nocc);
   std::vector<const char*> hdr_src, hdr_name;
   for (int i = 0; i < kOqRtcCount; ++i) {
     hdr_src.push_back(kOqRtcSrcs[i]);
     hdr_name.push_back(kOqRtcNames[i]);
   }
   nvrtcProgram prog;
-  if (A.CreateProgram(&prog, src.c_str(), "oqmc_spec.cu", kOqRtcCount, hdr_src.data(),
+  if (A.CreateProgram(&prog, src.c_str(), "oqmc_rtc.cu", kOqRtcCount, hdr_src.data(),
                       hdr_name.data()) != NVRTC_SUCCESS) {
     *err = "nvrtcCreateProgram failed";
     return -1;
   }
-  char names[6][128];
-  snprintf(names[0], 128, "k_moves<%d, double, double, 0, OqSpecBasis>", nocc);
-  snprintf(names[1], 128, "k_moves<%d, float, float, 0, OqSpecBasis>", nocc);
-  snprintf(names[2], 128, "k_eloc<%d, double, double, OqSpecBasis>", nocc);
-  snprintf(names[3], 128, "k_eloc<%d, float, float, OqSpecBasis>", nocc);
-  snprintf(names[4], 128, "k_moves<%d, double, double, 1, OqSpecBasis>", nocc);
-  snprintf(names[5], 128, "k_moves<%d, float, float, 1, OqSpecBasis>", nocc);
-  for (auto& n : names) A.AddNameExpression(prog, n);
+  for (const std::string& n : names) A.AddNameExpression(prog, n.c_str());
   const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-lineinfo",
                         "--device-as-default-execution-space"};
   const nvrtcResult rc = A.CompileProgram(prog, 4, opts);
@@ -338,30 +346,117 @@ int oq_spec_build(const OqSystem& S, const OqSplit& SP, const double* C, int noc
   }
   size_t nb = 0;
   A.GetCUBINSize(prog, &nb);
-  std::vector<char> cubin(nb);
-  A.GetCUBIN(prog, cubin.data());
-  std::string lowered[6];
-  for (int i = 0; i < 6; ++i) {
+  cubin->resize(nb);
+  A.GetCUBIN(prog, cubin->data());
+  lowered->assign(names.size(), "");
+  for (size_t i = 0; i < names.size(); ++i) {
     const char* ln = nullptr;
-    A.GetLoweredName(prog, names[i], &ln);
-    lowered[i] = ln ? ln : "";
+    A.GetLoweredName(prog, names[i].c_str(), &ln);
+    (*lowered)[i] = ln ? ln : "";
   }
   A.DestroyProgram(&prog);
-  OqSpecModule* m = new OqSpecModule();
-  if (A.ModuleLoadData(&m->mod, cubin.data()) != CUDA_SUCCESS) {
-    delete m;
+  return 0;
+}
+
+int oq_rtc_load(const std::vector<char>& cubin, const std::vector<std::string>& lowered,
+                void** mod_out, std::vector<void*>* fns, std::string* err) {
+  const Api& A = g_api;
+  CUmodule mod = nullptr;
+  if (A.ModuleLoadData(&mod, cubin.data()) != CUDA_SUCCESS) {
     *err = "cuModuleLoadData failed";
     return -1;
   }
-  for (int i = 0; i < 6; ++i) {
-    if (A.ModuleGetFunction(&m->fn[i], m->mod, lowered[i].c_str()) != CUDA_SUCCESS) {
-      A.ModuleUnload(m->mod);
-      delete m;
-      *err = "cuModuleGetFunction failed";
+  fns->assign(lowered.size(), nullptr);
+  for (size_t i = 0; i < lowered.size(); ++i) {
+    CUfunction f = nullptr;
+    if (A.ModuleGetFunction(&f, mod, lowered[i].c_str()) != CUDA_SUCCESS) {
+      A.ModuleUnload(mod);
+      *err = "cuModuleGetFunction failed for " + lowered[i];
       return -1;
     }
-    A.FuncSetAttribute(m->fn[i], CU_FUNC_ATTRIBUTE_PREFERRED_SHARED_MEMORY_CARVEOUT, 100);
+    A.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_PREFERRED_SHARED_MEMORY_CARVEOUT, 100);
+    (*fns)[i] = (void*)f;
   }
+  *mod_out = (void*)mod;
+  return 0;
+}
+
+int oq_rtc_build(const std::string& src, const std::vector<std::string>& names, void** mod_out,
+                 std::vector<void*>* fns, std::string* err) {
+  std::vector<char> cubin;
+  std::vector<std::string> lowered;
+  if (oq_rtc_compile(src, names, &cubin, &lowered, err) != 0) return -1;
+  return oq_rtc_load(cubin, lowered, mod_out, fns, err);
+}
+
+void oq_rtc_unload(void* mod) {
+  if (g_api.ok && mod) g_api.ModuleUnload((CUmodule)mod);
+}
+
+int oq_rtc_launch(void* fn, dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                  void** args) {
+  const Api& A = g_api;
+  CUfunction f = (CUfunction)fn;
+  if (smem > 48 * 1024 &&
+      A.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem) !=
+          CUDA_SUCCESS)
+    return -1;
+  return A.LaunchKernel(f, grid.x, grid.y, grid.z, block.x, block.y, block.z, (unsigned)smem,
+                        (CUstream)stream, args, nullptr) == CUDA_SUCCESS
+             ? 0
+             : -1;
+}
+
+int oq_rtc_occupancy(void* fn, int block, size_t smem, int* nblk) {
+  const Api& A = g_api;
+  CUfunction f = (CUfunction)fn;
+  if (smem > 48 * 1024 &&
+      A.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem) !=
+          CUDA_SUCCESS) {
+    *nblk = 0;
+    return 0;
+  }
+  return A.Occupancy(nblk, f, block, smem) == CUDA_SUCCESS ? 0 : -1;
+}
+
+int oq_rtc_regs(void* fn) {
+  int r = -1;
+  g_api.FuncGetAttribute(&r, CU_FUNC_ATTRIBUTE_NUM_REGS, (CUfunction)fn);
+  return r;
+}
+
+int oq_rtc_local_bytes(void* fn) {
+  int r = -1;
+  g_api.FuncGetAttribute(&r, CU_FUNC_ATTRIBUTE_LOCAL_SIZE_BYTES, (CUfunction)fn);
+  return r;
+}
+
+struct OqSpecModule {
+  CUmodule mod = nullptr;
+  // moves fixed-width d/f, eloc d/f, moves nucleus-scaled d/f
+  CUfunction fn[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+int oq_spec_build(const OqSystem& S, const OqSplit& SP, const double* C, int nocc,
+                  OqSpecModule** out, std::string* err) {
+  std::vector<std::string> names;
+  const char* forms[6] = {"k_moves<%d, double, double, 0, OqSpecBasis>",
+                          "k_moves<%d, float, float, 0, OqSpecBasis>",
+                          "k_eloc<%d, double, double, OqSpecBasis>",
+                          "k_eloc<%d, float, float, OqSpecBasis>",
+                          "k_moves<%d, double, double, 1, OqSpecBasis>",
+                          "k_moves<%d, float, float, 1, OqSpecBasis>"};
+  for (const char* f : forms) {
+    char b[128];
+    snprintf(b, sizeof b, f, nocc);
+    names.push_back(b);
+  }
+  void* mod = nullptr;
+  std::vector<void*> fns;
+  if (oq_rtc_build(generate(S, SP, C, nocc), names, &mod, &fns, err) != 0) return -1;
+  OqSpecModule* m = new OqSpecModule();
+  m->mod = (CUmodule)mod;
+  for (int i = 0; i < 6; ++i) m->fn[i] = (CUfunction)fns[i];
   *out = m;
   return 0;
 }

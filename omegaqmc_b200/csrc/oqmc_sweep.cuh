@@ -288,7 +288,8 @@ struct OqMoveArgs {
 };
 
 // Proposal width at x for the nucleus-scaled Gaussian move.
-__device__ __forceinline__ double oq_scaled_width(const OqSystem& S, double x, double y,
+template <class SJ>
+__device__ __forceinline__ double oq_scaled_width(const SJ& S, double x, double y,
                                                   double z, double step, double r0,
                                                   double fmn) {
   double r2 = 1e300;
@@ -303,8 +304,11 @@ __device__ __forceinline__ double oq_scaled_width(const OqSystem& S, double x, d
 // One single-electron Metropolis move of electron e to (nx, ny, nz) against
 // shared-memory state; log_extra is the log proposal-density ratio
 // log q(old)/q(new) (0 for symmetric proposals).  Returns acceptance.
-template <int NOCC, typename T, typename Real, class B>
-__device__ __forceinline__ bool oq_try_move(const OqSystem& S, const OqSplit& SP,
+// J supplies the nuclei and Jastrow constants (natm, nuc, has_j1, j1a, j1b,
+// has_j2, j2): the system struct itself or a compact copy of those fields;
+// S is handed to the basis policy.
+template <int NOCC, typename T, typename Real, class B, class SJ>
+__device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, const OqSplit& SP,
                                             const Real* __restrict__ C, double* pos,
                                             Real* Ai, int WPB, int tid, int e,
                                             double nx, double ny, double nz,
@@ -325,22 +329,22 @@ __device__ __forceinline__ bool oq_try_move(const OqSystem& S, const OqSplit& SP
     const double ax = nx - xj, ay = ny - yj, az = nz - zj;
     const double rn2 = ax * ax + ay * ay + az * az;
     valid = valid && (rn2 >= thr2);
-    if (S.has_j2) {
+    if (J.has_j2) {
       const double bx = ox - xj, by = oy - yj, bz = oz - zj;
       const T rn2t = (T)rn2, ro2t = (T)(bx * bx + by * by + bz * bz);
       const int o = ((e & 1) == (j & 1)) ? 0 : 2;
-      const T pa = (T)S.j2[o], pb = (T)S.j2[o + 1];
+      const T pa = (T)J.j2[o], pb = (T)J.j2[o + 1];
       dJ += oq_pade_q(pa, pb, rn2t * oq_rsqrt(rn2t)) - oq_pade_q(pa, pb, ro2t * oq_rsqrt(ro2t));
     }
   }
-  for (int I = 0; I < S.natm; ++I) {
-    const double ax = nx - S.nuc[I][0], ay = ny - S.nuc[I][1], az = nz - S.nuc[I][2];
+  for (int I = 0; I < J.natm; ++I) {
+    const double ax = nx - J.nuc[I][0], ay = ny - J.nuc[I][1], az = nz - J.nuc[I][2];
     const double rn2 = ax * ax + ay * ay + az * az;
     valid = valid && (rn2 >= thr2);
-    if (S.has_j1) {
-      const double bx = ox - S.nuc[I][0], by = oy - S.nuc[I][1], bz = oz - S.nuc[I][2];
+    if (J.has_j1) {
+      const double bx = ox - J.nuc[I][0], by = oy - J.nuc[I][1], bz = oz - J.nuc[I][2];
       const T rn2t = (T)rn2, ro2t = (T)(bx * bx + by * by + bz * bz);
-      const T pa = (T)S.j1a[I], pb = (T)S.j1b[I];
+      const T pa = (T)J.j1a[I], pb = (T)J.j1b[I];
       dJ += oq_pade_q(pa, pb, rn2t * oq_rsqrt(rn2t)) - oq_pade_q(pa, pb, ro2t * oq_rsqrt(ro2t));
     }
   }
@@ -445,7 +449,7 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
         const double nx = pos[(3 * e) * WPB + tid] + a.step * n3[0];
         const double ny = pos[(3 * e + 1) * WPB + tid] + a.step * n3[1];
         const double nz = pos[(3 * e + 2) * WPB + tid] + a.step * n3[2];
-        nacc += oq_try_move<NOCC, T, Real, B>(S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz, 0.0, u,
+        nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz, 0.0, u,
                                            logdet);
       }
     } else if (PROP == 1) {
@@ -462,7 +466,7 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
         const double d2 = (nx - ox) * (nx - ox) + (ny - oy) * (ny - oy) + (nz - oz) * (nz - oz);
         const double log_extra =
             3.0 * log(so / sn) + 0.5 * d2 * (1.0 / (so * so) - 1.0 / (sn * sn));
-        nacc += oq_try_move<NOCC, T, Real, B>(S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
+        nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
                                            log_extra, u, logdet);
       }
     } else {
@@ -493,7 +497,7 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
         sn += exp(-(dnx * dnx + dny * dny + dnz * dnz) * inv2s2 - mn);
       }
       const double log_qratio = (mo + log(so)) - (mn + log(sn));
-      nacc += oq_try_move<NOCC, T, Real, B>(S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
+      nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
                                          log_qratio, u, logdet);
     }
   }
@@ -508,6 +512,64 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if ((tid & 31) == 0) atomicAdd(a.acc_sum, v);
   }
+}
+
+// Local-energy contributions of electron e of one walker: its Coulomb terms
+// (e-e counted once, for partners j > e; gto.py:2406-2451), the Laplacian
+// term lap_e = sum_m A[m][i] L[i][m] - |Gamma_e|^2 + lap J_e and the squared
+// total gradient |Gamma_e + grad J_e|^2 (_slater_det_assemble, gto.py:728-778;
+// Padé VGL, gto.py:1575-1649).  pos points at the walker's x of electron 0
+// with stride ps between coordinates; A at its inverse entry (0,0,0) with
+// stride as between entries.  The four outputs are accumulated (+=).
+template <int NOCC, typename T, typename Real, class B, class SJ>
+__device__ __forceinline__ void oq_eloc_electron(const SJ& J, const OqSystem& S,
+                                                 const OqSplit& SP, const Real* __restrict__ C,
+                                                 const double* pos, size_t ps, const Real* A,
+                                                 size_t as, int e, double& ee, double& en,
+                                                 double& lp_tot, double& g2) {
+  constexpr int NE = 2 * NOCC;
+  const int s = e & 1, i = e >> 1;
+  const double xe = pos[(size_t)(3 * e) * ps], ye = pos[(size_t)(3 * e + 1) * ps],
+               ze = pos[(size_t)(3 * e + 2) * ps];
+  T mv[NOCC], mg[NOCC][3], ml[NOCC];
+  B::template mo_vgl<T, Real>(S, SP, C, xe, ye, ze, mv, mg, ml);
+  T gx = 0, gy = 0, gz = 0, lp = 0;
+#pragma unroll
+  for (int m = 0; m < NOCC; ++m) {
+    const T am = (T)A[(size_t)((s * NOCC + m) * NOCC + i) * as];
+    gx += am * mg[m][0]; gy += am * mg[m][1]; gz += am * mg[m][2];
+    lp += am * ml[m];
+  }
+  T jx = (T)0, jy = (T)0, jz = (T)0, jl = (T)0;
+  for (int j = 0; j < NE; ++j) {
+    if (j == e) continue;
+    const double dx = xe - pos[(size_t)(3 * j) * ps], dy = ye - pos[(size_t)(3 * j + 1) * ps],
+                 dz = ze - pos[(size_t)(3 * j + 2) * ps];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    if (j > e) ee += rsqrt(r2 + OQ_EPS);
+    if (J.has_j2) {
+      const int o = ((e & 1) == (j & 1)) ? 0 : 2;
+      const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
+      T upr, l;
+      oq_pade_vgl_q((T)J.j2[o], (T)J.j2[o + 1], r2t * rinv, rinv, upr, l);
+      jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
+    }
+  }
+  for (int I = 0; I < J.natm; ++I) {
+    const double dx = xe - J.nuc[I][0], dy = ye - J.nuc[I][1], dz = ze - J.nuc[I][2];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    en -= J.Z[I] * rsqrt(r2 + OQ_EPS);
+    if (J.has_j1) {
+      const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
+      T upr, l;
+      oq_pade_vgl_q((T)J.j1a[I], (T)J.j1b[I], r2t * rinv, rinv, upr, l);
+      jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
+    }
+  }
+  const double sgx = (double)gx, sgy = (double)gy, sgz = (double)gz;
+  const double Gx = sgx + (double)jx, Gy = sgy + (double)jy, Gz = sgz + (double)jz;
+  lp_tot += (double)lp - (sgx * sgx + sgy * sgy + sgz * sgz) + (double)jl;
+  g2 += Gx * Gx + Gy * Gy + Gz * Gz;
 }
 
 struct OqElocArgs {
@@ -533,7 +595,6 @@ __global__ void __launch_bounds__(64 * NOCC, (NOCC <= 6) ? 2 : 1)
 k_eloc(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
        const void* __restrict__ gC, OqElocArgs a) {
   constexpr int NE = 2 * NOCC;
-  constexpr int NN = NOCC * NOCC;
   extern __shared__ __align__(16) unsigned char smem[];
   OqSystem& S = *reinterpret_cast<OqSystem*>(smem);
   OqSplit& SP = *reinterpret_cast<OqSplit*>(smem + sizeof(OqSystem));
@@ -559,52 +620,10 @@ k_eloc(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
   const int w = blockIdx.x * 32 + lane;
   const bool live = w < W;
   double ee = 0.0, en = 0.0, lp_tot = 0.0, g2 = 0.0;
-  if (live) {
-    const int s = e & 1, i = e >> 1;
-    const double xe = a.pos[(size_t)(3 * e) * W + w], ye = a.pos[(size_t)(3 * e + 1) * W + w],
-                 ze = a.pos[(size_t)(3 * e + 2) * W + w];
-    T mv[NOCC], mg[NOCC][3], ml[NOCC];
-    B::template mo_vgl<T, Real>(S, SP, C, xe, ye, ze, mv, mg, ml);
-    const Real* A = reinterpret_cast<const Real*>(a.ainv);
-    T gx = 0, gy = 0, gz = 0, lp = 0;
-#pragma unroll
-    for (int m = 0; m < NOCC; ++m) {
-      const T am = (T)A[(size_t)((s * NOCC + m) * NOCC + i) * W + w];
-      gx += am * mg[m][0]; gy += am * mg[m][1]; gz += am * mg[m][2];
-      lp += am * ml[m];
-    }
-    T jx = (T)0, jy = (T)0, jz = (T)0, jl = (T)0;
-    for (int j = 0; j < NE; ++j) {
-      if (j == e) continue;
-      const double dx = xe - a.pos[(size_t)(3 * j) * W + w],
-                   dy = ye - a.pos[(size_t)(3 * j + 1) * W + w],
-                   dz = ze - a.pos[(size_t)(3 * j + 2) * W + w];
-      const double r2 = dx * dx + dy * dy + dz * dz;
-      if (j > e) ee += rsqrt(r2 + OQ_EPS);
-      if (S.has_j2) {
-        const int o = ((e & 1) == (j & 1)) ? 0 : 2;
-        const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
-        T upr, l;
-        oq_pade_vgl_q((T)S.j2[o], (T)S.j2[o + 1], r2t * rinv, rinv, upr, l);
-        jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
-      }
-    }
-    for (int I = 0; I < S.natm; ++I) {
-      const double dx = xe - S.nuc[I][0], dy = ye - S.nuc[I][1], dz = ze - S.nuc[I][2];
-      const double r2 = dx * dx + dy * dy + dz * dz;
-      en -= S.Z[I] * rsqrt(r2 + OQ_EPS);
-      if (S.has_j1) {
-        const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
-        T upr, l;
-        oq_pade_vgl_q((T)S.j1a[I], (T)S.j1b[I], r2t * rinv, rinv, upr, l);
-        jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
-      }
-    }
-    const double sgx = (double)gx, sgy = (double)gy, sgz = (double)gz;
-    const double Gx = sgx + (double)jx, Gy = sgy + (double)jy, Gz = sgz + (double)jz;
-    lp_tot = (double)lp - (sgx * sgx + sgy * sgy + sgz * sgz) + (double)jl;
-    g2 = Gx * Gx + Gy * Gy + Gz * Gz;
-  }
+  if (live)
+    oq_eloc_electron<NOCC, T, Real, B>(S, S, SP, C, a.pos + w, (size_t)W,
+                                       reinterpret_cast<const Real*>(a.ainv) + w, (size_t)W, e,
+                                       ee, en, lp_tot, g2);
   red[(e * 4 + 0) * 32 + lane] = ee;
   red[(e * 4 + 1) * 32 + lane] = en;
   red[(e * 4 + 2) * 32 + lane] = lp_tot;

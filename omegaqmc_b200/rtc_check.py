@@ -10,7 +10,7 @@ from . import _lib as L
 from .context import pack_system
 
 CSRC = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc")
-HEADERS = ("oqmc_common.cuh", "oqmc_ao.cuh", "oqmc_eval.cuh", "oqmc_sweep.cuh")
+HEADERS = ("oqmc_common.cuh", "oqmc_ao.cuh", "oqmc_eval.cuh", "oqmc_sweep.cuh", "oqmc_batch.cuh")
 
 
 def spec_source(system):
@@ -33,23 +33,36 @@ def _nvrtc():
     raise OSError("libnvrtc not found")
 
 
-def compile_spec(system):
-    """NVRTC-compile the specialised kernels; returns (ok, log, cubin bytes)."""
+def batch_source(systems):
+    """The generated source of the batched kernel for a list of systems."""
+    lib = L.load()
+    packed = [pack_system(s) for s in systems]
+    arr = (L.SystemDesc * len(systems))(*[p[0] for p in packed])
+    n = ctypes.c_size_t()
+    L.check(lib.oqmc_batch_source_desc(arr, len(systems), None, 0, ctypes.byref(n)), None, True)
+    buf = ctypes.create_string_buffer(n.value + 1)
+    L.check(lib.oqmc_batch_source_desc(arr, len(systems), buf, n.value + 1, None), None, True)
+    return buf.value.decode()
+
+
+BATCH_KERNELS = [f"k_batch<{t}, {mt}, {mb}>" for t in ("float, float", "double, double")
+                 for mt, mb in ((256, 1), (128, 3), (256, 2))]
+
+
+def compile_source(src, names):
+    """NVRTC-compile ``src`` with the library's headers and options for
+    sm_100a; returns (ok, log, cubin bytes)."""
     nv = _nvrtc()
-    src = spec_source(system)
     hs = [open(os.path.join(CSRC, h), "rb").read() for h in HEADERS]
     prog = ctypes.c_void_p()
     arr_s = (ctypes.c_char_p * len(hs))(*hs)
     arr_n = (ctypes.c_char_p * len(hs))(*[h.encode() for h in HEADERS])
-    rc = nv.nvrtcCreateProgram(ctypes.byref(prog), src.encode(), b"oqmc_spec.cu", len(hs),
+    rc = nv.nvrtcCreateProgram(ctypes.byref(prog), src.encode(), b"oqmc_rtc.cu", len(hs),
                                arr_s, arr_n)
     if rc:
         return False, f"nvrtcCreateProgram {rc}", b""
-    nocc = system.nocc
-    for t in ("double, double", "float, float"):
-        nv.nvrtcAddNameExpression(prog, f"k_eloc<{nocc}, {t}, OqSpecBasis>".encode())
-        for prop in (0, 1):
-            nv.nvrtcAddNameExpression(prog, f"k_moves<{nocc}, {t}, {prop}, OqSpecBasis>".encode())
+    for n in names:
+        nv.nvrtcAddNameExpression(prog, n.encode())
     opts = [b"--gpu-architecture=sm_100a", b"--std=c++17", b"-lineinfo",
             b"--device-as-default-execution-space"]
     rc = nv.nvrtcCompileProgram(prog, len(opts), (ctypes.c_char_p * len(opts))(*opts))
@@ -65,3 +78,14 @@ def compile_spec(system):
         cubin = cb.raw
     nv.nvrtcDestroyProgram(ctypes.byref(prog))
     return rc == 0, log.value.decode(errors="replace"), cubin
+
+
+def compile_spec(system):
+    """NVRTC-compile the specialised kernels; returns (ok, log, cubin bytes)."""
+    nocc = system.nocc
+    names = []
+    for t in ("double, double", "float, float"):
+        names.append(f"k_eloc<{nocc}, {t}, OqSpecBasis>")
+        for prop in (0, 1):
+            names.append(f"k_moves<{nocc}, {t}, {prop}, OqSpecBasis>")
+    return compile_source(spec_source(system), names)

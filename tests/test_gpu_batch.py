@@ -1,0 +1,140 @@
+"""Batched persistent launch over uneven molecules (oqmc_batch_*).
+
+The batch kernel draws the same Philox numbers as the per-system kernels, so
+per molecule a batched launch must leave the walkers of the per-system path
+(FP64 refresh, then sweeps) and the same measurement sums up to summation
+order."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import seeded_walkers
+from omegaqmc_b200 import molecules as M
+from omegaqmc_b200.batch import BatchedSampler
+from omegaqmc_b200.context import GTOContext
+from omegaqmc_b200.sampler import NSUM, PREC
+from omegaqmc_b200.system import build_system
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ["H2", "LiH", "H2O"]
+WALKERS = [300, 200, 500]          # not multiples of the tile sizes: ragged tails
+STEPS = [0.5, 0.6, 0.8]
+PROPS = ["plain", "scaled", "scaled"]
+
+
+def _system(name):
+    mf = M.make_mf(name)
+    return build_system(mf, M.benchmark_params_corr(mf.mol))
+
+
+@pytest.fixture(scope="module")
+def contexts():
+    ctxs = []
+    for n in NAMES:
+        c = GTOContext(_system(n))
+        c.specialize()
+        ctxs.append(c)
+    return ctxs
+
+
+def _walkers(ctxs, seed=1):
+    return [torch.as_tensor(seeded_walkers(c.system, W, 1.0, seed + k), device="cuda")
+            for k, (c, W) in enumerate(zip(ctxs, WALKERS))]
+
+
+def _per_system(ctx, X0, precision, prop, step, n_sweeps, me, seed, step_base):
+    ctx.set_proposal(1 if prop == "scaled" else 0, 1.0, 0.05)
+    X = X0.clone()
+    st = ctx.new_state(X.shape[0], PREC[precision])
+    sums = torch.zeros(n_sweeps // me, NSUM, dtype=torch.float64, device="cuda")
+    ctx.refresh(X, st, PREC[precision])
+    ctx.sweeps(X, st, PREC[precision], n_sweeps, step, seed, step_base, sums, measure_every=me)
+    torch.cuda.synchronize()
+    ctx.set_proposal(0)
+    return X, sums
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_batch_reproduces_per_system_path(contexts, precision):
+    X0 = _walkers(contexts)
+    b = BatchedSampler(contexts, [x.clone() for x in X0], STEPS, precision=precision,
+                       proposal=PROPS, cap=16)
+    b.configure(128, [128, 64, 32], variant=0)
+    n, me, seed, base = 20, 5, 1234, 100
+    b.reset(base)
+    b.run(n, me, seed)
+    torch.cuda.synchronize()
+    assert b.flags() == 0
+    for k, ctx in enumerate(contexts):
+        X, sums = _per_system(ctx, X0[k], precision, PROPS[k], STEPS[k], n, me, seed, base)
+        same = torch.all((b.walkers[k] == X).reshape(X.shape[0], -1), dim=1)
+        frac = float(same.float().mean())
+        assert frac > 0.99, (NAMES[k], frac)
+        moved = torch.any((X != X0[k]).reshape(X.shape[0], -1), dim=1)
+        assert float(moved.float().mean()) > 0.5
+        bs = b.sums[k][: n // me].cpu().numpy()
+        rs = sums.cpu().numpy()
+        np.testing.assert_array_equal(bs[:, 6], rs[:, 6])          # finite walkers
+        if frac == 1.0:
+            np.testing.assert_array_equal(bs[:, 5], rs[:, 5])      # accepted moves
+            np.testing.assert_allclose(bs[:, :5], rs[:, :5], rtol=1e-9, atol=1e-9)
+        else:
+            np.testing.assert_allclose(bs[:, 5], rs[:, 5], rtol=2e-2)
+
+
+def test_graph_replay_equals_launches(contexts):
+    X0 = _walkers(contexts, seed=7)
+    b = BatchedSampler(contexts, [x.clone() for x in X0], STEPS, proposal=PROPS, cap=32)
+    b.configure(128, [64, 64, 64], variant=2)
+    b.reset(0)
+    for _ in range(3):
+        b.run(10, 5, 99)
+    torch.cuda.synchronize()
+    ref_X = [x.clone() for x in b.walkers]
+    ref_S = [s.clone() for s in b.sums]
+    for k in range(len(contexts)):
+        b.walkers[k].copy_(X0[k])
+    b.reset(0)
+    b.capture(3, 10, 5, 99)
+    b.replay()
+    torch.cuda.synchronize()
+    for k in range(len(contexts)):
+        assert torch.equal(b.walkers[k], ref_X[k])
+        np.testing.assert_allclose(b.sums[k][:6].cpu().numpy(), ref_S[k][:6].cpu().numpy(),
+                                   rtol=1e-12, atol=1e-12)
+    # the device counters advanced: a second replay fills the next six slots
+    b.replay()
+    torch.cuda.synchronize()
+    assert float(b.sums[0][6:12, 6].sum()) == 6 * WALKERS[0]
+    assert b.flags() == 0
+
+
+def test_autotuner_picks_a_valid_shape(contexts):
+    X0 = _walkers(contexts, seed=3)
+    b = BatchedSampler(contexts, X0, STEPS, proposal=PROPS, cap=4)
+    cfg, ms = b.tune(n_sweeps=4)
+    assert ms > 0.0
+    t = cfg["threads"]
+    assert t in (64, 128, 256) and cfg["grid"] >= 1 and cfg["smem"] > 0
+    for w in cfg["walkers_per_tile"]:
+        assert w % 32 == 0 and t % w == 0
+    b.reset(0)
+    b.run(10, 5, 5)
+    torch.cuda.synchronize()
+    for k in range(len(contexts)):
+        e, acc, nw = b.energies(k, 2)
+        assert np.all(nw == WALKERS[k]) and np.all(np.isfinite(e))
+    assert b.flags() == 0
+
+
+def test_bad_tile_shapes_are_rejected(contexts):
+    b = BatchedSampler(contexts, _walkers(contexts), STEPS, cap=1)
+    with pytest.raises(ValueError):
+        b.configure(128, [96, 64, 32])       # 96 does not divide 128
+    with pytest.raises(ValueError):
+        b.configure(256, [64, 64, 64], variant=1)   # variant 1 allows 128 threads
+    with pytest.raises(ValueError):
+        b.configure(128, [256, 64, 64])
+    b.configure(64, [32, 32, 64])
+    assert b.config()["threads"] == 64

@@ -26,3 +26,24 @@ def test_spec_compiles_for_sm100a(name):
     ok, log, cubin = R.compile_spec(s)
     assert ok, log
     assert len(cubin) > 10000
+
+
+def test_batch_source_dispatches_every_system():
+    systems = [build_system(M.make_mf(n), M.benchmark_params_corr(M.make_mf(n).mol))
+               for n in ("H2", "LiH")]
+    src = R.batch_source(systems)
+    assert "struct OqSpecBasis_0" in src and "struct OqSpecBasis_1" in src
+    assert "oq_batch_tile<1, T, Real, OqSpecBasis_0>" in src
+    assert "oq_batch_tile<2, T, Real, OqSpecBasis_1>" in src
+
+
+def test_batch_kernel_compiles_for_sm100a():
+    try:
+        R._nvrtc()
+    except OSError:
+        pytest.skip("NVRTC not installed")
+    systems = [build_system(M.make_mf(n), M.benchmark_params_corr(M.make_mf(n).mol))
+               for n in ("H2", "LiH")]
+    ok, log, cubin = R.compile_source(R.batch_source(systems), R.BATCH_KERNELS[:1])
+    assert ok, log
+    assert len(cubin) > 10000
