@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--proposal", default="scaled", choices=["scaled", "plain"])
     ap.add_argument("--eloc", default="cc", choices=["cc", "tc"],
                     help="local energy on CUDA cores (specialised) or tensor cores (tcgen05)")
+    ap.add_argument("--workload", default="h2o", choices=["h2o", "batched"],
+                    help="h2o: the headline H2O metric; batched: H2, LiH, H2O, N2 and "
+                         "(H2O)2 in one persistent launch under a CUDA graph")
     ap.add_argument("--quick", action="store_true",
                     help="profiling mode: no equilibration, comparison, e2e or CPU legs")
     return ap.parse_args()
@@ -430,6 +433,201 @@ def run_ours(a):
         dist.destroy_process_group()
 
 
+BATCH = (("H2", 8192), ("LiH", 16384), ("H2O", 65536), ("N2", 32768), ("H2O_dimer", 16384))
+
+
+def run_batched(a):
+    """Five molecules of uneven size in one persistent launch per 50 sweeps,
+    the launches captured in a CUDA graph, tile shape from the autotuner.
+
+    value = walker-sweeps/s summed over the five molecules (all ranks);
+    per molecule the GPU time is apportioned by the tiles' own timers."""
+    import torch
+    import torch.distributed as dist
+    from omegaqmc_b200 import _lib as L
+    from omegaqmc_b200.batch import BatchedSampler
+    from omegaqmc_b200.context import GTOContext
+    from omegaqmc_b200.sampler import WalkerEnsemble, init_walkers_gaussian, NSUM, PREC
+    from oracle import gto_oracle as O  # noqa: F401  (tau estimator)
+
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    names = [n for n, _ in BATCH]
+    Ws = [w for _, w in BATCH]
+    systems = [build_system(n) for n in names]
+    ctxs, steps, X0 = [], [], []
+    t_spec = time.perf_counter()
+    for k, (s, W) in enumerate(zip(systems, Ws)):
+        c = GTOContext(s)
+        c.specialize()
+        c.set_proposal(1, SCALED_R0, SCALED_FMIN)
+        X = init_walkers_gaussian(s, W, 1.0, seed=100 * k + 1000 + rank)
+        # step adaptation of the nucleus-scaled proposal on a 4096-walker subset
+        ens = WalkerEnsemble(c, X[:4096], a.precision, seed=17 + k, refresh_every=REFRESH_EVERY)
+        steps.append(a.step_size or adapt_step(ens, 0.8))
+        del ens
+        ctxs.append(c)
+        X0.append(X)
+    t_spec = time.perf_counter() - t_spec
+    K = max(REFRESH_EVERY, (a.steps // REFRESH_EVERY) * REFRESH_EVERY)
+    n_launch = K // REFRESH_EVERY
+    b = BatchedSampler(ctxs, X0, steps, precision=a.precision, proposal="scaled",
+                       scale_r0=SCALED_R0, scale_fmin=SCALED_FMIN, cap=K)
+    seed = 4242 + 7919 * rank
+    # equilibration (no measurements), then the autotuner, then warm-up
+    # sweep-counter ranges of the phases (the RNG counter is 32-bit)
+    EQ_BASE, WARM_BASE, SEP_BASE, E2E_BASE = 10**7, 2 * 10**7, 3 * 10**7, 4 * 10**7
+    b.reset(EQ_BASE)
+    n_eq = 0 if a.quick else EQUIL_SWEEPS // 3
+    for _ in range(n_eq // REFRESH_EVERY):
+        b.run(REFRESH_EVERY, REFRESH_EVERY + 1, seed)
+    torch.cuda.synchronize()
+    default_cfg = b.config()
+    t_tune = time.perf_counter()
+    cfg, tune_ms = b.tune(n_sweeps=4, seed=seed ^ 0x55)
+    t_tune = time.perf_counter() - t_tune
+    b.reset(WARM_BASE)
+    for _ in range(max(1, a.warmup // REFRESH_EVERY)):
+        b.run(REFRESH_EVERY, REFRESH_EVERY + 1, seed)
+    b.capture(n_launch, REFRESH_EVERY, 1, seed)
+    b.reset(0)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        b.replay()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    busy = b.busy_ns()
+    flags = b.flags()
+    sums_np = [sm[:K].cpu().numpy() for sm in b.sums]
+
+    # per-system launches of the same kernels, one after the other (the
+    # comparison the batch has to beat): refresh + 50 sweeps per molecule
+    sep_ms = []
+    for c, X, st_, W in zip(ctxs, b.walkers, steps, Ws):
+        Xc = X.clone()
+        state = c.new_state(W, PREC[a.precision])
+        sums = torch.zeros(REFRESH_EVERY, NSUM, dtype=torch.float64, device=dev)
+        c.refresh(Xc, state, PREC[a.precision])
+        c.sweeps(Xc, state, PREC[a.precision], REFRESH_EVERY, st_, seed, SEP_BASE, sums)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for r in range(2):
+            c.refresh(Xc, state, PREC[a.precision])
+            c.sweeps(Xc, state, PREC[a.precision], REFRESH_EVERY, st_, seed,
+                     SEP_BASE + (r + 1) * REFRESH_EVERY, sums)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sep_ms.append(e0.elapsed_time(e1) / 2)
+
+    # e2e: walkers from pinned host memory every launch, results back
+    e2e = None
+    if not a.no_e2e:
+        hostX = [x.detach().to("cpu").pin_memory() for x in b.walkers]
+        hsums = [torch.empty(REFRESH_EVERY, NSUM, dtype=torch.float64).pin_memory()
+                 for _ in b.walkers]
+        Ke = min(n_launch, 10)
+        b.reset(E2E_BASE)
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for r in range(Ke):
+            for X, hX in zip(b.walkers, hostX):
+                X.copy_(hX, non_blocking=True)
+            b.run(REFRESH_EVERY, 1, seed)
+            for X, hX, sm, hs in zip(b.walkers, hostX, b.sums, hsums):
+                hX.copy_(X, non_blocking=True)
+                hs.copy_(sm[r * REFRESH_EVERY:(r + 1) * REFRESH_EVERY], non_blocking=True)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        bi = sum(x.numel() * 8 for x in b.walkers)
+        e2e = {"ms_per_step": f0.elapsed_time(f1) / (Ke * REFRESH_EVERY),
+               "h2d_bytes_per_step": bi / REFRESH_EVERY,
+               "d2h_bytes_per_step": (bi + len(b.walkers) * REFRESH_EVERY * NSUM * 8)
+                                     / REFRESH_EVERY}
+    t = torch.tensor([ms, e2e["ms_per_step"] if e2e else 0.0], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max, e2e_ms = float(t[0]), float(t[1])
+
+    rate = ctypes_peak(L, 0 if a.precision == "fp64" else 1)
+    tot_busy = float(sum(busy))
+    per = {}
+    flops_total = 0.0
+    dec_total = 0.0
+    for k, (n, s, W) in enumerate(zip(names, systems, Ws)):
+        sm = sums_np[k]
+        ser = sm[:, 3] / np.maximum(sm[:, 6], 1)
+        e_mean, e_serr, _, kappa = O.binning_analysis(ser)
+        acc = float(sm[:, 5].sum() / (K * W * s.n_e))
+        share = busy[k] / tot_busy
+        t_k = ms * share * 1e-3
+        wss = W * K / t_k
+        work = work_per_walker_sweep(s, acc)
+        flops_total += work["flops"] * W * K
+        dec_total += W * K / (ms * 1e-3) / kappa
+        per[n] = {"walkers": W, "step": steps[k], "acceptance": acc, "tau_int": kappa,
+                  "energy": {"mean": e_mean, "serr": e_serr},
+                  "gpu_time_share": share,
+                  "walker_sweeps_per_s": wss,
+                  "flops_per_walker_sweep": work["flops"],
+                  "achieved_tflops": work["flops"] * W * K / t_k / 1e12,
+                  "roofline_frac": work["flops"] * W * K / t_k / rate if rate else None,
+                  "separate_ms_per_sweep": sep_ms[k] / REFRESH_EVERY}
+    W_tot = sum(Ws)
+    achieved = flops_total / (ms * 1e-3)
+    line = {
+        "metric": "walker-sweeps/s, H2+LiH+H2O+N2+(H2O)2 batched in one persistent launch",
+        "value": W_tot * world * K / (ms_max * 1e-3), "unit": "walker-sweeps/s",
+        "n_gpus": world, "steps": K, "warmup": a.warmup, "ms_per_step": ms_max / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if a.precision == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": "batched H2/STO-3G 8192, LiH 16384, H2O 65536, N2 32768, "
+                               "(H2O)2 16384 walkers (cc-pVDZ-shaped); refresh + 50 sweeps per "
+                               "launch, E_L every sweep",
+                   "precision": a.precision, "parallelism": f"replicas x{world}",
+                   "graph": f"{n_launch} persistent launches captured in one CUDA graph",
+                   "tile_shape": cfg, "default_shape": default_cfg,
+                   "autotune_s": t_tune, "compile_s": t_spec,
+                   "l2": "walker state in shared memory for a whole launch; positions "
+                         "(34 MB) read and written once per launch"},
+        "decorrelated_samples_per_s": dec_total * world,
+        "systems": per,
+        "separate_launches_ms_per_sweep": sum(sep_ms) / REFRESH_EVERY,
+        "batched_speedup_vs_separate": (sum(sep_ms) / REFRESH_EVERY) / (ms / K),
+        "kernel_flags": flags,
+        "gpu_launches": n_launch,
+        "roofline": {"bound": "fp32" if a.precision == "mixed" else "fp64",
+                     "achieved": achieved / 1e12, "peak": rate / 1e12 if rate else None,
+                     "unit": "TFLOP/s", "frac": achieved / rate if rate else None,
+                     "traffic": None, "kernel": "k_batch (generated, all five molecules)",
+                     "peak_source": "own FMA microkernel (oqmc_measure_peak), of measured"},
+    }
+    if e2e:
+        line["e2e"] = {"value": W_tot * world / (e2e_ms * 1e-3), "unit": "walker-sweeps/s",
+                       "h2d_bytes_per_step": e2e["h2d_bytes_per_step"],
+                       "d2h_bytes_per_step": e2e["d2h_bytes_per_step"], "ms_per_step": e2e_ms}
+    line["clocks"] = clk.summary()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    b.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def ctypes_peak(L, kind):
     import ctypes
     import torch
@@ -453,6 +651,8 @@ def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "batched":
+        run_batched(a)
     else:
         run_ours(a)
 

@@ -34,6 +34,7 @@ struct Variant {
 // register budgets: <= 255, <= 168 and <= 128 registers per thread
 const Variant kVariants[] = {{256, 1}, {128, 3}, {256, 2}};
 const int kNumVariants = 3;
+const size_t kMaxSmem = 227 * 1024;   // opt-in shared memory per CTA on sm_100
 
 std::string batch_source(const std::vector<const OqSystem*>& S,
                          const std::vector<const OqSplit*>& SP,
@@ -432,7 +433,8 @@ int oqmc_batch_get_flags(oqmc_batch* b, unsigned* flags, int clear, void* stream
 
 // Autotuner.  Candidates: every register variant and CTA size (64, 128, 256
 // threads, within the variant's limit); for each, walkers per tile start at
-// min(threads, 128) for every system and are halved system by system
+// the largest power of two <= threads whose tile fits a CTA's shared memory
+// and are halved system by system
 // (largest shared-memory footprint first) while that makes the batch faster.
 // Each candidate is timed as the median of three launches of n_sweeps sweeps
 // with local energies every n_sweeps / 2 sweeps (not accumulated).  The
@@ -476,7 +478,15 @@ int oqmc_batch_tune(oqmc_batch* b, int n_sweeps, uint64_t seed, void* stream, fl
   for (int v = 0; v < kNumVariants; ++v) {
     for (int nt : {64, 128, 256}) {
       if (nt > kVariants[v].maxt) continue;
-      std::vector<int> wt(b->n, std::min(nt, 128));
+      // start from the largest tile (walkers = threads at most) whose shared
+      // memory fits one CTA
+      std::vector<int> wt(b->n, 32);
+      for (int k = 0; k < b->n; ++k)
+        for (int c = nt; c >= 32; c /= 2)
+          if (tile_smem(b->ctx[k]->nocc, c, nt, b->precision) <= kMaxSmem) {
+            wt[k] = c;
+            break;
+          }
       float cur;
       if (oqmc_batch_configure(b, nt, wt.data(), v) != OQ_OK) continue;
       launch(b, 2, 2, seed, 0, s);   // first launch of this variant: module warm-up
