@@ -278,6 +278,53 @@ int oqmc_batch_get_flags(oqmc_batch* b, unsigned* flags, int clear, void* stream
 int oqmc_batch_source_desc(const oqmc_system_desc* descs, int n, char* buf, size_t cap,
                            size_t* len);
 
+/* ------------------------------------------------------------------------
+ * Learned Metropolis proposal.  No counterpart in the reference, whose
+ * proposal is the plain Gaussian random walk (metropolis_move_alle,
+ * OmegaQMC/vmc_gto.py:815-839).  A per-electron MLP (32 features -> 128 ->
+ * 128 -> 128 -> 48, ReLU, BF16 weights and activations, FP32 accumulation on
+ * the tcgen05 tensor cores) outputs an 8-component isotropic Gaussian
+ * mixture for the electron's displacement; moves are accepted with the
+ * exact ratio |psi'|^2 q(x|x') / (|psi|^2 q(x'|x)) (the Metropolis-Hastings
+ * form of metropolis_move_1w, vmc_gto.py:841-905, as the basin move uses it,
+ * vmc_gto.py:925-957).  Parameters are a flat FP32 vector of
+ * oqmc_mlp_num_params() values: W1[128][32] b1 W2[128][128] b2 W3[128][128]
+ * b3 W4[48][128] b4.  Features of electron e: position relative to the
+ * nearest and second-nearest nucleus (6), displacements to the 8 nearest
+ * other electrons (24, nearest first), spin (+1 up / -1 down), 1.
+ * Outputs: logits 0..7, means 8..31, sigma_c = 0.02 + softplus(out[32+c]).
+ * ---------------------------------------------------------------------- */
+typedef struct oqmc_mlp oqmc_mlp;
+
+int oqmc_mlp_num_params(void);
+/* Allocate on the current device with He-uniform weights (seeded). */
+int oqmc_mlp_create(oqmc_mlp** out, uint64_t seed);
+int oqmc_mlp_destroy(oqmc_mlp* m);
+const char* oqmc_mlp_last_error(const oqmc_mlp* m);
+/* FP32 parameters to/from host memory (set also resets the Adam state). */
+int oqmc_mlp_get_params(oqmc_mlp* m, float* theta_host);
+int oqmc_mlp_set_params(oqmc_mlp* m, const float* theta_host);
+/* Training rows of walkers X0 (W, n_e, 3): BF16 features feat[W*n_e][32]
+ * (row = walker * n_e + electron) and, when X1 (positions some sweeps
+ * later) is given, the FP32 targets X1 - X0 in target[W*n_e][3]. */
+int oqmc_mlp_features(oqmc_ctx* ctx, const double* X0, const double* X1, int W,
+                      unsigned short* feat, float* target, void* stream);
+/* Network outputs out[R][48] (FP32) of R feature rows. */
+int oqmc_mlp_forward(oqmc_mlp* m, const unsigned short* feat, int R, float* out, void* stream);
+/* Gradient of the mean negative log-likelihood of the targets over the R
+ * rows (grad: device, num_params floats, overwritten) and the summed NLL
+ * (loss_sum: device double, may be NULL). */
+int oqmc_mlp_backward(oqmc_mlp* m, const unsigned short* feat, const float* target, int R,
+                      float* grad, double* loss_sum, void* stream);
+/* One Adam step (beta 0.9/0.999) on the mean NLL of the R rows. */
+int oqmc_mlp_step(oqmc_mlp* m, const unsigned short* feat, const float* target, int R,
+                  float lr, double* loss_sum, void* stream);
+int oqmc_mlp_get_flags(oqmc_mlp* m, unsigned* flags, int clear, void* stream);
+/* Use the network as the context's proposal in oqmc_sweeps (mixed
+ * precision, specialised context; NULL restores the previous proposal).
+ * The network is borrowed and must outlive its use. */
+int oqmc_set_mlp_proposal(oqmc_ctx* ctx, const oqmc_mlp* m);
+
 #ifdef __cplusplus
 }
 #endif

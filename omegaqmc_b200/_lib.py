@@ -113,6 +113,21 @@ _SIGS = [
     ("oqmc_batch_get_flags", c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint), c_int, c_void_p]),
     ("oqmc_batch_source_desc", c_int, [ctypes.POINTER(SystemDesc), c_int, ctypes.c_char_p,
                                        c_size_t, ctypes.POINTER(c_size_t)]),
+    ("oqmc_mlp_num_params", c_int, []),
+    ("oqmc_mlp_create", c_int, [ctypes.POINTER(c_void_p), c_uint64]),
+    ("oqmc_mlp_destroy", c_int, [c_void_p]),
+    ("oqmc_mlp_last_error", ctypes.c_char_p, [c_void_p]),
+    ("oqmc_mlp_get_params", c_int, [c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    ("oqmc_mlp_set_params", c_int, [c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    ("oqmc_mlp_features", c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
+                                  c_void_p]),
+    ("oqmc_mlp_forward", c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    ("oqmc_mlp_backward", c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
+                                  c_void_p]),
+    ("oqmc_mlp_step", c_int, [c_void_p, c_void_p, c_void_p, c_int, ctypes.c_float, c_void_p,
+                              c_void_p]),
+    ("oqmc_mlp_get_flags", c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint), c_int, c_void_p]),
+    ("oqmc_set_mlp_proposal", c_int, [c_void_p, c_void_p]),
 ]
 
 EXPORTED = [s[0] for s in _SIGS]
@@ -137,13 +152,14 @@ def load(path=None):
     return lib
 
 
-def check(code, ctx=None, batch=False):
+def check(code, ctx=None, batch=False, mlp=False):
     """Raise for a negative status, with the library's message (of a context,
-    or of a batch handle when ``batch`` is true)."""
+    of a batch handle when ``batch`` is true, of a network when ``mlp``)."""
     if code == OQ_OK:
         return
     lib = load()
-    msg = (lib.oqmc_batch_last_error(ctx) if batch else lib.oqmc_last_error(ctx))
+    msg = (lib.oqmc_batch_last_error(ctx) if batch else
+           lib.oqmc_mlp_last_error(ctx) if mlp else lib.oqmc_last_error(ctx))
     msg = msg.decode(errors="replace")
     if code == OQ_ERR_ARG:
         raise ValueError(msg)

@@ -54,7 +54,7 @@ def _run(cmd):
 
 
 RTC_HEADERS = ("oqmc_common.cuh", "oqmc_ao.cuh", "oqmc_eval.cuh", "oqmc_sweep.cuh",
-               "oqmc_batch.cuh")
+               "oqmc_batch.cuh", "oqmc_tc.cuh", "oqmc_mlp.cuh", "oqmc_mlp_sweep.cuh")
 
 
 def _embed_headers():
@@ -93,7 +93,8 @@ def build(force=False, jobs=None, verbose=False):
              (os.path.join(CSRC, "oqmc_noalloc.cu"), os.path.join(BUILD, "oqmc_noalloc.o"), []),
              (os.path.join(CSRC, "oqmc_rtc.cu"), os.path.join(BUILD, "oqmc_rtc.o"),
               ["-I" + BUILD]),
-             (os.path.join(CSRC, "oqmc_batch.cu"), os.path.join(BUILD, "oqmc_batch.o"), [])]
+             (os.path.join(CSRC, "oqmc_batch.cu"), os.path.join(BUILD, "oqmc_batch.o"), []),
+             (os.path.join(CSRC, "oqmc_mlp.cu"), os.path.join(BUILD, "oqmc_mlp.o"), [])]
     for n in NOCC_LIST:
         units.append((os.path.join(CSRC, "oqmc_inst.cu"),
                       os.path.join(BUILD, f"oqmc_inst_{n}.o"), [f"-DOQ_N={n}"]))

@@ -216,5 +216,12 @@ class GTOContext:
         """0: fixed-width Gaussian (reference); 1: nucleus-scaled width."""
         self._check(self.lib.oqmc_set_proposal(self._h, int(kind), float(r0), float(fmin_frac)))
 
+    def set_mlp_proposal(self, mlp):
+        """Propose moves with a trained :class:`~omegaqmc_b200.learned.MLPProposal`
+        (``None`` restores the previous proposal).  Needs ``specialize()``;
+        sweeps then run in mixed precision only."""
+        self._mlp = mlp
+        self._check(self.lib.oqmc_set_mlp_proposal(self._h, mlp._h if mlp is not None else None))
+
     def set_split(self, tight_alpha):
         self._check(self.lib.oqmc_set_split(self._h, float(tight_alpha)))

@@ -10,6 +10,8 @@
 
 #include "oqmc_launch.h"
 #include "oqmc_rtc.h"
+#include "oqmc_mlp_host.h"
+#include "oqmc_mlp_sweep.cuh"
 #include "../../include/oqmc_b200.h"
 
 #include "oqmc_ctx.h"
@@ -283,6 +285,7 @@ extern "C" int oqmc_create(oqmc_ctx** out, const oqmc_system_desc* d) {
 int oqmc_destroy(oqmc_ctx* ctx) {
   if (!ctx) return OQ_OK;
   oq_spec_destroy(ctx->spec);
+  oq_rtc_unload(ctx->mlp_mod);
   cudaFree(ctx->d_Btc);
   delete[] ctx->h_C;
   cudaFree(ctx->d_sys);
@@ -300,6 +303,33 @@ int oqmc_set_proposal(oqmc_ctx* ctx, int kind, double r0, double fmin_frac) {
     return set_err(ctx, OQ_ERR_ARG, "bad proposal parameters%s");
   ctx->proposal = kind;
   if (kind == 1) { ctx->scale_r0 = r0; ctx->scale_fmin = fmin_frac; }
+  return OQ_OK;
+}
+
+int oqmc_set_mlp_proposal(oqmc_ctx* ctx, const oqmc_mlp* m) {
+  if (!ctx) return OQ_ERR_ARG;
+  if (!m) {
+    ctx->mlp = nullptr;
+    return OQ_OK;
+  }
+  if (!ctx->spec)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED,
+                   "the learned proposal needs a specialised context (oqmc_specialize)%s");
+  if (ctx->n_e > 32 || oq_mlp_sweep_smem(ctx->nocc) > 232448)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED,
+                   "walker state and network do not fit one CTA's shared memory%s");
+  if (!ctx->mlp_fn) {
+    const std::string src = std::string("#include \"oqmc_mlp_sweep.cuh\"\n\n") +
+                            oq_spec_basis_source(ctx->hsys, ctx->hsplit, ctx->h_C, ctx->nocc,
+                                                 "OqSpecBasis");
+    std::vector<void*> fns;
+    std::string err;
+    if (oq_rtc_build(src, {"k_moves_mlp<" + std::to_string(ctx->nocc) + ", OqSpecBasis>"},
+                     &ctx->mlp_mod, &fns, &err) != 0)
+      return set_err(ctx, OQ_ERR_UNSUPPORTED, "%s", err.c_str());
+    ctx->mlp_fn = fns[0];
+  }
+  ctx->mlp = m;
   return OQ_OK;
 }
 
@@ -377,6 +407,16 @@ int oqmc_set_split(oqmc_ctx* ctx, double tight_alpha) {
   if (ctx->spec) {   // the specialised kernels carry the split radii as literals
     const int rc = oqmc_specialize(ctx, 1);
     if (rc != OQ_OK) return rc;
+  }
+  if (ctx->mlp_mod) {   // so does the learned-proposal kernel: rebuild it
+    oq_rtc_unload(ctx->mlp_mod);
+    ctx->mlp_mod = ctx->mlp_fn = nullptr;
+    const oqmc_mlp* m = ctx->mlp;
+    ctx->mlp = nullptr;
+    if (m) {
+      const int rc = oqmc_set_mlp_proposal(ctx, m);
+      if (rc != OQ_OK) return rc;
+    }
   }
   OQ_CUDA(ctx, cudaMemcpy(ctx->d_split, &ctx->hsplit, sizeof(OqSplit), cudaMemcpyHostToDevice));
   return OQ_OK;
@@ -538,6 +578,16 @@ static int launch_moves(oqmc_ctx* ctx, const OqMoveArgs& m, int wpb, size_t sm, 
                         void* stream) {
   const OqLaunch L = make_launch(ctx, stream, sm);
   const int mixed = precision == OQ_PREC_MIXED;
+  if (ctx->mlp && m.mode == 0) {
+    OqMoveArgs mm = m;
+    const void* C = (const void*)ctx->d_C32;
+    OqMlpWeights nw{ctx->mlp->wbf, ctx->mlp->theta};
+    void* args[5] = {(void*)&L.sys, (void*)&L.split, (void*)&C, (void*)&mm, (void*)&nw};
+    if (oq_rtc_launch(ctx->mlp_fn, dim3((m.W + 127) / 128), dim3(128),
+                      oq_mlp_sweep_smem(ctx->nocc), L.stream, args) != 0)
+      return set_err(ctx, OQ_ERR_CUDA, "learned-proposal move kernel launch failed%s");
+    return OQ_OK;
+  }
   if (ctx->spec && m.mode == 0) {
     OqMoveArgs mm = m;
     const void* C = mixed ? (const void*)ctx->d_C32 : (const void*)ctx->d_C64;
@@ -566,6 +616,8 @@ int oqmc_sweeps(oqmc_ctx* ctx, double* X, int W, void* state, int precision, int
   if (W == 0 || n_sweeps == 0) return OQ_OK;
   if (!X || !state || (n_sweeps >= measure_every && !sums))
     return set_err(ctx, OQ_ERR_ARG, "null buffer%s");
+  if (ctx->mlp && precision != OQ_PREC_MIXED)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED, "the learned proposal runs in mixed precision only%s");
   size_t sm;
   wpb = pick_wpb(ctx, wpb, precision, &sm);
   if (wpb == -1) return set_err(ctx, OQ_ERR_ARG, "walkers_per_block must be 32, 64 or 128%s");

@@ -22,6 +22,9 @@ struct oqmc_ctx {
   unsigned char* d_Btc;   // split MO-coefficient operands of k_eloc_tc
   double* h_C;            // host copy of the MO coefficients (for specialisation)
   double scale_r0, scale_fmin;
+  const struct oqmc_mlp* mlp;   // learned proposal (borrowed), or null
+  void* mlp_mod;                // its specialised sweep kernel (module, function)
+  void* mlp_fn;
   char err[512];
 };
 

@@ -10,7 +10,8 @@ from . import _lib as L
 from .context import pack_system
 
 CSRC = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc")
-HEADERS = ("oqmc_common.cuh", "oqmc_ao.cuh", "oqmc_eval.cuh", "oqmc_sweep.cuh", "oqmc_batch.cuh")
+HEADERS = ("oqmc_common.cuh", "oqmc_ao.cuh", "oqmc_eval.cuh", "oqmc_sweep.cuh", "oqmc_batch.cuh",
+           "oqmc_tc.cuh", "oqmc_mlp.cuh", "oqmc_mlp_sweep.cuh")
 
 
 def spec_source(system):
@@ -78,6 +79,13 @@ def compile_source(src, names):
         cubin = cb.raw
     nv.nvrtcDestroyProgram(ctypes.byref(prog))
     return rc == 0, log.value.decode(errors="replace"), cubin
+
+
+def compile_mlp_sweep(system):
+    """NVRTC-compile the learned-proposal sweep kernel of ``system`` (the
+    source oqmc_set_mlp_proposal builds); returns (ok, log, cubin bytes)."""
+    src = spec_source(system).replace('#include "oqmc_sweep.cuh"', '#include "oqmc_mlp_sweep.cuh"')
+    return compile_source(src, [f"k_moves_mlp<{system.nocc}, OqSpecBasis>"])
 
 
 def compile_spec(system):
