@@ -58,9 +58,10 @@ def parse():
     ap.add_argument("--proposal", default="scaled", choices=["scaled", "plain"])
     ap.add_argument("--eloc", default="cc", choices=["cc", "tc"],
                     help="local energy on CUDA cores (specialised) or tensor cores (tcgen05)")
-    ap.add_argument("--workload", default="h2o", choices=["h2o", "batched"],
+    ap.add_argument("--workload", default="h2o", choices=["h2o", "batched", "learned"],
                     help="h2o: the headline H2O metric; batched: H2, LiH, H2O, N2 and "
-                         "(H2O)2 in one persistent launch under a CUDA graph")
+                         "(H2O)2 in one persistent launch under a CUDA graph; learned: N2 "
+                         "with the trained MLP proposal against the plain random walk")
     ap.add_argument("--quick", action="store_true",
                     help="profiling mode: no equilibration, comparison, e2e or CPU legs")
     return ap.parse_args()
@@ -628,6 +629,139 @@ def run_batched(a):
         dist.destroy_process_group()
 
 
+MLP_FLOPS_PER_ROW = 2 * (32 * 128 + 2 * 128 * 128 + 128 * 48)   # one forward pass
+
+
+def run_learned(a):
+    """N2 cc-pVDZ-shaped, 32,768 walkers, mixed precision: the plain
+    fixed-width random walk against the learned MLP proposal at equal GPU
+    time.  The network is trained (own tcgen05 kernels) on 10^6 walker
+    configurations the plain sampler produced, targets = 8-sweep
+    displacements.
+
+    value = decorrelated samples/s of the learned sampler (walker-sweeps/s /
+    tau_int of E_L); the plain sampler's figure and the ratio are reported
+    beside it."""
+    import torch
+    import torch.distributed as dist
+    from omegaqmc_b200 import _lib as L
+    from omegaqmc_b200.context import GTOContext
+    from omegaqmc_b200.learned import MLPProposal, collect_training_set, train_proposal
+    from omegaqmc_b200.sampler import WalkerEnsemble, init_walkers_gaussian, NSUM
+    from oracle import gto_oracle as O  # noqa: F401  (tau estimator)
+
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    system = build_system("N2")
+    ctx = GTOContext(system)
+    ctx.specialize()
+    W = 32768 if a.walkers == 65536 else a.walkers
+    ens = WalkerEnsemble(ctx, init_walkers_gaussian(system, W, 1.0, seed=31 + rank), "mixed",
+                         seed=2025 + 7919 * rank, refresh_every=REFRESH_EVERY)
+    step = a.step_size or adapt_step(ens, STEP_DEFAULT["N2"])
+    ens.run(0 if a.quick else EQUIL_SWEEPS, step)
+    stream = torch.cuda.current_stream()
+
+    def timed(e, n):
+        sums = torch.zeros(n, NSUM, dtype=torch.float64, device=dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e.run(n, step, sums=sums)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sn = sums.cpu().numpy()
+        ser = sn[:, 3] / np.maximum(sn[:, 6], 1)
+        m, se, _, kap = O.binning_analysis(ser)
+        return (e0.elapsed_time(e1), m, se, kap, float(sn[:, 5].sum() / (n * W * system.n_e)))
+
+    # training data and training (timed with events, outside the comparison)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t2 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    feat, tgt = collect_training_set(ens, 10**6, 8, step)
+    t1.record(stream)
+    mlp = MLPProposal(seed=11 + rank)
+    n_train, batch = 2000, 8192
+    hist = train_proposal(mlp, feat, tgt, steps=n_train, batch=batch, lr=2e-3, log_every=500)
+    t2.record(stream)
+    torch.cuda.synchronize()
+    rows = int(feat.shape[0])
+    del feat, tgt
+    collect_ms, train_ms = t0.elapsed_time(t1), t1.elapsed_time(t2)
+
+    # equal GPU time: the plain sampler for K_p sweeps, the learned one for
+    # as many sweeps as fit in the same time
+    K_p = max(a.steps, 1000) * 5
+    ens.run(max(a.warmup, 3), step)
+    with ClockSampler(local) as clk:
+        ms_p, e_p, se_p, tau_p, acc_p = timed(ens, K_p)
+        lens = WalkerEnsemble(ctx, ens.X, "mixed", seed=99 + rank, refresh_every=REFRESH_EVERY)
+        ctx.set_mlp_proposal(mlp)
+        lens.run(max(a.warmup // 10, 3), step)
+        probe_ms = timed(lens, 20)[0] / 20
+        K_l = max(50, int(ms_p / probe_ms))
+        ms_l, e_l, se_l, tau_l, acc_l = timed(lens, K_l)
+    flags = (ctx.flags(), mlp.flags())
+    ctx.set_mlp_proposal(None)
+    t = torch.tensor([ms_l, ms_p], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_l, ms_p = float(t[0]), float(t[1])
+    wss_l = W * world * K_l / (ms_l * 1e-3)
+    wss_p = W * world * K_p / (ms_p * 1e-3)
+    value = wss_l / tau_l
+    plain = wss_p / tau_p
+    mlp_flops = 2.0 * system.n_e * W * K_l * MLP_FLOPS_PER_ROW
+    bf16_peak = None
+    peaks = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks):
+        bf16_peak = json.load(open(peaks)).get("bf16_tflops")
+    ach = mlp_flops / (ms_l * 1e-3) / 1e12
+    train_tflops = 3.0 * n_train * batch * MLP_FLOPS_PER_ROW / (train_ms * 1e-3) / 1e12
+    line = {
+        "metric": "decorrelated samples/s (walker-steps/s / tau_int), learned MLP proposal vs "
+                  "plain random walk at equal GPU time, N2 32k walkers",
+        "value": value, "unit": "decorrelated samples/s", "n_gpus": world, "steps": K_l,
+        "warmup": a.warmup, "ms_per_step": ms_l / K_l, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (network) + f32/f64 (psi)",
+        "data": "synthetic",
+        "config": {"workload": f"N2 cc-pVDZ-shaped, {W} walkers/GPU, mixed precision, "
+                               "single-electron sweeps + E_L every sweep",
+                   "network": "per-electron MLP 32->128->128->128->48 (ReLU), 8-component "
+                              "Gaussian mixture, BF16 on tcgen05",
+                   "training": f"{rows} rows from 10^6 plain-sampler configurations "
+                               f"(8-sweep displacements), {n_train} Adam steps x {batch}",
+                   "equal_time": f"plain {K_p} sweeps vs learned {K_l} sweeps",
+                   "parallelism": f"replicas x{world}"},
+        "learned": {"tau_int": tau_l, "acceptance": acc_l, "energy": {"mean": e_l, "serr": se_l},
+                    "ms_per_sweep": ms_l / K_l, "walker_sweeps_per_s": wss_l},
+        "plain_random_walk": {"value": plain, "tau_int": tau_p, "acceptance": acc_p,
+                              "energy": {"mean": e_p, "serr": se_p}, "step": step,
+                              "ms_per_sweep": ms_p / K_p, "walker_sweeps_per_s": wss_p},
+        "gain_equal_time": value / plain, "gain_per_sweep": tau_p / tau_l,
+        "energy_diff_sigma": abs(e_l - e_p) / max(np.hypot(se_l, se_p), 1e-300),
+        "training": {"collect_ms": collect_ms, "train_ms": train_ms, "loss": hist,
+                     "train_tflops": train_tflops},
+        "kernel_flags": list(flags),
+        "gpu_launches": int(math.ceil(K_l / REFRESH_EVERY)) * 2,
+        "roofline": {"bound": "tensor", "achieved": ach, "peak": bf16_peak, "unit": "TFLOP/s",
+                     "frac": ach / bf16_peak if bf16_peak else None, "traffic": None,
+                     "kernel": "k_moves_mlp (network flops only, two passes per move)",
+                     "peak_source": "MEASURED_PEAKS.json bf16_tflops, of measured"},
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def ctypes_peak(L, kind):
     import ctypes
     import torch
@@ -653,6 +787,8 @@ def main():
         run_reference(a)
     elif a.workload == "batched":
         run_batched(a)
+    elif a.workload == "learned":
+        run_learned(a)
     else:
         run_ours(a)
 

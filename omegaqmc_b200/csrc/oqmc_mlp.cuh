@@ -119,30 +119,38 @@ __device__ __forceinline__ void oq_mlp_pre_issue() {
 // Hidden-layer epilogue: row r of D (TMEM lane r) + bias, ReLU, BF16 into
 // the K-major buffer `act` (KC = 16).  Optionally also into the transposed
 // buffer `ht` ([128 features x 128 rows], KC = 16) and a 128-bit ReLU mask.
+// Columns are read 64 at a time (four loads in flight, one wait).
 __device__ __forceinline__ void oq_mlp_hidden_epilogue(uint32_t tmem_row, const float* bias,
                                                        unsigned char* act, int r,
                                                        unsigned char* ht, uint32_t* mask) {
 #pragma unroll 1
-  for (int c0 = 0; c0 < OQ_MLP_H; c0 += 16) {
-    float v[16];
-    oq_tmem_ld16(tmem_row + (uint32_t)c0, v);
-    uint32_t mbits = 0;
+  for (int h0 = 0; h0 < OQ_MLP_H; h0 += 64) {
+    uint32_t raw[64];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const float z = v[j] + bias[c0 + j];
-      v[j] = z > 0.0f ? z : 0.0f;
-      mbits |= (z > 0.0f ? 1u : 0u) << j;
-    }
-    oq_mlp_store_row16(act, r, c0, 16, v);
-    if (mask) mask[c0 >> 5] |= mbits << (c0 & 16);
-    if (ht) {
+    for (int q = 0; q < 4; ++q) oq_tmem_ld16_nw(tmem_row + (uint32_t)(h0 + 16 * q), raw + 16 * q);
+    oq_tmem_wait_ld();
 #pragma unroll
-      for (int j = 0; j < 16; j += 2) {
-        const uint32_t p = oq_bf16x2(v[j], v[j + 1]);
-        *reinterpret_cast<unsigned short*>(ht + oq_kmajor_off2(c0 + j, r, 16)) =
-            (unsigned short)(p & 0xFFFFu);
-        *reinterpret_cast<unsigned short*>(ht + oq_kmajor_off2(c0 + j + 1, r, 16)) =
-            (unsigned short)(p >> 16);
+    for (int q = 0; q < 4; ++q) {
+      const int c0 = h0 + 16 * q;
+      float v[16];
+      uint32_t mbits = 0;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const float z = __uint_as_float(raw[16 * q + j]) + bias[c0 + j];
+        v[j] = z > 0.0f ? z : 0.0f;
+        mbits |= (z > 0.0f ? 1u : 0u) << j;
+      }
+      oq_mlp_store_row16(act, r, c0, 16, v);
+      if (mask) mask[c0 >> 5] |= mbits << (c0 & 16);
+      if (ht) {
+#pragma unroll
+        for (int j = 0; j < 16; j += 2) {
+          const uint32_t p = oq_bf16x2(v[j], v[j + 1]);
+          *reinterpret_cast<unsigned short*>(ht + oq_kmajor_off2(c0 + j, r, 16)) =
+              (unsigned short)(p & 0xFFFFu);
+          *reinterpret_cast<unsigned short*>(ht + oq_kmajor_off2(c0 + j + 1, r, 16)) =
+              (unsigned short)(p >> 16);
+        }
       }
     }
   }
@@ -151,13 +159,12 @@ __device__ __forceinline__ void oq_mlp_hidden_epilogue(uint32_t tmem_row, const 
 // Output epilogue: 48 FP32 outputs of row r.
 __device__ __forceinline__ void oq_mlp_out_epilogue(uint32_t tmem_row, const float* bias,
                                                     float out[OQ_MLP_NOUT]) {
+  uint32_t raw[OQ_MLP_NOUT];
 #pragma unroll
-  for (int c0 = 0; c0 < OQ_MLP_NOUT; c0 += 16) {
-    float v[16];
-    oq_tmem_ld16(tmem_row + (uint32_t)c0, v);
+  for (int q = 0; q < OQ_MLP_NOUT / 16; ++q) oq_tmem_ld16_nw(tmem_row + (uint32_t)(16 * q), raw + 16 * q);
+  oq_tmem_wait_ld();
 #pragma unroll
-    for (int j = 0; j < 16; ++j) out[c0 + j] = v[j] + bias[c0 + j];
-  }
+  for (int j = 0; j < OQ_MLP_NOUT; ++j) out[j] = __uint_as_float(raw[j]) + bias[j];
 }
 
 // Load biases b1..b3 (128 each) and b4 (48) from the FP32 parameter vector.
@@ -254,6 +261,72 @@ __device__ __forceinline__ void oq_mix_sample(const float out[OQ_MLP_NOUT], doub
   d[0] = out[8 + 3 * sel] + sg * n3[0];
   d[1] = out[9 + 3 * sel] + sg * n3[1];
   d[2] = out[10 + 3 * sel] + sg * n3[2];
+}
+
+// FP32 versions for the sampler (fast exponentials; the proposal density is
+// evaluated by the same function that defines the draw's mixture, so the
+// rounding enters the acceptance ratio at the 1e-6 level only).
+__device__ __forceinline__ float oq_softplus_f(float x) {
+  return x > 20.0f ? x : __logf(1.0f + __expf(x));
+}
+
+__device__ __forceinline__ float oq_mix_logq_f(const float out[OQ_MLP_NOUT], float dx, float dy,
+                                               float dz) {
+  float amax = out[0];
+#pragma unroll
+  for (int c = 1; c < OQ_MLP_NMIX; ++c) amax = fmaxf(amax, out[c]);
+  float zs = 0.0f;
+#pragma unroll
+  for (int c = 0; c < OQ_MLP_NMIX; ++c) zs += __expf(out[c] - amax);
+  const float lz = amax + __logf(zs);
+  float L[OQ_MLP_NMIX], lmax = -3.0e38f;
+#pragma unroll
+  for (int c = 0; c < OQ_MLP_NMIX; ++c) {
+    const float sg = (float)OQ_MLP_SIGMIN + oq_softplus_f(out[32 + c]);
+    const float ex = dx - out[8 + 3 * c], ey = dy - out[9 + 3 * c], ez = dz - out[10 + 3 * c];
+    const float is = 1.0f / sg;
+    L[c] = out[c] - lz + 3.0f * __logf(is) - 2.7568156f - 0.5f * (ex * ex + ey * ey + ez * ez) * is * is;
+    lmax = fmaxf(lmax, L[c]);
+  }
+  float s = 0.0f;
+#pragma unroll
+  for (int c = 0; c < OQ_MLP_NMIX; ++c) s += __expf(L[c] - lmax);
+  return lmax + __logf(s);
+}
+
+__device__ __forceinline__ void oq_mix_sample_f(const float out[OQ_MLP_NOUT], float uc,
+                                                const double n3[3], double d[3]) {
+  float amax = out[0];
+#pragma unroll
+  for (int c = 1; c < OQ_MLP_NMIX; ++c) amax = fmaxf(amax, out[c]);
+  float w[OQ_MLP_NMIX], zs = 0.0f;
+#pragma unroll
+  for (int c = 0; c < OQ_MLP_NMIX; ++c) {
+    w[c] = __expf(out[c] - amax);
+    zs += w[c];
+  }
+  // component: first c whose cumulative weight exceeds uc (branch-free scan)
+  const float thr = uc * zs;
+  int sel = OQ_MLP_NMIX - 1;
+  float acc = 0.0f;
+  bool found = false;
+#pragma unroll
+  for (int c = 0; c < OQ_MLP_NMIX; ++c) {
+    acc += w[c];
+    const bool hit = !found && acc > thr;
+    sel = hit ? c : sel;
+    found = found || hit;
+  }
+  float sg = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
+#pragma unroll
+  for (int c = 0; c < OQ_MLP_NMIX; ++c)
+    if (c == sel) {
+      sg = (float)OQ_MLP_SIGMIN + oq_softplus_f(out[32 + c]);
+      mx = out[8 + 3 * c]; my = out[9 + 3 * c]; mz = out[10 + 3 * c];
+    }
+  d[0] = (double)(mx + sg * (float)n3[0]);
+  d[1] = (double)(my + sg * (float)n3[1]);
+  d[2] = (double)(mz + sg * (float)n3[2]);
 }
 
 // Negative log-likelihood of target d and its gradient with respect to the

@@ -8,7 +8,7 @@
 //   1. every thread writes the features of its walker's electron e and the
 //      CTA runs the network on the tensor cores -> mixture q(. | x);
 //   2. the thread draws the displacement d (component from a uniform, then
-//      mu + sigma * N(0, 1)) and evaluates log q(d | x);
+//      mu + sigma * N(0, 1)) and evaluates log q(d | x) (FP32 mixture math);
 //   3. features at x' = x + d -> network -> log q(-d | x');
 //   4. oq_try_move accepts with |psi(x')/psi(x)|^2 q(x|x') / q(x'|x)
 //      (Sherman-Morrison update on acceptance).
@@ -81,7 +81,7 @@ k_moves_mlp(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gspli
       oq_move_randoms(a.seed, (uint32_t)w, gstep, (uint32_t)e, n3, u);
       const OqU4 c2 = {(uint32_t)w, gstep, (uint32_t)e, 2u};
       const OqU4 rc = oq_philox(c2, (uint32_t)a.seed, (uint32_t)(a.seed >> 32));
-      const double uc = ((double)rc.x + 0.5) * 2.3283064365386963e-10;
+      const float uc = ((float)rc.x + 0.5f) * 2.3283064365386963e-10f;
       const double ox = P(e, 0), oy = P(e, 1), oz = P(e, 2);
       float f[OQ_MLP_K0], out[OQ_MLP_NOUT];
       oq_mlp_features(J, P, NE, e, ox, oy, oz, f);
@@ -89,17 +89,17 @@ k_moves_mlp(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gspli
       ok = oq_mlp_forward_tile(act, wreg, bias, tmem, sy, out, nullptr, nullptr);
       if (!ok) break;
       double d[3];
-      oq_mix_sample(out, uc, n3, d);
+      oq_mix_sample_f(out, uc, n3, d);
       const double nx = ox + d[0], ny = oy + d[1], nz = oz + d[2];
-      const double lqf = oq_mix_logq(out, nx - ox, ny - oy, nz - oz);
+      const float lqf = oq_mix_logq_f(out, (float)(nx - ox), (float)(ny - oy), (float)(nz - oz));
       oq_mlp_features(J, P, NE, e, nx, ny, nz, f);
       oq_mlp_store_features(act, tid, f);
       ok = oq_mlp_forward_tile(act, wreg, bias, tmem, sy, out, nullptr, nullptr);
       if (!ok) break;
-      const double lqr = oq_mix_logq(out, ox - nx, oy - ny, oz - nz);
+      const float lqr = oq_mix_logq_f(out, (float)(ox - nx), (float)(oy - ny), (float)(oz - nz));
       if (live)
         nacc += oq_try_move<NOCC, float, float, B>(J, S, SP, C, pos, Ai, WT, tid, e, nx, ny, nz,
-                                                   lqr - lqf, u, logdet);
+                                                   (double)(lqr - lqf), u, logdet);
     }
   }
   if (live) {

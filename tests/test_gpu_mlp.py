@@ -117,17 +117,18 @@ def _tau_energy(sums):
 
 
 def test_learned_proposal_is_exact_and_decorrelates_faster(n2):
-    """N2, 4096 walkers: the plain fixed-width sampler and the learned
-    proposal sample the same |psi|^2 (energies agree) and the learned one
-    has a much shorter autocorrelation time of E_L per sweep and per second."""
+    """N2, 16384 walkers: the plain fixed-width sampler and the learned
+    proposal sample the same |psi|^2 (energies agree), and the learned one
+    has a much shorter autocorrelation time of E_L per sweep and more
+    decorrelated samples per second of GPU time."""
     s, ctx = n2
     ctx.specialize()
-    W = 4096
+    W = 16384
     ens = WalkerEnsemble(ctx, seeded_walkers(s, W, 1.0, 9), "mixed", seed=21)
-    step = 0.3
-    ens.run(2000, step)
+    step = 0.5
+    ens.run(3000, step)
     # plain sampler: the comparison (and the source of the training data)
-    n_plain = 3000
+    n_plain = 6000
     sp = torch.zeros(n_plain, NSUM, dtype=torch.float64, device="cuda")
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -136,15 +137,16 @@ def test_learned_proposal_is_exact_and_decorrelates_faster(n2):
     torch.cuda.synchronize()
     t_plain = e0.elapsed_time(e1) / n_plain
     mp, sep, kp, _ = _tau_energy(sp)
-    feat, tgt = collect_training_set(ens, 400000, 8, step)
+    feat, tgt = collect_training_set(ens, 10**6, 8, step)
     mlp = MLPProposal(seed=3)
-    train_proposal(mlp, feat, tgt, steps=1500, batch=8192, lr=2e-3)
+    train_proposal(mlp, feat, tgt, steps=2000, batch=8192, lr=2e-3)
+    del feat, tgt
     # learned proposal on a copy of the equilibrated walkers
     lens = WalkerEnsemble(ctx, ens.X, "mixed", seed=77)
     ctx.set_mlp_proposal(mlp)
     try:
         lens.run(100, step)
-        n_l = 600
+        n_l = 800
         sl = torch.zeros(n_l, NSUM, dtype=torch.float64, device="cuda")
         e0.record()
         lens.run(n_l, step, sums=sl)
@@ -156,8 +158,8 @@ def test_learned_proposal_is_exact_and_decorrelates_faster(n2):
     ml, sel, kl, accl = _tau_energy(sl)
     acc = accl / (n_l * W * s.n_e)
     assert ctx.flags() == 0 and mlp.flags() == 0
-    assert acc > 0.05
+    assert acc > 0.2
     assert abs(ml - mp) < 4.0 * np.hypot(sel, sep), (ml, sel, mp, sep)
-    assert kl < kp / 2.0, (kl, kp)
+    assert kl < kp / 5.0, (kl, kp)
     # decorrelated samples per second: W / (tau * seconds per sweep)
-    assert (1.0 / (kl * t_l)) > (1.0 / (kp * t_plain)), (kl, t_l, kp, t_plain)
+    assert (1.0 / (kl * t_l)) > 1.5 * (1.0 / (kp * t_plain)), (kl, t_l, kp, t_plain)
