@@ -502,10 +502,12 @@ def run_batched(a):
     if world > 1:
         dist.barrier()
     with ClockSampler(local) as clk:
+        torch.cuda.nvtx.range_push("batched_timed")
         ev0.record(stream)
         b.replay()
         ev1.record(stream)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
     ms = ev0.elapsed_time(ev1)
     busy = b.busy_ns()
     flags = b.flags()
@@ -683,12 +685,15 @@ def run_learned(a):
     t1 = torch.cuda.Event(enable_timing=True)
     t2 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
-    feat, tgt = collect_training_set(ens, 10**6, 8, step)
+    n_cfg = 10**5 if a.quick else 10**6
+    feat, tgt = collect_training_set(ens, n_cfg, 8, step)
     t1.record(stream)
     mlp = MLPProposal(seed=11 + rank)
-    n_train, batch = 2000, 8192
+    n_train, batch = (300 if a.quick else 2000), 8192
+    torch.cuda.nvtx.range_push("mlp_train")
     hist = train_proposal(mlp, feat, tgt, steps=n_train, batch=batch, lr=2e-3, log_every=500)
     t2.record(stream)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     rows = int(feat.shape[0])
     del feat, tgt
@@ -696,7 +701,7 @@ def run_learned(a):
 
     # equal GPU time: the plain sampler for K_p sweeps, the learned one for
     # as many sweeps as fit in the same time
-    K_p = max(a.steps, 1000) * 5
+    K_p = a.steps if a.quick else max(a.steps, 1000) * 5
     ens.run(max(a.warmup, 3), step)
     with ClockSampler(local) as clk:
         ms_p, e_p, se_p, tau_p, acc_p = timed(ens, K_p)
@@ -705,7 +710,9 @@ def run_learned(a):
         lens.run(max(a.warmup // 10, 3), step)
         probe_ms = timed(lens, 20)[0] / 20
         K_l = max(50, int(ms_p / probe_ms))
+        torch.cuda.nvtx.range_push("learned_timed")
         ms_l, e_l, se_l, tau_l, acc_l = timed(lens, K_l)
+        torch.cuda.nvtx.range_pop()
     flags = (ctx.flags(), mlp.flags())
     ctx.set_mlp_proposal(None)
     t = torch.tensor([ms_l, ms_p], dtype=torch.float64, device=dev)
@@ -734,7 +741,7 @@ def run_learned(a):
                                "single-electron sweeps + E_L every sweep",
                    "network": "per-electron MLP 32->128->128->128->48 (ReLU), 8-component "
                               "Gaussian mixture, BF16 on tcgen05",
-                   "training": f"{rows} rows from 10^6 plain-sampler configurations "
+                   "training": f"{rows} rows from {n_cfg} plain-sampler configurations "
                                f"(8-sweep displacements), {n_train} Adam steps x {batch}",
                    "equal_time": f"plain {K_p} sweeps vs learned {K_l} sweeps",
                    "parallelism": f"replicas x{world}"},
