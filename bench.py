@@ -4,17 +4,23 @@ One step = one sweep of all walkers: every electron proposes a single-electron
 Gaussian move (exact Metropolis acceptance, Sherman-Morrison inverse update),
 then the local energy of every walker is evaluated and reduced.  A full FP64
 LU refresh of each inverse runs every 50 sweeps inside the timed region.
+Default path: one fused persistent launch per 50 sweeps (refresh, moves,
+local energies; the batched entry points with one molecule), the timed
+launches replayed from a CUDA graph; --path split runs the separate move and
+local-energy kernels through oqmc_sweeps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--precision mixed|fp64] [--system H2O] [--walkers 65536]
+                    [--path persistent|split] [--workload h2o|batched|learned]
 
 value     = walkers x sweeps/s / tau_int(E_L)  (decorrelated samples/s, all ranks)
 tau_int   = kappa of the reference's do_binning_analysis (OmegaQMC/utils.py:86-150)
             on the walker-mean E_L series (sweeps); from the timed series when it
             has >= 1000 sweeps, else from an untimed 2000-sweep run.
-e2e       = the same metric through the public API with host buffers: every step
-            copies the walker positions host->device (pinned), runs the sweep
-            and copies positions + the step's reductions back.
+e2e       = the same metric through the public API with host buffers: every call
+            copies the walker positions host->device (pinned), runs its sweeps
+            (50 per call on the persistent path, 1 on the split path) and copies
+            positions + the reductions back.
 --impl reference  times the reference algorithm (all-electron moves, log|psi|
             recomputed twice per step, E_L every step) restated in C/OpenMP on
             all host cores.
@@ -40,6 +46,10 @@ sys.path.insert(0, ROOT)
 REFRESH_EVERY = 50
 EQUIL_SWEEPS = 3000
 SCALED_R0, SCALED_FMIN = 1.0, 0.05
+# nucleus-scaled proposal of the persistent headline path (chosen by measured
+# tau_int on H2O: fmin 0.02 and acceptance 0.5 gave tau 1.5 sweeps, against
+# 2.4 for fmin 0.05 and 4.1 at the reference's 0.4 target)
+HEAD_R0, HEAD_FMIN, HEAD_ACC = 1.0, 0.02, 0.5
 
 
 def parse():
@@ -62,6 +72,9 @@ def parse():
                     help="h2o: the headline H2O metric; batched: H2, LiH, H2O, N2 and "
                          "(H2O)2 in one persistent launch under a CUDA graph; learned: N2 "
                          "with the trained MLP proposal against the plain random walk")
+    ap.add_argument("--path", default="persistent", choices=["persistent", "split"],
+                    help="persistent: one fused launch per 50 sweeps (refresh, moves, E_L) "
+                         "under a CUDA graph; split: separate move / local-energy kernels")
     ap.add_argument("--quick", action="store_true",
                     help="profiling mode: no equilibration, comparison, e2e or CPU legs")
     return ap.parse_args()
@@ -434,6 +447,252 @@ def run_ours(a):
         dist.destroy_process_group()
 
 
+def run_persistent(a):
+    """The headline: one molecule through the fused persistent kernel (the
+    batched entry points with a single system).  Each launch = FP64 LU
+    refresh + 50 single-electron sweeps with E_L every sweep; the timed
+    region replays a CUDA graph of K/50 launches.  The plain FP64 sampler
+    (fixed-width Gaussian, the reference's 0.4 acceptance rule) runs through
+    the same path for the comparison."""
+    import torch
+    import torch.distributed as dist
+    from omegaqmc_b200 import _lib as L
+    from omegaqmc_b200.batch import BatchedSampler
+    from omegaqmc_b200.context import GTOContext
+    from omegaqmc_b200.sampler import WalkerEnsemble, init_walkers_gaussian, NSUM
+    from oracle import gto_oracle as O  # noqa: F401  (tau estimator is the oracle's restatement)
+
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    system = build_system(a.system)
+    ctx = GTOContext(system)
+    t_spec = time.perf_counter()
+    ctx.specialize()
+    W = a.walkers
+    K = max(REFRESH_EVERY, (a.steps // REFRESH_EVERY) * REFRESH_EVERY)
+    n_launch = K // REFRESH_EVERY
+    seed = 2024 + 7919 * rank
+    scaled = a.proposal == "scaled"
+    X0 = init_walkers_gaussian(system, W, 1.0, seed=1000 + rank)
+    b = BatchedSampler([ctx], [X0], [a.step_size or 0.8], precision=a.precision,
+                       proposal=a.proposal, scale_r0=HEAD_R0, scale_fmin=HEAD_FMIN,
+                       cap=max(K, 2000))
+    t_spec = time.perf_counter() - t_spec
+    stream = torch.cuda.current_stream()
+    EQ1, EQ2, WARM, KERN, E2E = 10**7, 2 * 10**7, 3 * 10**7, 4 * 10**7, 5 * 10**7
+
+    def sweeps_no_meas(n, base):
+        b.reset(base)
+        for _ in range(max(1, n // REFRESH_EVERY)):
+            b.run(REFRESH_EVERY, REFRESH_EVERY + 1, seed)
+
+    if not a.quick:
+        sweeps_no_meas(EQUIL_SWEEPS // 3, EQ1)
+        if not a.step_size:
+            b.adapt_steps(HEAD_ACC if scaled else 0.4, seed=seed ^ 1)
+        sweeps_no_meas(2 * EQUIL_SWEEPS // 3, EQ2)
+    cfg, _ = b.tune(4, seed=seed ^ 0x55)
+    step = b.steps()[0]
+    sweeps_no_meas(max(a.warmup, 3), WARM)
+    b.capture(n_launch, REFRESH_EVERY, 1, seed)
+    b.reset(0)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        torch.cuda.nvtx.range_push("headline_timed")
+        ev0.record(stream)
+        b.replay()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+    if world > 1:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    flags = b.flags()
+    s_np = b.sums[0][:K].cpu().numpy()
+    series = s_np[:, 3] / np.maximum(s_np[:, 6], 1)
+    acc = float(s_np[:, 5].sum() / (K * W * system.n_e))
+    if K >= 1000 or a.quick:
+        tau_series, tau_src = series, f"timed series ({K} sweeps)"
+    else:
+        b.reset(E2E + 10**6)
+        for _ in range(40):
+            b.run(REFRESH_EVERY, 1, seed)
+        aux = b.sums[0][:2000].cpu().numpy()
+        tau_series = aux[:, 3] / np.maximum(aux[:, 6], 1)
+        tau_src = "untimed 2000-sweep series"
+    e_mean, e_serr, e_sdev, kappa = O.binning_analysis(tau_series)
+
+    # one launch (refresh + 50 sweeps) timed on its own: the roofline denominator
+    b.reset(KERN)
+    k0 = torch.cuda.Event(enable_timing=True)
+    k1 = torch.cuda.Event(enable_timing=True)
+    k0.record(stream)
+    b.run(REFRESH_EVERY, 1, seed)
+    k1.record(stream)
+    torch.cuda.synchronize()
+    launch_ms = k0.elapsed_time(k1)
+
+    plain = prec = None
+    if not a.quick and (a.precision != "fp64" or a.proposal != "plain"):
+        # the comparison: plain FP64 sampler through the same path
+        pb = BatchedSampler([ctx], [b.walkers[0].clone()], [STEP_DEFAULT.get(a.system, 0.3)],
+                            precision="fp64", proposal="plain", cap=4000)
+        pstep = pb.adapt_steps(0.4, seed=seed ^ 2)[0]
+        pb.reset(EQ1 + 10**6)
+        for _ in range(10):
+            pb.run(REFRESH_EVERY, REFRESH_EVERY + 1, seed ^ 3)
+        pb.tune(4, seed=seed ^ 4)
+        Kp = 4000
+        pb.reset(0)
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(Kp // REFRESH_EVERY):
+            pb.run(REFRESH_EVERY, 1, seed ^ 3)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        pms = p0.elapsed_time(p1)
+        pn = pb.sums[0][:Kp].cpu().numpy()
+        pser = pn[:, 3] / np.maximum(pn[:, 6], 1)
+        pm, pse, _, pk = O.binning_analysis(pser)
+        pw = W * Kp / (pms * 1e-3)
+        plain = {"value": pw * world / pk, "walker_sweeps_per_s": pw * world, "tau_int": pk,
+                 "proposal": "fixed-width Gaussian", "step": pstep, "precision": "fp64",
+                 "ms_per_step": pms / Kp, "steps": Kp, "path": "same persistent kernel, FP64",
+                 "energy": {"mean": pm, "serr": pse},
+                 "energy_diff_sigma": abs(pm - e_mean) / max(np.hypot(pse, e_serr), 1e-300)}
+        # precision: FP64 sampler with the same proposal, and the mixed vs FP64
+        # local energy on identical configurations
+        pb.set_proposal(0, proposal="scaled", scale_r0=HEAD_R0, scale_fmin=HEAD_FMIN)
+        pb.adapt_steps(HEAD_ACC, seed=seed ^ 5)
+        pb.reset(EQ2 + 10**6)
+        for _ in range(10):
+            pb.run(REFRESH_EVERY, REFRESH_EVERY + 1, seed ^ 6)
+        pb.reset(0)
+        Kf = 4000
+        for _ in range(Kf // REFRESH_EVERY):
+            pb.run(REFRESH_EVERY, 1, seed ^ 6)
+        fn = pb.sums[0][:Kf].cpu().numpy()
+        fm, fse, _, fk = O.binning_analysis(fn[:, 3] / np.maximum(fn[:, 6], 1))
+        ctx.set_proposal(0)
+        ens = WalkerEnsemble(ctx, b.walkers[0], a.precision, seed=seed ^ 7)
+        ep = torch.empty(W, 4, dtype=torch.float64, device=dev)
+        ens.run(1, 1e-9, eparts_last=ep)
+        ref = ctx.evaluate(ens.X, want_grad=False, want_lap=False)["e_loc"]
+        dE = (ep[:, 3] - ref).cpu().numpy()
+        prec = {"fp64_same_proposal": {"energy": {"mean": fm, "serr": fse}, "tau_int": fk,
+                                       "steps": Kf},
+                "sampled_diff_Ha": e_mean - fm,
+                "sampled_diff_sigma": abs(e_mean - fm) / max(np.hypot(fse, e_serr), 1e-300),
+                "eloc_same_configs": {"walkers": W, "mean_diff_Ha": float(dE.mean()),
+                                      "serr_Ha": float(dE.std() / np.sqrt(W)),
+                                      "median_abs_Ha": float(np.median(np.abs(dE))),
+                                      "p99_abs_Ha": float(np.quantile(np.abs(dE), 0.99))}}
+        del pb, ens
+
+    e2e = None
+    if not a.no_e2e:
+        # host buffers through the public API: each call = 50 sweeps; the
+        # walkers go host -> device before and device -> host after every
+        # call, with the call's measurement sums
+        Ke = min(n_launch, 10)
+        hostX = b.walkers[0].detach().to("cpu").pin_memory()
+        hsum = torch.empty(REFRESH_EVERY, NSUM, dtype=torch.float64).pin_memory()
+        b.reset(E2E)
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for r in range(Ke):
+            b.walkers[0].copy_(hostX, non_blocking=True)
+            b.run(REFRESH_EVERY, 1, seed)
+            hostX.copy_(b.walkers[0], non_blocking=True)
+            hsum.copy_(b.sums[0][r * REFRESH_EVERY:(r + 1) * REFRESH_EVERY], non_blocking=True)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        bi = b.walkers[0].numel() * 8
+        e2e = {"ms_per_step": f0.elapsed_time(f1) / (Ke * REFRESH_EVERY),
+               "h2d_bytes_per_step": bi / REFRESH_EVERY,
+               "d2h_bytes_per_step": (bi + REFRESH_EVERY * NSUM * 8) / REFRESH_EVERY}
+
+    t = torch.tensor([ms, e2e["ms_per_step"] if e2e else 0.0], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max, e2e_ms = float(t[0]), float(t[1])
+    wss = W * world * K / (ms_max * 1e-3)
+    value = wss / kappa
+    work = work_per_walker_sweep(system, acc)
+    peak_kind = 0 if a.precision == "fp64" else 1
+    rate = ctypes_peak(L, peak_kind)
+    achieved = work["flops"] * W * REFRESH_EVERY / (launch_ms * 1e-3)
+    traffic = ncu_traffic(f"{a.system}/persistent", a.precision)
+    line = {
+        "metric": "decorrelated samples/s (walker-steps/s / tau_int) vs plain FP64, H2O 64k walkers",
+        "value": value, "unit": "decorrelated samples/s", "n_gpus": world, "steps": K,
+        "warmup": a.warmup, "ms_per_step": ms_max / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if a.precision == "mixed" else "f64",
+        "data": "synthetic",
+        "config": {"workload": f"{a.system} cc-pVDZ-shaped, {W} walkers/GPU, single-electron "
+                               f"sweeps + E_L every sweep, FP64 LU refresh every {REFRESH_EVERY}",
+                   "precision": a.precision, "walkers_per_gpu": W, "step": step,
+                   "parallelism": f"replicas x{world}",
+                   "trial": "RHF determinant + Pade J2 (b=3)",
+                   "kernels": "fused persistent launch per 50 sweeps (refresh, moves, E_L), "
+                              f"NVRTC-specialised to the molecule (compile {t_spec:.1f} s, "
+                              "untimed), CUDA graph of the timed launches",
+                   "tile_shape": cfg,
+                   "proposal": (f"nucleus-scaled Gaussian (r0={HEAD_R0}, fmin={HEAD_FMIN}, "
+                                f"acceptance target {HEAD_ACC}), exact MH" if scaled
+                                else "fixed-width Gaussian"),
+                   "equilibration_sweeps": EQUIL_SWEEPS + 200,
+                   "l2": "walker state in shared memory for a whole launch; positions "
+                         "(15.7 MB) read and written once per 50-sweep launch"},
+        "walker_sweeps_per_s": wss, "tau_int": kappa, "tau_source": tau_src,
+        "energy": {"mean": e_mean, "serr": e_serr}, "acceptance": acc, "kernel_flags": flags,
+        "gpu_launches": n_launch,
+        "roofline": {"bound": "fp64" if peak_kind == 0 else "fp32",
+                     "achieved": achieved / 1e12, "peak": rate / 1e12, "unit": "TFLOP/s",
+                     "frac": achieved / rate if rate else None, "traffic": traffic,
+                     "kernel": "k_batch (one launch: refresh + 50 sweeps)",
+                     "kernel_ms_per_launch": launch_ms,
+                     "flops_per_walker_sweep": work["flops"],
+                     "peak_source": "own FMA microkernel (oqmc_measure_peak), of measured"},
+    }
+    if plain:
+        line["plain_fp64"] = plain
+        line["speedup_vs_plain_fp64"] = value / plain["value"]
+    if prec:
+        line["precision_check"] = prec
+    if e2e:
+        line["e2e"] = {"value": W * world / (e2e_ms * 1e-3) / kappa,
+                       "unit": "decorrelated samples/s",
+                       "h2d_bytes_per_step": e2e["h2d_bytes_per_step"],
+                       "d2h_bytes_per_step": e2e["d2h_bytes_per_step"],
+                       "ms_per_step": e2e_ms,
+                       "note": "each API call runs 50 sweeps; walkers copied in and out per call"}
+    if rank == 0 and not a.no_cpu and world == 1:
+        cores = len(os.sched_getaffinity(0))
+        r, kap, acc_c, sample, _ = cpu_reference(system, a.cpu_seconds, cores, (3 * 0.1) ** 0.5)
+        line["cpu_baseline"] = {"value": r / kap, "unit": "decorrelated samples/s",
+                                "cores": cores, "kind": "port", "sample": sample,
+                                "walker_steps_per_s": r, "tau_int": kap}
+    line["clocks"] = clk.summary()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    b.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 BATCH = (("H2", 8192), ("LiH", 16384), ("H2O", 65536), ("N2", 32768), ("H2O_dimer", 16384))
 
 
@@ -796,8 +1055,10 @@ def main():
         run_batched(a)
     elif a.workload == "learned":
         run_learned(a)
-    else:
+    elif a.path == "split" or a.eloc == "tc":
         run_ours(a)
+    else:
+        run_persistent(a)
 
 
 if __name__ == "__main__":

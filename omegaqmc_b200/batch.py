@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import ctypes
 
+import numpy as np
 import torch
 
 from . import _lib as L
@@ -76,6 +77,48 @@ class BatchedSampler:
             e.sums = self.sums[k].data_ptr()
             e.cap = self.cap
         self._check(self.lib.oqmc_batch_bind(self._h, self._entries))
+
+    def set_proposal(self, k, step=None, proposal=None, scale_r0=None, scale_fmin=None):
+        """Change molecule k's proposal settings (re-plans the tiles; a
+        captured graph must be captured again)."""
+        e = self._entries[k]
+        if step is not None:
+            e.step = float(step)
+        if proposal is not None:
+            e.proposal = PROPOSALS[proposal]
+        if scale_r0 is not None:
+            e.scale_r0 = float(scale_r0)
+        if scale_fmin is not None:
+            e.scale_fmin = float(scale_fmin)
+        cfg = self.config() if getattr(self, "_h", None) is not None else None
+        self._check(self.lib.oqmc_batch_bind(self._h, self._entries))
+        if cfg is not None:
+            self.configure(cfg["threads"], cfg["walkers_per_tile"], cfg["variant"])
+
+    def steps(self):
+        return [self._entries[k].step for k in range(self.n)]
+
+    def adapt_steps(self, target=0.4, rounds=40, sweeps=5, seed=0x5EED, step_base=3 * 10**9):
+        """Equilibrate with the reference's step rule, log s += 0.05 (acc -
+        target) (OmegaQMC/vmc_gto.py:121-126), applied to every molecule
+        once per round of ``sweeps`` sweeps (five times the rate, once per
+        round); leaves the measurement slots cleared."""
+        self.reset(step_base)
+        for r in range(rounds):
+            for sm in self.sums:
+                sm[0].zero_()
+            self.reset(step_base + r * sweeps, clear_sums=False)
+            self.run(sweeps, sweeps, seed)
+            for k in range(self.n):
+                W = self.walkers[k].shape[0]
+                acc = float(self.sums[k][0, 5]) / (sweeps * W * self.contexts[k].n_e)
+                e = self._entries[k]
+                e.step = float(np.exp(np.log(e.step) + 0.05 * sweeps * (acc - target)))
+            cfg = self.config()
+            self._check(self.lib.oqmc_batch_bind(self._h, self._entries))
+            self.configure(cfg["threads"], cfg["walkers_per_tile"], cfg["variant"])
+        self.reset(0)
+        return self.steps()
 
     # -- lifetime --------------------------------------------------------
     def close(self):
