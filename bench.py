@@ -457,6 +457,7 @@ def run_persistent(a):
     import torch
     import torch.distributed as dist
     from omegaqmc_b200 import _lib as L
+    from omegaqmc_b200 import replicas as RP
     from omegaqmc_b200.batch import BatchedSampler
     from omegaqmc_b200.context import GTOContext
     from omegaqmc_b200.sampler import WalkerEnsemble, init_walkers_gaussian, NSUM
@@ -515,17 +516,19 @@ def run_persistent(a):
         dist.barrier()
     ms = ev0.elapsed_time(ev1)
     flags = b.flags()
-    s_np = b.sums[0][:K].cpu().numpy()
-    series = s_np[:, 3] / np.maximum(s_np[:, 6], 1)
-    acc = float(s_np[:, 5].sum() / (K * W * system.n_e))
+    # replicas: the measurement sums of all ranks add up to those of the
+    # union of their walkers
+    s_np = RP.combine_sums(b.sums[0][:K].clone()).cpu().numpy()
+    series = RP.walker_mean_series(s_np)
+    acc = float(s_np[:, 5].sum() / (K * W * world * system.n_e))
     if K >= 1000 or a.quick:
         tau_series, tau_src = series, f"timed series ({K} sweeps)"
     else:
         b.reset(E2E + 10**6)
         for _ in range(40):
             b.run(REFRESH_EVERY, 1, seed)
-        aux = b.sums[0][:2000].cpu().numpy()
-        tau_series = aux[:, 3] / np.maximum(aux[:, 6], 1)
+        aux = RP.combine_sums(b.sums[0][:2000].clone()).cpu().numpy()
+        tau_series = RP.walker_mean_series(aux)
         tau_src = "untimed 2000-sweep series"
     e_mean, e_serr, e_sdev, kappa = O.binning_analysis(tau_series)
 

@@ -28,6 +28,7 @@ import torch
 
 from .context import GTOContext
 from .cusp import cusp_params_for_mol
+from . import replicas as RP
 from .sampler import NSUM, WalkerEnsemble, init_walkers_ball
 from .system import build_system
 
@@ -192,7 +193,12 @@ class VMCDriverGTO:
             raise NotImplementedError("force estimators are not on this path")
         seed = int(np.asarray(rng_key).ravel()[0]) if not isinstance(rng_key, int) else rng_key
         s = self.system
-        X = init_walkers_ball(s, num_walkers, seed)
+        # replicas: with an initialised torch.distributed process group every
+        # rank samples num_walkers walkers of its own and the block statistics
+        # are summed over the ranks (the reference shards the walker axis,
+        # OmegaQMC/utils.py:1148-1159)
+        rank, world = RP.world_info()
+        X = init_walkers_ball(s, num_walkers, RP.rank_seed(seed, rank))
         mc_stepsize = (3 * mc_timestep) ** 0.5
         E_b = []
         block_cnt_start = 1
@@ -204,7 +210,8 @@ class VMCDriverGTO:
             X = np.asarray(d["walkers"])
             E_b = list(np.asarray(d["E_blocks"]))
             print("Restarting ...")
-        ens = WalkerEnsemble(self.ctx, X, self.precision, seed=seed + 7919 * block_cnt_start)
+        ens = WalkerEnsemble(self.ctx, X, self.precision,
+                             seed=RP.rank_seed(seed + 7919 * block_cnt_start, rank))
         if not mode_restart and num_steps_basin > 0:
             acc = ens.basin(num_steps_basin, BASIN_RELOC_SIGMA)
             print(f"ℹ️\tBasin thermalization: {num_steps_basin} "
@@ -215,14 +222,18 @@ class VMCDriverGTO:
             for _ in range(num_blocks_equil * num_steps_per_block):
                 one.zero_()
                 ens.run(1, mc_stepsize, sums=one)
-                ratio = float(one[0, 5]) / (ens.W * s.n_e)
+                RP.combine_sums(one)
+                ratio = float(one[0, 5]) / (ens.W * world * s.n_e)
                 mc_stepsize = float(np.exp(np.log(mc_stepsize) + STEP_SIZE_ADAPTATION_RATE
                                            * (ratio - TARGET_ACCEPTANCE_RATE)))
             print(f"ℹ️\tEquilibration acceptance rate: {ratio:.2f}")
         mc_timestep = mc_stepsize * mc_stepsize / 3
         print(f"ℹ️\tAdjusted step size: {mc_stepsize:.4f} bohr "
               f"~ {mc_timestep:.4f} Ha⁻¹ in Brownian time")
-        fout = sys.stdout if not fname_log else open(fname_log, "w", 1)
+        if rank > 0:
+            fout = open(os.devnull, "w")
+        else:
+            fout = sys.stdout if not fname_log else open(fname_log, "w", 1)
         print("# block_cnt        E_loc_mean      E_loc_std"
               "       eePotential     enPotential     Kinetic"
               "          weight_block        Δt_block"
@@ -231,7 +242,8 @@ class VMCDriverGTO:
         block_cnt = block_cnt_start - 1
         for block_cnt in range(block_cnt_start, block_cnt_start + num_blocks):
             n_sw = num_steps_per_block * num_steps_decorr
-            sums = ens.run(n_sw, mc_stepsize, measure_every=num_steps_decorr).cpu().numpy()
+            sums = RP.combine_sums(ens.run(n_sw, mc_stepsize,
+                                           measure_every=num_steps_decorr)).cpu().numpy()
             nv = np.maximum(sums[:, 6], 1.0)
             ee_s, en_s, ke_s = sums[:, 0] / nv, sums[:, 1] / nv, sums[:, 2] / nv
             E_loc_s = ee_s + en_s + ke_s + self.enr_nn
@@ -240,7 +252,7 @@ class VMCDriverGTO:
             E_b.append(E_mean)
             t_cur = datetime.now()
             weight = float(sums[:, 6].sum())
-            acc = float(sums[:, 5].sum()) / (n_sw * ens.W * s.n_e)
+            acc = float(sums[:, 5].sum()) / (n_sw * ens.W * world * s.n_e)
             print(f"{block_cnt:>8d}{E_mean:>24.8e}{std_E_s:>16.8e}"
                   f"{ee_s.mean():>16.8e}{en_s.mean():>16.8e}{ke_s.mean():>16.8e}"
                   f"{weight:>16.8e}{(t_cur - t_prev).total_seconds():>16.6f}"
@@ -272,7 +284,8 @@ class VMCDriverGTO:
             "mc_stepsize": float(mc_stepsize),
             "walkers": ens.X.cpu().numpy(),
         }
-        path = self._save(self.ofname_chkpt, data)
+        path = self._save(self.ofname_chkpt if world == 1 else
+                          f"{self.ofname_chkpt}.rank{rank}", data)
         self.results = {"E_blocks": np.array(E_b), "energy": e_mean, "serr": e_serr,
                         "kappa": e_kappa, "mc_stepsize": mc_stepsize, "chk": path}
         return None

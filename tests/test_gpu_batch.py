@@ -138,3 +138,23 @@ def test_bad_tile_shapes_are_rejected(contexts):
         b.configure(128, [256, 64, 64])
     b.configure(64, [32, 32, 64])
     assert b.config()["threads"] == 64
+
+
+def test_step_adaptation_reaches_the_target_acceptance(contexts):
+    b = BatchedSampler(contexts, _walkers(contexts, seed=5), STEPS, proposal=PROPS, cap=8)
+    b.configure(128, [64, 64, 64], variant=2)
+    steps = b.adapt_steps(0.5, rounds=30)
+    assert all(s > 0 for s in steps)
+    b.reset(0)
+    b.run(40, 20, 3)
+    torch.cuda.synchronize()
+    for k, c in enumerate(contexts):
+        acc = float(b.sums[k][:2, 5].sum()) / (40 * WALKERS[k] * c.n_e)
+        assert abs(acc - 0.5) < 0.1, (NAMES[k], acc)
+    # switch molecule 0 to the nucleus-scaled proposal in place
+    b.set_proposal(0, proposal="scaled", scale_r0=1.0, scale_fmin=0.02)
+    assert b.config()["walkers_per_tile"] == [64, 64, 64]
+    b.reset(0)
+    b.run(10, 5, 4)
+    torch.cuda.synchronize()
+    assert b.flags() == 0
