@@ -583,7 +583,7 @@ static int launch_moves(oqmc_ctx* ctx, const OqMoveArgs& m, int wpb, size_t sm, 
     const void* C = (const void*)ctx->d_C32;
     OqMlpWeights nw{ctx->mlp->wbf, ctx->mlp->theta};
     void* args[5] = {(void*)&L.sys, (void*)&L.split, (void*)&C, (void*)&mm, (void*)&nw};
-    if (oq_rtc_launch(ctx->mlp_fn, dim3((m.W + 127) / 128), dim3(128),
+    if (oq_rtc_launch(ctx->mlp_fn, dim3((m.W + 127) / 128), dim3(256),
                       oq_mlp_sweep_smem(ctx->nocc), L.stream, args) != 0)
       return set_err(ctx, OQ_ERR_CUDA, "learned-proposal move kernel launch failed%s");
     return OQ_OK;

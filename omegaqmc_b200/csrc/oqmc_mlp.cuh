@@ -116,15 +116,17 @@ __device__ __forceinline__ void oq_mlp_pre_issue() {
   oq_tc_fence_after();
 }
 
-// Hidden-layer epilogue: row r of D (TMEM lane r) + bias, ReLU, BF16 into
-// the K-major buffer `act` (KC = 16).  Optionally also into the transposed
-// buffer `ht` ([128 features x 128 rows], KC = 16) and a 128-bit ReLU mask.
-// Columns are read 64 at a time (four loads in flight, one wait).
+// Hidden-layer epilogue: columns [c_begin, c_end) of row r of D (TMEM lane
+// r) + bias, ReLU, BF16 into the K-major buffer `act` (KC = 16).  Optionally
+// also into the transposed buffer `ht` ([128 features x 128 rows], KC = 16)
+// and a 128-bit ReLU mask.  Columns are read 64 at a time (four loads in
+// flight, one wait).
 __device__ __forceinline__ void oq_mlp_hidden_epilogue(uint32_t tmem_row, const float* bias,
                                                        unsigned char* act, int r,
-                                                       unsigned char* ht, uint32_t* mask) {
+                                                       unsigned char* ht, uint32_t* mask,
+                                                       int c_begin = 0, int c_end = OQ_MLP_H) {
 #pragma unroll 1
-  for (int h0 = 0; h0 < OQ_MLP_H; h0 += 64) {
+  for (int h0 = c_begin; h0 < c_end; h0 += 64) {
     uint32_t raw[64];
 #pragma unroll
     for (int q = 0; q < 4; ++q) oq_tmem_ld16_nw(tmem_row + (uint32_t)(h0 + 16 * q), raw + 16 * q);
@@ -188,27 +190,33 @@ __device__ __forceinline__ void oq_mlp_load_weights(unsigned char* wreg,
 }
 
 // Forward pass of the 128 rows whose BF16 inputs are in `act` (K = 32,
-// KC = 4); leaves the thread's 48 outputs in out.  `ht`/`mask` (training)
-// receive the transposed hidden activations and ReLU masks of layers 1..3.
-// Returns false when an MMA wait timed out (uniform over the CTA).
+// KC = 4); leaves row r's 48 outputs in `out` of thread r (r < 128).
+// With 256 threads, threads 128-255 (warps 4-7, the same TMEM lane quarters
+// as warps 0-3) write columns 64-127 of every hidden layer and threads
+// 0-127 columns 0-63.  `ht`/`mask` (training, 128 threads) receive the
+// transposed hidden activations and ReLU masks of layers 1..3.  Returns
+// false when an MMA wait timed out (uniform over the CTA).
 __device__ __forceinline__ bool oq_mlp_forward_tile(unsigned char* act, const unsigned char* wreg,
                                                     const float* bias, uint32_t tmem,
                                                     OqMlpSync& sy, float out[OQ_MLP_NOUT],
                                                     unsigned char* const* ht, uint32_t* mask) {
-  const int r = threadIdx.x;
+  const int r = threadIdx.x & 127;
+  const bool pair = blockDim.x == 256;
+  const int c_begin = pair ? (threadIdx.x >= 128 ? 64 : 0) : 0;
+  const int c_end = pair ? c_begin + 64 : OQ_MLP_H;
   const uint32_t trow = tmem + ((uint32_t)((r >> 5) * 32) << 16);
   const unsigned char* W[4] = {wreg, wreg + OQ_MLP_SM_W1, wreg + OQ_MLP_SM_W1 + OQ_MLP_SM_WH,
                                wreg + OQ_MLP_SM_W1 + 2 * OQ_MLP_SM_WH};
   for (int l = 0; l < 4; ++l) {
     oq_mlp_pre_issue();
-    if (r == 0)
+    if (threadIdx.x == 0)
       oq_mlp_mma(tmem, act, W[l], l == 3 ? OQ_MLP_NOUT : OQ_MLP_H, l == 0 ? OQ_MLP_K0 : OQ_MLP_H,
                  sy.bar);
     if (!oq_mlp_wait(sy)) return false;
     if (l < 3)
       oq_mlp_hidden_epilogue(trow, bias + l * OQ_MLP_H, act, r, ht ? ht[l] : nullptr,
-                             mask ? mask + 4 * l : nullptr);
-    else
+                             mask ? mask + 4 * l : nullptr, c_begin, c_end);
+    else if (threadIdx.x < 128)
       oq_mlp_out_epilogue(trow, bias + 3 * OQ_MLP_H, out);
   }
   oq_tc_fence_before();

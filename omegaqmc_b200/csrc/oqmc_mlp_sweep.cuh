@@ -1,7 +1,8 @@
 // Metropolis sweeps with the learned proposal (mixed precision).
 //
-// One CTA = 128 walkers = 128 threads = the 128 rows of every network
-// evaluation.  The walkers' positions and inverse Slater matrices stay in
+// One CTA = 128 walkers = the 128 rows of every network evaluation, run by
+// 256 threads: thread t < 128 owns walker t; threads 128-255 only share the
+// hidden-layer epilogues (columns 64-127).  The walkers' positions and inverse Slater matrices stay in
 // shared memory for the whole launch (as in k_moves), next to the BF16
 // weights in the canonical tensor-core layout.  For each electron e of a
 // sweep:
@@ -35,7 +36,7 @@ struct OqMlpWeights {
 };
 
 template <int NOCC, class B>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(256, 1)
 k_moves_mlp(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
             const void* __restrict__ gC, OqMoveArgs a, OqMlpWeights nw) {
   constexpr int NE = 2 * NOCC;
@@ -53,18 +54,21 @@ k_moves_mlp(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gspli
   const OqSystem& S = *gsys;
   const OqSplit& SP = *gsplit;
   const float* C = reinterpret_cast<const float*>(gC);
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x & 127, warp = threadIdx.x >> 5;
+  const bool owner = threadIdx.x < 128;     // owns walker tid
   const int W = a.W;
   const int w = blockIdx.x * WT + tid;
-  const bool live = w < W;
+  const bool live = owner && w < W;
   if (warp == 0) oq_tmem_alloc(slot, 128);
   if (tid == 0) oq_mbar_init(bar, 1);
   oq_jas_load(J, S);
   oq_mlp_load_weights(wreg, nw.wbf);
   oq_mlp_load_bias(bias, nw.theta);
   const float* gA = reinterpret_cast<const float*>(a.ainv);
-  for (int k = 0; k < 3 * NE; ++k) pos[k * WT + tid] = live ? a.pos[(size_t)k * W + w] : 0.0;
-  for (int k = 0; k < 2 * NN; ++k) Ai[k * WT + tid] = live ? gA[(size_t)k * W + w] : 0.0f;
+  if (owner) {
+    for (int k = 0; k < 3 * NE; ++k) pos[k * WT + tid] = live ? a.pos[(size_t)k * W + w] : 0.0;
+    for (int k = 0; k < 2 * NN; ++k) Ai[k * WT + tid] = live ? gA[(size_t)k * W + w] : 0.0f;
+  }
   oq_tc_fence_before();
   __syncthreads();
   oq_tc_fence_after();
@@ -84,19 +88,28 @@ k_moves_mlp(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gspli
       const float uc = ((float)rc.x + 0.5f) * 2.3283064365386963e-10f;
       const double ox = P(e, 0), oy = P(e, 1), oz = P(e, 2);
       float f[OQ_MLP_K0], out[OQ_MLP_NOUT];
-      oq_mlp_features(J, P, NE, e, ox, oy, oz, f);
-      oq_mlp_store_features(act, tid, f);
+      if (owner) {
+        oq_mlp_features(J, P, NE, e, ox, oy, oz, f);
+        oq_mlp_store_features(act, tid, f);
+      }
       ok = oq_mlp_forward_tile(act, wreg, bias, tmem, sy, out, nullptr, nullptr);
       if (!ok) break;
-      double d[3];
-      oq_mix_sample_f(out, uc, n3, d);
+      double d[3] = {0.0, 0.0, 0.0};
+      float lqf = 0.0f;
+      if (owner) {
+        oq_mix_sample_f(out, uc, n3, d);
+        lqf = oq_mix_logq_f(out, (float)d[0], (float)d[1], (float)d[2]);
+      }
       const double nx = ox + d[0], ny = oy + d[1], nz = oz + d[2];
-      const float lqf = oq_mix_logq_f(out, (float)(nx - ox), (float)(ny - oy), (float)(nz - oz));
-      oq_mlp_features(J, P, NE, e, nx, ny, nz, f);
-      oq_mlp_store_features(act, tid, f);
+      if (owner) {
+        oq_mlp_features(J, P, NE, e, nx, ny, nz, f);
+        oq_mlp_store_features(act, tid, f);
+      }
       ok = oq_mlp_forward_tile(act, wreg, bias, tmem, sy, out, nullptr, nullptr);
       if (!ok) break;
-      const float lqr = oq_mix_logq_f(out, (float)(ox - nx), (float)(oy - ny), (float)(oz - nz));
+      const float lqr = owner ? oq_mix_logq_f(out, (float)(ox - nx), (float)(oy - ny),
+                                             (float)(oz - nz))
+                              : 0.0f;
       if (live)
         nacc += oq_try_move<NOCC, float, float, B>(J, S, SP, C, pos, Ai, WT, tid, e, nx, ny, nz,
                                                    (double)(lqr - lqf), u, logdet);
