@@ -333,6 +333,88 @@ int oqmc_set_mlp_proposal(oqmc_ctx* ctx, const oqmc_mlp* m) {
   return OQ_OK;
 }
 
+// Jastrow-parameter derivatives, one thread per walker, FP64: d ln|psi|/dp
+// and dE_L/dp for p = (J2 like a, like b, unlike a, unlike b, J1 a_I, b_I per
+// atom), from the positions and the full gradient G of ln|psi| (oqmc_eval).
+// For u = a r/(1+b r): du/da = r/den, du/db = -a r^2/den^2; u' = a/den^2,
+// u'' = -2ab/den^3; E_L changes only through -1/2 sum_e (lap_e + |G_e|^2).
+__device__ __forceinline__ void oq_pade_dp(double a, double b, double r, double du[2],
+                                           double dup[2], double dL[2]) {
+  const double den = 1.0 + b * r, id = 1.0 / den, id2 = id * id, id3 = id2 * id;
+  du[0] = r * id;
+  du[1] = -a * r * r * id2;
+  dup[0] = id2;
+  dup[1] = -2.0 * a * r * id3;
+  const double dupp0 = -2.0 * b * id3, dupp1 = -2.0 * a * id3 + 6.0 * a * b * r * id3 * id;
+  dL[0] = dupp0 + 2.0 * dup[0] / r;
+  dL[1] = dupp1 + 2.0 * dup[1] / r;
+}
+
+__global__ void k_param_derivs(const OqSystem* __restrict__ gsys, const double* __restrict__ X,
+                               const double* __restrict__ G, int W, int n_e,
+                               double* __restrict__ dlog, double* __restrict__ del) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  const OqSystem& S = *gsys;
+  const int n_raw = 4 + 2 * S.natm;
+  const double* x = X + (size_t)w * n_e * 3;
+  const double* g = G + (size_t)w * n_e * 3;
+  double* dl = dlog + (size_t)w * n_raw;
+  double* de = del + (size_t)w * n_raw;
+  for (int k = 0; k < n_raw; ++k) { dl[k] = 0.0; de[k] = 0.0; }
+  if (S.has_j2) {
+    double al[4] = {0, 0, 0, 0}, ae[4] = {0, 0, 0, 0};
+    for (int i = 0; i < n_e; ++i)
+      for (int j = i + 1; j < n_e; ++j) {
+        const double dx = x[3 * i] - x[3 * j], dy = x[3 * i + 1] - x[3 * j + 1],
+                     dz = x[3 * i + 2] - x[3 * j + 2];
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        const double gd = ((g[3 * i] - g[3 * j]) * dx + (g[3 * i + 1] - g[3 * j + 1]) * dy +
+                           (g[3 * i + 2] - g[3 * j + 2]) * dz) / r;
+        const int o = ((i & 1) == (j & 1)) ? 0 : 2;
+        double du[2], dup[2], dL[2];
+        oq_pade_dp(S.j2[o], S.j2[o + 1], r, du, dup, dL);
+        for (int q = 0; q < 2; ++q) {
+          al[o + q] += du[q];
+          ae[o + q] -= dL[q] + dup[q] * gd;
+        }
+      }
+    for (int k = 0; k < 4; ++k) { dl[k] = al[k]; de[k] = ae[k]; }
+  }
+  if (S.has_j1) {
+    for (int I = 0; I < S.natm; ++I) {
+      double sl0 = 0, sl1 = 0, se0 = 0, se1 = 0;
+      for (int e = 0; e < n_e; ++e) {
+        const double dx = x[3 * e] - S.nuc[I][0], dy = x[3 * e + 1] - S.nuc[I][1],
+                     dz = x[3 * e + 2] - S.nuc[I][2];
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        const double gd = (g[3 * e] * dx + g[3 * e + 1] * dy + g[3 * e + 2] * dz) / r;
+        double du[2], dup[2], dL[2];
+        oq_pade_dp(S.j1a[I], S.j1b[I], r, du, dup, dL);
+        sl0 += du[0]; sl1 += du[1];
+        se0 -= 0.5 * (dL[0] + 2.0 * dup[0] * gd);
+        se1 -= 0.5 * (dL[1] + 2.0 * dup[1] * gd);
+      }
+      dl[4 + 2 * I] = sl0; dl[5 + 2 * I] = sl1;
+      de[4 + 2 * I] = se0; de[5 + 2 * I] = se1;
+    }
+  }
+}
+
+int oqmc_param_count(const oqmc_ctx* ctx) { return ctx ? 4 + 2 * ctx->natm : OQ_ERR_ARG; }
+
+int oqmc_param_derivs(oqmc_ctx* ctx, const double* X, int W, const double* grad, double* dlogpsi,
+                      double* dEL, void* stream) {
+  if (!ctx) return OQ_ERR_ARG;
+  if (W < 0 || (W > 0 && (!X || !grad || !dlogpsi || !dEL)))
+    return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
+  if (W == 0) return OQ_OK;
+  k_param_derivs<<<(W + 127) / 128, 128, 0, (cudaStream_t)stream>>>(ctx->d_sys, X, grad, W,
+                                                                     ctx->n_e, dlogpsi, dEL);
+  OQ_CUDA(ctx, cudaGetLastError());
+  return OQ_OK;
+}
+
 // TF32 rounding as cvt.rna (nearest, ties away from zero) and BF16 (nearest even)
 static float host_tf32(float f) {
   uint32_t u;

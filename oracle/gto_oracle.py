@@ -389,3 +389,58 @@ def binning_analysis(a):
         kappa += 2.0 * ac[k]
     serr = sdev * math.sqrt(kappa / n)
     return float(xbar), float(serr), float(sdev), float(kappa)
+
+
+# ---------------------------------------------------------------------------
+# Jastrow-parameter derivatives (the per-walker inputs of the linear-method
+# optimiser, compute_walker_derivs, OmegaQMC/vmcopt_gto_linear.py:686-703)
+# ---------------------------------------------------------------------------
+def _pade_param_terms(a, b, r):
+    """d/da, d/db of u = a r/(1+b r), of u' and of L = u'' + 2u'/r."""
+    den = 1.0 + b * r
+    du = (r / den, -a * r * r / den ** 2)
+    dup = (1.0 / den ** 2, -2.0 * a * r / den ** 3)
+    dupp = (-2.0 * b / den ** 3, -2.0 * a / den ** 3 + 6.0 * a * b * r / den ** 4)
+    dL = tuple(dupp[k] + 2.0 * dup[k] / r for k in range(2))
+    return du, dup, dL
+
+
+def param_derivatives(system, X, grad=None):
+    """Per-walker d log|psi| / dp and d E_L / dp for the raw Padé parameters
+    p = (J2 like a, like b, unlike a, unlike b, then J1 a_I, b_I per atom).
+
+    lnpsi depends on p only through J; E_L only through its kinetic part
+    -1/2 sum_e (lap_e + |G_e|^2) with G_e the full gradient of ln|psi|
+    (from ``evaluate`` unless given), so dE_L/dp = -1/2 sum_e (d lap_e/dp +
+    2 G_e . dG_e/dp).  Terms absent from the system give zero columns."""
+    X = np.asarray(X, dtype=np.float64)
+    W, n_e, _ = X.shape
+    if grad is None:
+        grad = evaluate(system, X)["grad"]
+    n_raw = 4 + 2 * system.natm
+    dl = np.zeros((W, n_raw))
+    de = np.zeros((W, n_raw))
+    if system.has_j2:
+        i, j = _pairs(n_e)
+        d = X[:, i] - X[:, j]
+        r = np.sqrt(np.sum(d * d, axis=-1))
+        rhat = d / r[..., None]
+        gdot = np.sum((grad[:, i] - grad[:, j]) * rhat, axis=-1)
+        same = (i % 2) == (j % 2)
+        for k, mask in ((0, same), (1, ~same)):
+            a, b = system.j2[k]
+            du, dup, dL = _pade_param_terms(a, b, r)
+            for q in range(2):
+                dl[:, 2 * k + q] = np.sum(du[q] * mask, axis=-1)
+                de[:, 2 * k + q] = -np.sum((dL[q] + dup[q] * gdot) * mask, axis=-1)
+    if system.has_j1:
+        for I in range(system.natm):
+            d = X - system.nuc[I][None, None, :]
+            r = np.sqrt(np.sum(d * d, axis=-1))                 # (W, n_e)
+            gdot = np.sum(grad * d, axis=-1) / r
+            a, b = system.j1[I]
+            du, dup, dL = _pade_param_terms(a, b, r)
+            for q in range(2):
+                dl[:, 4 + 2 * I + q] = np.sum(du[q], axis=-1)
+                de[:, 4 + 2 * I + q] = -0.5 * np.sum(dL[q] + 2.0 * dup[q] * gdot, axis=-1)
+    return dl, de
