@@ -336,6 +336,10 @@ int oqmc_mlp_get_flags(oqmc_mlp* m, unsigned* flags, int clear, void* stream);
  * precision, specialised context; NULL restores the previous proposal).
  * The network is borrowed and must outlive its use. */
 int oqmc_set_mlp_proposal(oqmc_ctx* ctx, const oqmc_mlp* m);
+/* Walker groups of 128 per CTA of the learned-proposal sweep (2 or 4,
+ * default 4): the groups share the weights in shared memory and overlap
+ * each other's network and wavefunction work. */
+int oqmc_set_mlp_groups(oqmc_ctx* ctx, int groups);
 
 #ifdef __cplusplus
 }

@@ -128,6 +128,7 @@ _SIGS = [
                               c_void_p]),
     ("oqmc_mlp_get_flags", c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint), c_int, c_void_p]),
     ("oqmc_set_mlp_proposal", c_int, [c_void_p, c_void_p]),
+    ("oqmc_set_mlp_groups", c_int, [c_void_p, c_int]),
     ("oqmc_param_count", c_int, [c_void_p]),
     ("oqmc_param_derivs", c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
                                   c_void_p]),

@@ -223,5 +223,9 @@ class GTOContext:
         self._mlp = mlp
         self._check(self.lib.oqmc_set_mlp_proposal(self._h, mlp._h if mlp is not None else None))
 
+    def set_mlp_groups(self, groups):
+        """128-walker groups per CTA of the learned-proposal sweep (2 or 4)."""
+        self._check(self.lib.oqmc_set_mlp_groups(self._h, int(groups)))
+
     def set_split(self, tight_alpha):
         self._check(self.lib.oqmc_set_split(self._h, float(tight_alpha)))

@@ -315,21 +315,31 @@ int oqmc_set_mlp_proposal(oqmc_ctx* ctx, const oqmc_mlp* m) {
   if (!ctx->spec)
     return set_err(ctx, OQ_ERR_UNSUPPORTED,
                    "the learned proposal needs a specialised context (oqmc_specialize)%s");
-  if (ctx->n_e > 32 || oq_mlp_sweep_smem(ctx->nocc) > 232448)
-    return set_err(ctx, OQ_ERR_UNSUPPORTED,
-                   "walker state and network do not fit one CTA's shared memory%s");
-  if (!ctx->mlp_fn) {
+  if (ctx->n_e > 32)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED, "the learned proposal handles up to 32 electrons%s");
+  if (!ctx->mlp_fn[0]) {
     const std::string src = std::string("#include \"oqmc_mlp_sweep.cuh\"\n\n") +
                             oq_spec_basis_source(ctx->hsys, ctx->hsplit, ctx->h_C, ctx->nocc,
                                                  "OqSpecBasis");
+    const std::string n = std::to_string(ctx->nocc);
     std::vector<void*> fns;
     std::string err;
-    if (oq_rtc_build(src, {"k_moves_mlp<" + std::to_string(ctx->nocc) + ", OqSpecBasis>"},
+    if (oq_rtc_build(src, {"k_moves_mlp<" + n + ", OqSpecBasis, 2>",
+                           "k_moves_mlp<" + n + ", OqSpecBasis, 4>"},
                      &ctx->mlp_mod, &fns, &err) != 0)
       return set_err(ctx, OQ_ERR_UNSUPPORTED, "%s", err.c_str());
-    ctx->mlp_fn = fns[0];
+    ctx->mlp_fn[0] = fns[0];
+    ctx->mlp_fn[1] = fns[1];
+    if (ctx->mlp_groups != 2) ctx->mlp_groups = 4;
   }
   ctx->mlp = m;
+  return OQ_OK;
+}
+
+int oqmc_set_mlp_groups(oqmc_ctx* ctx, int groups) {
+  if (!ctx) return OQ_ERR_ARG;
+  if (groups != 2 && groups != 4) return set_err(ctx, OQ_ERR_ARG, "groups must be 2 or 4%s");
+  ctx->mlp_groups = groups;
   return OQ_OK;
 }
 
@@ -492,7 +502,7 @@ int oqmc_set_split(oqmc_ctx* ctx, double tight_alpha) {
   }
   if (ctx->mlp_mod) {   // so does the learned-proposal kernel: rebuild it
     oq_rtc_unload(ctx->mlp_mod);
-    ctx->mlp_mod = ctx->mlp_fn = nullptr;
+    ctx->mlp_mod = ctx->mlp_fn[0] = ctx->mlp_fn[1] = nullptr;
     const oqmc_mlp* m = ctx->mlp;
     ctx->mlp = nullptr;
     if (m) {
@@ -665,8 +675,9 @@ static int launch_moves(oqmc_ctx* ctx, const OqMoveArgs& m, int wpb, size_t sm, 
     const void* C = (const void*)ctx->d_C32;
     OqMlpWeights nw{ctx->mlp->wbf, ctx->mlp->theta};
     void* args[5] = {(void*)&L.sys, (void*)&L.split, (void*)&C, (void*)&mm, (void*)&nw};
-    if (oq_rtc_launch(ctx->mlp_fn, dim3((m.W + 127) / 128), dim3(256),
-                      oq_mlp_sweep_smem(ctx->nocc), L.stream, args) != 0)
+    const int G = ctx->mlp_groups == 2 ? 2 : 4;
+    if (oq_rtc_launch(ctx->mlp_fn[G == 4 ? 1 : 0], dim3((m.W + 128 * G - 1) / (128 * G)),
+                      dim3(128 * G), oq_mlp_sweep_smem(G), L.stream, args) != 0)
       return set_err(ctx, OQ_ERR_CUDA, "learned-proposal move kernel launch failed%s");
     return OQ_OK;
   }

@@ -23,8 +23,9 @@ struct oqmc_ctx {
   double* h_C;            // host copy of the MO coefficients (for specialisation)
   double scale_r0, scale_fmin;
   const struct oqmc_mlp* mlp;   // learned proposal (borrowed), or null
-  void* mlp_mod;                // its specialised sweep kernel (module, function)
-  void* mlp_fn;
+  void* mlp_mod;                // its specialised sweep kernels (module; 2 and 4 groups)
+  void* mlp_fn[2];
+  int mlp_groups;               // walker groups per CTA of the learned-proposal sweep
   char err[512];
 };
 

@@ -1,14 +1,19 @@
 // Metropolis sweeps with the learned proposal (mixed precision).
 //
-// One CTA = 128 walkers = the 128 rows of every network evaluation, run by
-// 256 threads: thread t < 128 owns walker t; threads 128-255 only share the
-// hidden-layer epilogues (columns 64-127).  The walkers' positions and inverse Slater matrices stay in
-// shared memory for the whole launch (as in k_moves), next to the BF16
-// weights in the canonical tensor-core layout.  For each electron e of a
-// sweep:
-//   1. every thread writes the features of its walker's electron e and the
-//      CTA runs the network on the tensor cores -> mixture q(. | x);
-//   2. the thread draws the displacement d (component from a uniform, then
+// A CTA runs G independent groups of 128 walkers; group g is warps
+// 4g..4g+3, thread r of the group owns walker r of its tile and row r of the
+// group's network evaluations (TMEM lane r, columns [128g, 128g + 128)).  The
+// BF16 weights (canonical tensor-core layout) are shared by the groups; each
+// group has its own activation tile, mbarrier and named barrier, so the
+// groups advance independently and one group's network latency overlaps the
+// others' CUDA-core work.  The walker state (positions, inverse Slater
+// matrices, log|det|) stays in global memory, walker-minor (L2-resident):
+// keeping it in shared memory would leave room for one group only.
+//
+// For each electron e of a sweep:
+//   1. the group writes the features of its walkers' electron e and runs the
+//      network on the tensor cores -> mixture q(. | x);
+//   2. each thread draws the displacement d (component from a uniform, then
 //      mu + sigma * N(0, 1)) and evaluates log q(d | x) (FP32 mixture math);
 //   3. features at x' = x + d -> network -> log q(-d | x');
 //   4. oq_try_move accepts with |psi(x')/psi(x)|^2 q(x|x') / q(x'|x)
@@ -22,12 +27,11 @@
 #define OQ_MLPS_BIAS 1024
 #define OQ_MLPS_BAR (OQ_MLPS_BIAS + OQ_MLP_SM_BIAS)
 #define OQ_MLPS_ACT 3072
-#define OQ_MLPS_W (OQ_MLPS_ACT + OQ_MLP_SM_ACT)
-#define OQ_MLPS_POS (OQ_MLPS_W + OQ_MLP_SM_WEIGHTS)
+#define OQ_MLPS_MAXG 4
 
-// Shared memory of k_moves_mlp for NOCC occupied orbitals per spin.
-__host__ __device__ constexpr size_t oq_mlp_sweep_smem(int nocc) {
-  return (size_t)OQ_MLPS_POS + (size_t)6 * nocc * 128 * 8 + (size_t)2 * nocc * nocc * 128 * 4;
+// Shared memory of k_moves_mlp with G walker groups.
+__host__ __device__ constexpr size_t oq_mlp_sweep_smem(int groups) {
+  return (size_t)OQ_MLPS_ACT + (size_t)groups * OQ_MLP_SM_ACT + OQ_MLP_SM_WEIGHTS;
 }
 
 struct OqMlpWeights {
@@ -35,49 +39,93 @@ struct OqMlpWeights {
   const float* theta;          // FP32 parameters (biases read from here)
 };
 
-template <int NOCC, class B>
-__global__ void __launch_bounds__(256, 1)
+// Named barrier `id` over n threads, and its OR-reduction of a predicate.
+__device__ __forceinline__ void oq_group_sync(int id, int n) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+__device__ __forceinline__ bool oq_group_or(bool v, int id, int n) {
+  uint32_t r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n"
+      " selp.u32 %0, 1, 0, q;\n}"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id), "r"(n)
+      : "memory");
+  return r != 0;
+}
+
+// Network forward pass of one group's 128 rows (inputs already in `act`),
+// synchronising only the group's 128 threads (named barrier bar_id).
+// Returns false (for every thread of the group) when an MMA wait timed out.
+__device__ __forceinline__ bool oq_mlp_forward_group(unsigned char* act, const unsigned char* wreg,
+                                                     const float* bias, uint32_t tmem_cols,
+                                                     uint64_t* bar, uint32_t& phase, int r,
+                                                     int bar_id, float out[OQ_MLP_NOUT]) {
+  const uint32_t trow = tmem_cols + ((uint32_t)((r >> 5) * 32) << 16);
+  const unsigned char* W[4] = {wreg, wreg + OQ_MLP_SM_W1, wreg + OQ_MLP_SM_W1 + OQ_MLP_SM_WH,
+                               wreg + OQ_MLP_SM_W1 + 2 * OQ_MLP_SM_WH};
+  for (int l = 0; l < 4; ++l) {
+    oq_fence_async_smem();
+    oq_tc_fence_before();
+    oq_group_sync(bar_id, 128);
+    oq_tc_fence_after();
+    if (r == 0)
+      oq_mlp_mma(tmem_cols, act, W[l], l == 3 ? OQ_MLP_NOUT : OQ_MLP_H,
+                 l == 0 ? OQ_MLP_K0 : OQ_MLP_H, bar);
+    const bool ok = oq_mbar_wait(bar, phase);
+    phase ^= 1u;
+    oq_tc_fence_after();
+    if (oq_group_or(!ok, bar_id, 128)) return false;
+    if (l < 3)
+      oq_mlp_hidden_epilogue(trow, bias + l * OQ_MLP_H, act, r, nullptr, nullptr);
+    else
+      oq_mlp_out_epilogue(trow, bias + 3 * OQ_MLP_H, out);
+  }
+  oq_tc_fence_before();
+  return true;
+}
+
+template <int NOCC, class B, int G>
+__global__ void __launch_bounds__(128 * G, 1)
 k_moves_mlp(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
             const void* __restrict__ gC, OqMoveArgs a, OqMlpWeights nw) {
   constexpr int NE = 2 * NOCC;
-  constexpr int NN = NOCC * NOCC;
-  constexpr int WT = 128;
+  static_assert(G >= 1 && G <= OQ_MLPS_MAXG, "1..4 walker groups");
   extern __shared__ __align__(16) unsigned char smem[];
   OqJas& J = *reinterpret_cast<OqJas*>(smem);
   float* bias = reinterpret_cast<float*>(smem + OQ_MLPS_BIAS);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + OQ_MLPS_BAR);
-  uint32_t* slot = reinterpret_cast<uint32_t*>(smem + OQ_MLPS_BAR + 8);
-  unsigned char* act = smem + OQ_MLPS_ACT;
-  unsigned char* wreg = smem + OQ_MLPS_W;
-  double* pos = reinterpret_cast<double*>(smem + OQ_MLPS_POS);   // [3 NE][128]
-  float* Ai = reinterpret_cast<float*>(pos + 3 * NE * WT);        // [2 NN][128]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + OQ_MLPS_BAR);     // [G]
+  uint32_t* slot = reinterpret_cast<uint32_t*>(smem + OQ_MLPS_BAR + 8 * OQ_MLPS_MAXG);
+  unsigned char* wreg = smem + OQ_MLPS_ACT + G * OQ_MLP_SM_ACT;
   const OqSystem& S = *gsys;
   const OqSplit& SP = *gsplit;
   const float* C = reinterpret_cast<const float*>(gC);
-  const int tid = threadIdx.x & 127, warp = threadIdx.x >> 5;
-  const bool owner = threadIdx.x < 128;     // owns walker tid
+  const int g = threadIdx.x >> 7, r = threadIdx.x & 127, warp = threadIdx.x >> 5;
+  unsigned char* act = smem + OQ_MLPS_ACT + g * OQ_MLP_SM_ACT;
   const int W = a.W;
-  const int w = blockIdx.x * WT + tid;
-  const bool live = owner && w < W;
-  if (warp == 0) oq_tmem_alloc(slot, 128);
-  if (tid == 0) oq_mbar_init(bar, 1);
+  const int w = (blockIdx.x * G + g) * 128 + r;
+  const bool live = w < W;
+  const int wr = live ? w : W - 1;          // rows past the end read a valid walker
+  constexpr uint32_t TCOLS = G == 1 ? 128u : G == 2 ? 256u : 512u;
+  if (warp == 0) oq_tmem_alloc(slot, TCOLS);
+  if (threadIdx.x < G) oq_mbar_init(bars + threadIdx.x, 1);
   oq_jas_load(J, S);
   oq_mlp_load_weights(wreg, nw.wbf);
   oq_mlp_load_bias(bias, nw.theta);
-  const float* gA = reinterpret_cast<const float*>(a.ainv);
-  if (owner) {
-    for (int k = 0; k < 3 * NE; ++k) pos[k * WT + tid] = live ? a.pos[(size_t)k * W + w] : 0.0;
-    for (int k = 0; k < 2 * NN; ++k) Ai[k * WT + tid] = live ? gA[(size_t)k * W + w] : 0.0f;
-  }
   oq_tc_fence_before();
   __syncthreads();
   oq_tc_fence_after();
-  const uint32_t tmem = *slot;
-  OqMlpSync sy{bar, 0u};
-  double logdet = live ? a.logdet[w] : 0.0;
+  const uint32_t tbase = *slot;
+  const uint32_t tmem = tbase + (uint32_t)(128 * g);
+  uint64_t* bar = bars + g;
+  const int bar_id = 1 + g;
+  uint32_t phase = 0u;
+  double* pos = a.pos;
+  float* Ai = reinterpret_cast<float*>(a.ainv);
+  double logdet = a.logdet[wr];
   int nacc = 0;
   bool ok = true;
-  auto P = [&](int j, int c) { return pos[(3 * j + c) * WT + tid]; };
+  auto P = [&](int j, int c) { return pos[(size_t)(3 * j + c) * W + wr]; };
   for (int t = 0; t < a.n_steps && ok; ++t) {
     const uint32_t gstep = (uint32_t)(a.step_base + t);
     for (int e = 0; e < NE; ++e) {
@@ -88,51 +136,39 @@ k_moves_mlp(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gspli
       const float uc = ((float)rc.x + 0.5f) * 2.3283064365386963e-10f;
       const double ox = P(e, 0), oy = P(e, 1), oz = P(e, 2);
       float f[OQ_MLP_K0], out[OQ_MLP_NOUT];
-      if (owner) {
-        oq_mlp_features(J, P, NE, e, ox, oy, oz, f);
-        oq_mlp_store_features(act, tid, f);
-      }
-      ok = oq_mlp_forward_tile(act, wreg, bias, tmem, sy, out, nullptr, nullptr);
+      oq_mlp_features(J, P, NE, e, ox, oy, oz, f);
+      oq_mlp_store_features(act, r, f);
+      ok = oq_mlp_forward_group(act, wreg, bias, tmem, bar, phase, r, bar_id, out);
       if (!ok) break;
-      double d[3] = {0.0, 0.0, 0.0};
-      float lqf = 0.0f;
-      if (owner) {
-        oq_mix_sample_f(out, uc, n3, d);
-        lqf = oq_mix_logq_f(out, (float)d[0], (float)d[1], (float)d[2]);
-      }
+      double d[3];
+      oq_mix_sample_f(out, uc, n3, d);
+      const float lqf = oq_mix_logq_f(out, (float)d[0], (float)d[1], (float)d[2]);
       const double nx = ox + d[0], ny = oy + d[1], nz = oz + d[2];
-      if (owner) {
-        oq_mlp_features(J, P, NE, e, nx, ny, nz, f);
-        oq_mlp_store_features(act, tid, f);
-      }
-      ok = oq_mlp_forward_tile(act, wreg, bias, tmem, sy, out, nullptr, nullptr);
+      oq_mlp_features(J, P, NE, e, nx, ny, nz, f);
+      oq_mlp_store_features(act, r, f);
+      ok = oq_mlp_forward_group(act, wreg, bias, tmem, bar, phase, r, bar_id, out);
       if (!ok) break;
-      const float lqr = owner ? oq_mix_logq_f(out, (float)(ox - nx), (float)(oy - ny),
-                                             (float)(oz - nz))
-                              : 0.0f;
+      const float lqr = oq_mix_logq_f(out, (float)(ox - nx), (float)(oy - ny), (float)(oz - nz));
       if (live)
-        nacc += oq_try_move<NOCC, float, float, B>(J, S, SP, C, pos, Ai, WT, tid, e, nx, ny, nz,
+        nacc += oq_try_move<NOCC, float, float, B>(J, S, SP, C, pos, Ai, W, w, e, nx, ny, nz,
                                                    (double)(lqr - lqf), u, logdet);
     }
   }
-  if (live) {
-    for (int k = 0; k < 3 * NE; ++k) a.pos[(size_t)k * W + w] = pos[k * WT + tid];
-    float* gAw = reinterpret_cast<float*>(a.ainv);
-    for (int k = 0; k < 2 * NN; ++k) gAw[(size_t)k * W + w] = Ai[k * WT + tid];
-    a.logdet[w] = logdet;
-  }
+  if (live) a.logdet[w] = logdet;
   if (a.acc_sum) {
     double v = (double)nacc;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if ((tid & 31) == 0) atomicAdd(a.acc_sum, v);
+    if ((threadIdx.x & 31) == 0) atomicAdd(a.acc_sum, v);
+  }
+  if (!ok && r == 0) {
+    oq_mbar_wait(bar, phase ^ 1u);          // let the group's outstanding MMA drain
+    atomicOr(a.flags, OQ_FLAG_TIMEOUT);
   }
   oq_tc_fence_before();
   __syncthreads();
   if (warp == 0) {
     oq_tc_fence_after();
-    if (!ok) oq_mbar_wait(bar, sy.phase ^ 1u);
-    oq_tmem_dealloc(tmem, 128);
+    oq_tmem_dealloc(tbase, TCOLS);
   }
-  if (!ok && tid == 0) atomicOr(a.flags, OQ_FLAG_TIMEOUT);
 }

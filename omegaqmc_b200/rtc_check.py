@@ -85,7 +85,7 @@ def compile_mlp_sweep(system):
     """NVRTC-compile the learned-proposal sweep kernel of ``system`` (the
     source oqmc_set_mlp_proposal builds); returns (ok, log, cubin bytes)."""
     src = spec_source(system).replace('#include "oqmc_sweep.cuh"', '#include "oqmc_mlp_sweep.cuh"')
-    return compile_source(src, [f"k_moves_mlp<{system.nocc}, OqSpecBasis>"])
+    return compile_source(src, [f"k_moves_mlp<{system.nocc}, OqSpecBasis, {g}>" for g in (2, 4)])
 
 
 def compile_spec(system):
