@@ -337,8 +337,9 @@ int oqmc_mlp_get_flags(oqmc_mlp* m, unsigned* flags, int clear, void* stream);
  * The network is borrowed and must outlive its use. */
 int oqmc_set_mlp_proposal(oqmc_ctx* ctx, const oqmc_mlp* m);
 /* Walker groups of 128 per CTA of the learned-proposal sweep (2 or 4,
- * default 4): the groups share the weights in shared memory and overlap
- * each other's network and wavefunction work. */
+ * default 2): the groups share the weights in shared memory and overlap
+ * each other's network and wavefunction work.  32,768 walkers make 256
+ * groups, so 4 per CTA would leave most of the 148 SMs idle. */
 int oqmc_set_mlp_groups(oqmc_ctx* ctx, int groups);
 
 #ifdef __cplusplus

@@ -330,7 +330,7 @@ int oqmc_set_mlp_proposal(oqmc_ctx* ctx, const oqmc_mlp* m) {
       return set_err(ctx, OQ_ERR_UNSUPPORTED, "%s", err.c_str());
     ctx->mlp_fn[0] = fns[0];
     ctx->mlp_fn[1] = fns[1];
-    if (ctx->mlp_groups != 2) ctx->mlp_groups = 4;
+    if (ctx->mlp_groups != 4) ctx->mlp_groups = 2;
   }
   ctx->mlp = m;
   return OQ_OK;
@@ -675,7 +675,7 @@ static int launch_moves(oqmc_ctx* ctx, const OqMoveArgs& m, int wpb, size_t sm, 
     const void* C = (const void*)ctx->d_C32;
     OqMlpWeights nw{ctx->mlp->wbf, ctx->mlp->theta};
     void* args[5] = {(void*)&L.sys, (void*)&L.split, (void*)&C, (void*)&mm, (void*)&nw};
-    const int G = ctx->mlp_groups == 2 ? 2 : 4;
+    const int G = ctx->mlp_groups == 4 ? 4 : 2;
     if (oq_rtc_launch(ctx->mlp_fn[G == 4 ? 1 : 0], dim3((m.W + 128 * G - 1) / (128 * G)),
                       dim3(128 * G), oq_mlp_sweep_smem(G), L.stream, args) != 0)
       return set_err(ctx, OQ_ERR_CUDA, "learned-proposal move kernel launch failed%s");
