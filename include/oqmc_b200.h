@@ -83,6 +83,20 @@ typedef struct {
   const double* cusp_q0;   /* natm */
   const double* cusp_coeff;/* natm*8 */
   double e_nn;             /* nuclear repulsion (eps-softened) */
+  /* Cubic B-spline Jastrow terms (psi/gto.py:1657-1931), full coefficient
+   * vectors c[0..N+3] (parameters N + 4, cusp and boundary coefficients
+   * included) on knots k * r_cut / (N + 1). */
+  int has_bs2;
+  int bs2_ncoef_like, bs2_ncoef_unlike;   /* N + 4, at most 32 */
+  double bs2_rcut;
+  const double* bs2_coef_like;
+  const double* bs2_coef_unlike;
+  int has_bs1;
+  int bs1_ntype;                           /* element types, at most 4 */
+  const int* bs1_type;                     /* natm: type of each atom, -1 none */
+  const int* bs1_ncoef;                    /* ntype */
+  const double* bs1_rcut;                  /* ntype */
+  const double* bs1_coef;                  /* ntype blocks of ncoef values */
 } oqmc_system_desc;
 
 /* Library version string. */

@@ -45,6 +45,10 @@ class SystemDesc(ctypes.Structure):
         ("cusp", c_int), ("cusp_rc", P_double), ("cusp_q0", P_double),
         ("cusp_coeff", P_double),
         ("e_nn", c_double),
+        ("has_bs2", c_int), ("bs2_ncoef_like", c_int), ("bs2_ncoef_unlike", c_int),
+        ("bs2_rcut", c_double), ("bs2_coef_like", P_double), ("bs2_coef_unlike", P_double),
+        ("has_bs1", c_int), ("bs1_ntype", c_int), ("bs1_type", P_int), ("bs1_ncoef", P_int),
+        ("bs1_rcut", P_double), ("bs1_coef", P_double),
     ]
 
 

@@ -85,6 +85,32 @@ def pack_system(system: System):
     d.has_j2 = int(system.has_j2)
     d.cusp = int(system.cusp)
     d.e_nn = system.e_nn
+    bs2 = getattr(system, "bs2", None)
+    if bs2 is not None:
+        arr["bs2_coef_like"] = np.ascontiguousarray(bs2["like"], dtype=np.float64)
+        arr["bs2_coef_unlike"] = np.ascontiguousarray(bs2["unlike"], dtype=np.float64)
+        d.has_bs2 = 1
+        d.bs2_ncoef_like = arr["bs2_coef_like"].shape[0]
+        d.bs2_ncoef_unlike = arr["bs2_coef_unlike"].shape[0]
+        d.bs2_rcut = float(bs2["r_cut"])
+    bs1 = getattr(system, "bs1", None)
+    if bs1 is not None:
+        # one table per distinct (coefficients, cutoff): the atoms of an element
+        types, tidx = [], []
+        for entry in bs1:
+            if entry is None:
+                tidx.append(-1)
+                continue
+            key = (tuple(np.asarray(entry[0]).tolist()), float(entry[1]))
+            if key not in types:
+                types.append(key)
+            tidx.append(types.index(key))
+        arr["bs1_type"] = np.array(tidx, dtype=np.int32)
+        arr["bs1_ncoef"] = np.array([len(t[0]) for t in types], dtype=np.int32)
+        arr["bs1_rcut"] = np.array([t[1] for t in types], dtype=np.float64)
+        arr["bs1_coef"] = np.concatenate([np.array(t[0], dtype=np.float64) for t in types])
+        d.has_bs1 = 1
+        d.bs1_ntype = len(types)
     for k, v in arr.items():
         ct = ctypes.c_int if v.dtype == np.int32 else ctypes.c_double
         setattr(d, k, v.ctypes.data_as(ctypes.POINTER(ct)))

@@ -186,9 +186,49 @@ static int fill_system(const oqmc_system_desc* d, OqSystem& S) {
   S.nshell = shell;
   S.nprim_total = prim;
   if (ao != d->nbf) return set_err(nullptr, OQ_ERR_ARG, "group table does not add up to nbf AOs%s");
+  if (d->has_bs2) {
+    const int nl = d->bs2_ncoef_like, nu = d->bs2_ncoef_unlike;
+    if (nl < 6 || nu < 6 || nl > OQ_MAX_BSC || nu > OQ_MAX_BSC || !(d->bs2_rcut > 0.0) ||
+        !d->bs2_coef_like || !d->bs2_coef_unlike)
+      return set_err(nullptr, OQ_ERR_ARG, "bad two-body B-spline table%s");
+    S.has_bs2 = 1;
+    S.bs2_n_like = nl - 4;
+    S.bs2_n_unlike = nu - 4;
+    S.bs2_rcut = d->bs2_rcut;
+    S.bs2_dinv_like = (double)(nl - 3) / d->bs2_rcut;
+    S.bs2_dinv_unlike = (double)(nu - 3) / d->bs2_rcut;
+    for (int k = 0; k < nl; ++k) S.bs2_like[k] = d->bs2_coef_like[k];
+    for (int k = 0; k < nu; ++k) S.bs2_unlike[k] = d->bs2_coef_unlike[k];
+  }
+  for (int i = 0; i < OQ_MAX_NUC; ++i) S.bs1_type[i] = -1;
+  if (d->has_bs1) {
+    if (d->bs1_ntype < 1 || d->bs1_ntype > OQ_MAX_BST || !d->bs1_type || !d->bs1_ncoef ||
+        !d->bs1_rcut || !d->bs1_coef)
+      return set_err(nullptr, OQ_ERR_ARG, "bad one-body B-spline table%s");
+    S.has_bs1 = 1;
+    int off = 0;
+    for (int t = 0; t < d->bs1_ntype; ++t) {
+      const int n = d->bs1_ncoef[t];
+      if (n < 6 || n > OQ_MAX_BSC || !(d->bs1_rcut[t] > 0.0))
+        return set_err(nullptr, OQ_ERR_ARG, "bad one-body B-spline table%s");
+      S.bs1_n[t] = n - 4;
+      S.bs1_rcut[t] = d->bs1_rcut[t];
+      S.bs1_dinv[t] = (double)(n - 3) / d->bs1_rcut[t];
+      for (int k = 0; k < n; ++k) S.bs1_c[t][k] = d->bs1_coef[off + k];
+      off += n;
+    }
+    for (int i = 0; i < d->natm; ++i) {
+      const int t = d->bs1_type[i];
+      if (t < -1 || t >= d->bs1_ntype)
+        return set_err(nullptr, OQ_ERR_ARG, "bad one-body B-spline atom type%s");
+      S.bs1_type[i] = t;
+    }
+  }
   build_harm_table(S.harm);
   return OQ_OK;
 }
+
+static_assert(sizeof(OqSystem) % 16 == 0, "OqSystem is copied in 16-byte chunks");
 
 static void split_for(const OqSystem& S, double tight_alpha, OqSplit& sp) {
   for (int g = 0; g < OQ_MAX_GROUP; ++g) sp.r2[g] = 0.0;
@@ -440,6 +480,9 @@ static uint16_t host_bf16(float f) {
 }
 
 int oqmc_use_tensor_cores(oqmc_ctx* ctx, int enable) {
+  if (ctx && enable && (ctx->hsys.has_bs1 || ctx->hsys.has_bs2))
+    return set_err(ctx, OQ_ERR_UNSUPPORTED,
+                   "the tensor-core local energy supports Pade Jastrow terms only%s");
   if (!ctx) return OQ_ERR_ARG;
   if (!enable) { ctx->use_tc = 0; return OQ_OK; }
   if (ctx->nocc > 16 || 128 / ctx->n_e < 1)

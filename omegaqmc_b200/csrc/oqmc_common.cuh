@@ -28,6 +28,8 @@ typedef unsigned long long uint64_t;
 #define OQ_MAX_E 32
 #define OQ_MAX_COL 4          // contraction columns sharing one exponent list
 #define OQ_MAX_TERMS 96       // monomial terms of the f and g harmonics
+#define OQ_MAX_BSC 32         // B-spline Jastrow coefficients (parameters + 4)
+#define OQ_MAX_BST 4          // element types with a one-body B-spline
 
 // Harmonic monomial tables for am = 3, 4 (am <= 2 are hand-written).
 // term t of component c of am: coef * x^i y^j z^k, packed i | j<<4 | k<<8.
@@ -55,6 +57,15 @@ struct OqSystem {
   int pad2;
   double alpha[OQ_MAX_PRIM];
   double norm[OQ_MAX_NORM];
+  // cubic B-spline Jastrow terms (coefficients c[0..n+3], knots k/dinv,
+  // zero beyond the cutoff): two-body like/unlike, one-body per element type
+  int has_bs1, has_bs2, bs2_n_like, bs2_n_unlike;
+  double bs2_rcut, bs2_dinv_like, bs2_dinv_unlike, bs_pad;
+  double bs2_like[OQ_MAX_BSC], bs2_unlike[OQ_MAX_BSC];
+  int bs1_type[OQ_MAX_NUC];          // element type of each atom, -1: none
+  int bs1_n[OQ_MAX_BST];
+  double bs1_rcut[OQ_MAX_BST], bs1_dinv[OQ_MAX_BST];
+  double bs1_c[OQ_MAX_BST][OQ_MAX_BSC];
   OqHarmTable harm;
 };
 
@@ -157,6 +168,59 @@ __device__ __forceinline__ void oq_pade_vgl_q(T a, T b, T r, T rinv, T& up_r, T&
   const T aq2 = a * q * q;
   up_r = aq2 * rinv;
   lap = (T)-2 * b * aq2 * q + (T)2 * up_r;
+}
+
+// Uniform-knot cubic B-spline u(r) = sum_k w_k(t) c[i+k], x = r dinv,
+// i = clamp(floor(x), 0, n), t = x - i, with the cubic B-spline weights
+// (1-t)^3/6, (3t^3-6t^2+4)/6, (-3t^3+3t^2+3t+1)/6, t^3/6; zero for r >= rcut
+// (_bspline_eval / _bspline_eval_vgl and the callers' cutoff mask,
+// OmegaQMC/psi/gto.py:36-119, 1684-1931).
+template <typename T> __device__ __forceinline__ T oq_floor(T x);
+template <> __device__ __forceinline__ double oq_floor<double>(double x) { return floor(x); }
+template <> __device__ __forceinline__ float oq_floor<float>(float x) { return floorf(x); }
+
+template <typename T>
+__device__ __forceinline__ int oq_bs_index(T x, int n, T& t) {
+  int i = (int)oq_floor<T>(x);
+  i = i < 0 ? 0 : (i > n ? n : i);
+  t = x - (T)i;
+  return i;
+}
+
+template <typename T>
+__device__ __forceinline__ T oq_bs_val(const double* c, int n, T dinv, T rcut, T r) {
+  if (!(r < rcut)) return (T)0;
+  T t;
+  const int i = oq_bs_index<T>(r * dinv, n, t);
+  const T t2 = t * t, t3 = t2 * t;
+  return (T)(1.0 / 6.0) *
+         ((-t3 + (T)3 * t2 - (T)3 * t + (T)1) * (T)c[i] +
+          ((T)3 * t3 - (T)6 * t2 + (T)4) * (T)c[i + 1] +
+          ((T)-3 * t3 + (T)3 * t2 + (T)3 * t + (T)1) * (T)c[i + 2] + t3 * (T)c[i + 3]);
+}
+
+// u'/r and u'' + 2u'/r of the B-spline (the Jastrow gradient factor and
+// Laplacian of one pair), both zero beyond the cutoff.
+template <typename T>
+__device__ __forceinline__ void oq_bs_vgl(const double* c, int n, T dinv, T rcut, T r, T rinv,
+                                          T& up_r, T& lap) {
+  if (!(r < rcut)) {
+    up_r = (T)0;
+    lap = (T)0;
+    return;
+  }
+  T t;
+  const int i = oq_bs_index<T>(r * dinv, n, t);
+  const T t2 = t * t;
+  const T c0 = (T)c[i], c1 = (T)c[i + 1], c2 = (T)c[i + 2], c3 = (T)c[i + 3];
+  const T d1 = (T)(1.0 / 6.0) * dinv *
+               ((-(T)3 * t2 + (T)6 * t - (T)3) * c0 + ((T)9 * t2 - (T)12 * t) * c1 +
+                (-(T)9 * t2 + (T)6 * t + (T)3) * c2 + (T)3 * t2 * c3);
+  const T d2 = (T)(1.0 / 6.0) * dinv * dinv *
+               ((-(T)6 * t + (T)6) * c0 + ((T)18 * t - (T)12) * c1 +
+                (-(T)18 * t + (T)6) * c2 + (T)6 * t * c3);
+  up_r = d1 * rinv;
+  lap = d2 + (T)2 * up_r;
 }
 
 // ---------------------------------------------------------------------------

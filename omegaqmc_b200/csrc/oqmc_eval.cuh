@@ -71,6 +71,29 @@ __device__ __forceinline__ double oq_jastrow_value(const OqSystem& S, const doub
         J += oq_pade(S.j1a[I], S.j1b[I], sqrt(dx * dx + dy * dy + dz * dz));
       }
   }
+  if (S.has_bs2) {
+    for (int i = 0; i < n_e; ++i)
+      for (int j = i + 1; j < n_e; ++j) {
+        const double dx = x[3 * i] - x[3 * j], dy = x[3 * i + 1] - x[3 * j + 1],
+                     dz = x[3 * i + 2] - x[3 * j + 2];
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        const bool like = (i & 1) == (j & 1);
+        J += oq_bs_val<double>(like ? S.bs2_like : S.bs2_unlike,
+                               like ? S.bs2_n_like : S.bs2_n_unlike,
+                               like ? S.bs2_dinv_like : S.bs2_dinv_unlike, S.bs2_rcut, r);
+      }
+  }
+  if (S.has_bs1) {
+    for (int i = 0; i < n_e; ++i)
+      for (int I = 0; I < S.natm; ++I) {
+        const int ty = S.bs1_type[I];
+        if (ty < 0) continue;
+        const double dx = x[3 * i] - S.nuc[I][0], dy = x[3 * i + 1] - S.nuc[I][1],
+                     dz = x[3 * i + 2] - S.nuc[I][2];
+        J += oq_bs_val<double>(S.bs1_c[ty], S.bs1_n[ty], S.bs1_dinv[ty], S.bs1_rcut[ty],
+                               sqrt(dx * dx + dy * dy + dz * dz));
+      }
+  }
   return J;
 }
 
@@ -137,6 +160,20 @@ k_eval(const OqSystem* __restrict__ gsys, const double* __restrict__ gC,
         gx += upr * dx; gy += upr * dy; gz += upr * dz; lp += l;
       }
     }
+    if (S.has_bs2) {
+      for (int j = 0; j < NE; ++j) {
+        if (j == e) continue;
+        const double dx = x[3 * e] - x[3 * j], dy = x[3 * e + 1] - x[3 * j + 1],
+                     dz = x[3 * e + 2] - x[3 * j + 2];
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        const bool like = (e & 1) == (j & 1);
+        double upr, l;
+        oq_bs_vgl<double>(like ? S.bs2_like : S.bs2_unlike, like ? S.bs2_n_like : S.bs2_n_unlike,
+                          like ? S.bs2_dinv_like : S.bs2_dinv_unlike, S.bs2_rcut, r, 1.0 / r,
+                          upr, l);
+        gx += upr * dx; gy += upr * dy; gz += upr * dz; lp += l;
+      }
+    }
     if (S.has_j1) {
       for (int I = 0; I < S.natm; ++I) {
         const double dx = x[3 * e] - S.nuc[I][0], dy = x[3 * e + 1] - S.nuc[I][1],
@@ -144,6 +181,19 @@ k_eval(const OqSystem* __restrict__ gsys, const double* __restrict__ gC,
         const double r = sqrt(dx * dx + dy * dy + dz * dz);
         double upr, l;
         oq_pade_vgl(S.j1a[I], S.j1b[I], r, upr, l);
+        gx += upr * dx; gy += upr * dy; gz += upr * dz; lp += l;
+      }
+    }
+    if (S.has_bs1) {
+      for (int I = 0; I < S.natm; ++I) {
+        const int ty = S.bs1_type[I];
+        if (ty < 0) continue;
+        const double dx = x[3 * e] - S.nuc[I][0], dy = x[3 * e + 1] - S.nuc[I][1],
+                     dz = x[3 * e + 2] - S.nuc[I][2];
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        double upr, l;
+        oq_bs_vgl<double>(S.bs1_c[ty], S.bs1_n[ty], S.bs1_dinv[ty], S.bs1_rcut[ty], r, 1.0 / r,
+                          upr, l);
         gx += upr * dx; gy += upr * dy; gz += upr * dz; lp += l;
       }
     }

@@ -336,6 +336,16 @@ __device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, cons
       const T pa = (T)J.j2[o], pb = (T)J.j2[o + 1];
       dJ += oq_pade_q(pa, pb, rn2t * oq_rsqrt(rn2t)) - oq_pade_q(pa, pb, ro2t * oq_rsqrt(ro2t));
     }
+    if (S.has_bs2) {
+      const double bx = ox - xj, by = oy - yj, bz = oz - zj;
+      const T rn2t = (T)rn2, ro2t = (T)(bx * bx + by * by + bz * bz);
+      const bool like = (e & 1) == (j & 1);
+      const double* c = like ? S.bs2_like : S.bs2_unlike;
+      const int n = like ? S.bs2_n_like : S.bs2_n_unlike;
+      const T dinv = (T)(like ? S.bs2_dinv_like : S.bs2_dinv_unlike), rc = (T)S.bs2_rcut;
+      dJ += oq_bs_val<T>(c, n, dinv, rc, rn2t * oq_rsqrt(rn2t)) -
+            oq_bs_val<T>(c, n, dinv, rc, ro2t * oq_rsqrt(ro2t));
+    }
   }
   for (int I = 0; I < J.natm; ++I) {
     const double ax = nx - J.nuc[I][0], ay = ny - J.nuc[I][1], az = nz - J.nuc[I][2];
@@ -346,6 +356,14 @@ __device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, cons
       const T rn2t = (T)rn2, ro2t = (T)(bx * bx + by * by + bz * bz);
       const T pa = (T)J.j1a[I], pb = (T)J.j1b[I];
       dJ += oq_pade_q(pa, pb, rn2t * oq_rsqrt(rn2t)) - oq_pade_q(pa, pb, ro2t * oq_rsqrt(ro2t));
+    }
+    if (S.has_bs1 && S.bs1_type[I] >= 0) {
+      const int ty = S.bs1_type[I];
+      const double bx = ox - J.nuc[I][0], by = oy - J.nuc[I][1], bz = oz - J.nuc[I][2];
+      const T rn2t = (T)rn2, ro2t = (T)(bx * bx + by * by + bz * bz);
+      const T dinv = (T)S.bs1_dinv[ty], rc = (T)S.bs1_rcut[ty];
+      dJ += oq_bs_val<T>(S.bs1_c[ty], S.bs1_n[ty], dinv, rc, rn2t * oq_rsqrt(rn2t)) -
+            oq_bs_val<T>(S.bs1_c[ty], S.bs1_n[ty], dinv, rc, ro2t * oq_rsqrt(ro2t));
     }
   }
   // new MO row and the ratio vector w_j = sum_m v_m A[m][j]; R = w_i
@@ -554,6 +572,15 @@ __device__ __forceinline__ void oq_eloc_electron(const SJ& J, const OqSystem& S,
       oq_pade_vgl_q((T)J.j2[o], (T)J.j2[o + 1], r2t * rinv, rinv, upr, l);
       jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
     }
+    if (S.has_bs2) {
+      const bool like = (e & 1) == (j & 1);
+      const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
+      T upr, l;
+      oq_bs_vgl<T>(like ? S.bs2_like : S.bs2_unlike, like ? S.bs2_n_like : S.bs2_n_unlike,
+                   (T)(like ? S.bs2_dinv_like : S.bs2_dinv_unlike), (T)S.bs2_rcut, r2t * rinv,
+                   rinv, upr, l);
+      jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
+    }
   }
   for (int I = 0; I < J.natm; ++I) {
     const double dx = xe - J.nuc[I][0], dy = ye - J.nuc[I][1], dz = ze - J.nuc[I][2];
@@ -563,6 +590,14 @@ __device__ __forceinline__ void oq_eloc_electron(const SJ& J, const OqSystem& S,
       const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
       T upr, l;
       oq_pade_vgl_q((T)J.j1a[I], (T)J.j1b[I], r2t * rinv, rinv, upr, l);
+      jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
+    }
+    if (S.has_bs1 && S.bs1_type[I] >= 0) {
+      const int ty = S.bs1_type[I];
+      const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
+      T upr, l;
+      oq_bs_vgl<T>(S.bs1_c[ty], S.bs1_n[ty], (T)S.bs1_dinv[ty], (T)S.bs1_rcut[ty], r2t * rinv,
+                   rinv, upr, l);
       jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
     }
   }

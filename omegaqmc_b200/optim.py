@@ -70,6 +70,9 @@ def raw_to_flat(raw, params_corr, atom_symbols, cusp):
 def walker_derivatives(ctx: GTOContext, X, params_corr, stream=None):
     """(E_L (W,), d ln|psi|/dp (W, P), dE_L/dp (W, P)) in the flat parameter
     order, for walkers X (W, n_e, 3), evaluated in FP64 on the GPU."""
+    if getattr(ctx.system, "bs1", None) is not None or getattr(ctx.system, "bs2", None) is not None:
+        raise NotImplementedError("parameter derivatives cover the Padé terms only; "
+                                  "this trial has B-spline Jastrow terms")
     X = ctx.walkers_tensor(X)
     W = X.shape[0]
     ev = ctx.evaluate(X, want_grad=True, want_lap=False, stream=stream)

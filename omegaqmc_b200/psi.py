@@ -98,7 +98,7 @@ class PsiGTO:
             for kk, v in p.items():
                 if isinstance(v, dict):
                     p[kk] = {a: _np(b) for a, b in v.items()}
-            system = build_system(mf, p, self.params_cusp)
+            system = build_system(mf, p, self.params_cusp, self.jastrow_config)
             ctx = GTOContext(system)
             if len(self._ctx) > 16:
                 self._ctx.clear()

@@ -260,11 +260,12 @@ def parse_params_corr(params_corr, mol, cusp):
     Jastrows are not part of this path).
     """
     params_corr = {} if params_corr is None else dict(params_corr)
-    extra = [k for k in params_corr if k not in ("J1_pade", "J2_pade")]
+    extra = [k for k in params_corr
+             if k not in ("J1_pade", "J2_pade", "J1_bspline", "J2_bspline")]
     if extra:
         raise NotImplementedError(
-            f"Jastrow terms {extra} are not supported; only J1_pade and "
-            "J2_pade are implemented on this path")
+            f"Jastrow terms {extra} are not supported; J1/J2 Padé and B-spline "
+            "terms are implemented on this path")
     natm = mol.natm
     Z = mol.atom_charges().astype(np.float64)
     j1 = np.zeros((natm, 2))
@@ -307,6 +308,77 @@ def parse_params_corr(params_corr, mol, cusp):
     return has_j1, j1, has_j2, j2
 
 
+def bspline_coefs(params, delta_r, cusp_val):
+    """Full coefficient vector (N + 4) of a cubic B-spline Jastrow term from
+    its N parameters: c[1..N] = params, c[0] = params[1] - 2 dr cusp (the
+    cusp condition u'(0) = cusp), c[N+1..N+3] = 0 (u, u', u'' vanish at the
+    cutoff).  Restates _build_bspline_coefs (``gto.py:18-33``)."""
+    p = np.ravel(np.asarray(params, dtype=np.float64))
+    return np.concatenate([[p[1] - 2.0 * delta_r * cusp_val], p, np.zeros(3)])
+
+
+def parse_bspline(params_corr, mol, cusp, jastrow_config=None):
+    """B-spline J1/J2 tables ``(bs2, bs1)``.
+
+    ``bs2``: None or ``{"like": coefs, "unlike": coefs, "r_cut": r}`` with the
+    Kato cusps 1/4 (like) and 1/2 (unlike) built into the coefficients;
+    ``bs1``: None or a per-atom list of ``(coefs, r_cut)`` (None for atoms
+    whose element has no one-body spline), cusp value 0 with cusp-corrected
+    orbitals and -Z without (``gto.py:1657-1931``).  Cutoffs come from
+    ``jastrow_config`` (``{"J2": {"r_cut": r}, "J1": {sym: {"r_cut": r}}}``;
+    10 bohr for every term when it is None, ``gto.py:948-968``).  Entries
+    need at least 2 parameters (``ValueError``, ``vmc_gto.py:580-592``);
+    Padé and B-spline terms of the same body are summed with a warning
+    (``vmc_gto.py:609-617``)."""
+    params_corr = {} if params_corr is None else params_corr
+    for key in ("J1_bspline", "J2_bspline"):
+        if key not in params_corr:
+            continue
+        v = params_corr[key]
+        if not isinstance(v, dict):
+            raise TypeError(f"{key} must be a dict, got {type(v)}")
+        for sk, sv in v.items():
+            if np.ravel(np.asarray(sv)).shape[0] < 2:
+                raise ValueError(f"{key}['{sk}'] must have >= 2 coefficients")
+    for body in ("J1", "J2"):
+        if f"{body}_pade" in params_corr and f"{body}_bspline" in params_corr:
+            warnings.warn(f"Both {body}_pade and {body}_bspline are present; "
+                          "their contributions will be summed.", stacklevel=3)
+    bs2 = None
+    if "J2_bspline" in params_corr:
+        if jastrow_config is None:
+            rc2 = 10.0
+        elif "J2" in jastrow_config:
+            rc2 = float(jastrow_config["J2"]["r_cut"])
+        else:
+            raise ValueError("J2_bspline needs jastrow_config['J2']['r_cut']")
+        p2 = params_corr["J2_bspline"]
+        bs2 = {"r_cut": rc2}
+        for key, cv in (("like", 0.25), ("unlike", 0.5)):
+            p = np.ravel(np.asarray(p2[key], dtype=np.float64))
+            bs2[key] = bspline_coefs(p, rc2 / (p.shape[0] + 1), cv)
+    bs1 = None
+    if "J1_bspline" in params_corr:
+        p1 = params_corr["J1_bspline"]
+        Z = mol.atom_charges().astype(np.float64)
+        bs1 = []
+        for ia in range(mol.natm):
+            sym = mol.atom_symbol(ia)
+            if jastrow_config is None:
+                rc1 = 10.0
+            elif "J1" in jastrow_config and sym in jastrow_config["J1"]:
+                rc1 = float(jastrow_config["J1"][sym]["r_cut"])
+            else:
+                bs1.append(None)
+                continue
+            p = np.ravel(np.asarray(p1[sym], dtype=np.float64))
+            cv = 0.0 if cusp else -Z[ia]
+            bs1.append((bspline_coefs(p, rc1 / (p.shape[0] + 1), cv), rc1))
+        if all(b is None for b in bs1):
+            bs1 = None
+    return bs2, bs1
+
+
 # --------------------------------------------------------------------------
 # Flattened system
 # --------------------------------------------------------------------------
@@ -334,6 +406,8 @@ class System:
     cusp_q0: np.ndarray        # (natm,)
     cusp_coeff: np.ndarray     # (natm, 8)
     symbols: list = field(default_factory=list)
+    bs2: object = None         # B-spline J2: {"like", "unlike": coefs, "r_cut"}
+    bs1: object = None         # B-spline J1: per atom (coefs, r_cut) or None
 
     @property
     def natm(self):
@@ -385,7 +459,7 @@ class System:
         return sum(sh.nprim for sh in self.shells)
 
 
-def build_system(mf, params_corr=None, params_cusp=None):
+def build_system(mf, params_corr=None, params_cusp=None, jastrow_config=None):
     """Build a :class:`System` from a PySCF-style mean-field object.
 
     Args:
@@ -395,6 +469,7 @@ def build_system(mf, params_corr=None, params_cusp=None):
             "J2_pade": {"like": [a, b], "unlike": [a, b]}}``.
         params_cusp: ``{sym: {"q0": float, "coeff": (8,)}}`` or None for no
             cusp correction (``gto.py:846-888``).
+        jastrow_config: B-spline cutoffs (see :func:`parse_bspline`).
     """
     mol = mf.mol
     n_e = mol.tot_electrons()
@@ -427,8 +502,11 @@ def build_system(mf, params_corr=None, params_cusp=None):
             if cf.shape[0] != 8:
                 raise ValueError(f"cusp coeff for {sym} must have 8 entries")
             coeff[ia] = cf
-    has_j1, j1, has_j2, j2 = parse_params_corr(params_corr, mol, cusp)
+    pc = {} if params_corr is None else params_corr
+    has_j1, j1, has_j2, j2 = parse_params_corr(
+        {k: v for k, v in pc.items() if not k.endswith("_bspline")}, mol, cusp)
+    bs2, bs1 = parse_bspline(pc, mol, cusp, jastrow_config)
     return System(nuc=mol.atom_coords(unit="Bohr"), Z=Z, shells=shells, C=C,
                   n_up=n_up, n_dn=n_dn, has_j1=has_j1, j1=j1, has_j2=has_j2,
                   j2=j2, cusp=cusp, cusp_rc=rc, cusp_q0=q0,
-                  cusp_coeff=coeff, symbols=mol.elements)
+                  cusp_coeff=coeff, symbols=mol.elements, bs2=bs2, bs1=bs1)

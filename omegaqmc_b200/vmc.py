@@ -125,18 +125,19 @@ def get_vmc_gto_func(mf, params_corr, cusp_scheme="Quady2025", gr_scheme="scheme
     timestamp_init = datetime.now()
     print("Begin time: {}".format(timestamp_init))
     return VMCDriverGTO(mf, params_corr, params_cusp, prefix, timestamp_init,
-                        precision=precision, proposal=proposal, specialize=specialize)
+                        precision=precision, proposal=proposal, specialize=specialize,
+                        jastrow_config=jastrow_config)
 
 
 class VMCDriverGTO:
     """Runs VMC sampling of one trial wavefunction (``vmc_gto.py:672-1617``)."""
 
     def __init__(self, mf, params_corr, params_cusp, prefix, timestamp_init,
-                 precision="fp64", proposal="plain", specialize=True):
+                 precision="fp64", proposal="plain", specialize=True, jastrow_config=None):
         self.mf = mf
         self.params_corr = params_corr
         self.params_cusp = params_cusp
-        self.system = build_system(mf, params_corr, params_cusp)
+        self.system = build_system(mf, params_corr, params_cusp, jastrow_config)
         self.ctx = GTOContext(self.system)
         if specialize:
             try:

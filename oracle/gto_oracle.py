@@ -257,8 +257,33 @@ def _pairs(n_e):
     return np.triu_indices(n_e, k=1)
 
 
+def bspline_vgl(c, r, r_cut):
+    """Uniform-knot cubic B-spline u(r), u'(r), u''(r) with coefficients
+    c[0..N+3] on knots k * dr, dr = r_cut / (N + 1), zero for r >= r_cut
+    (``_bspline_eval_vgl``, ``gto.py:67-119``, with the callers' cutoff
+    mask)."""
+    c = np.asarray(c, dtype=np.float64)
+    n = c.shape[0] - 4
+    dinv = (n + 1) / r_cut
+    x = r * dinv
+    i = np.clip(np.floor(x).astype(np.int64), 0, n)
+    t = x - i
+    t2, t3 = t * t, t * t * t
+    w = [(-t3 + 3 * t2 - 3 * t + 1) / 6, (3 * t3 - 6 * t2 + 4) / 6,
+         (-3 * t3 + 3 * t2 + 3 * t + 1) / 6, t3 / 6]
+    w1 = [(-3 * t2 + 6 * t - 3) / 6, (9 * t2 - 12 * t) / 6, (-9 * t2 + 6 * t + 3) / 6,
+          3 * t2 / 6]
+    w2 = [(-6 * t + 6) / 6, (18 * t - 12) / 6, (-18 * t + 6) / 6, 6 * t / 6]
+    cs = [c[i + k] for k in range(4)]
+    val = sum(w[k] * cs[k] for k in range(4))
+    d1 = sum(w1[k] * cs[k] for k in range(4)) * dinv
+    d2 = sum(w2[k] * cs[k] for k in range(4)) * dinv * dinv
+    m = (r < r_cut).astype(np.float64)
+    return val * m, d1 * m, d2 * m
+
+
 def jastrow_value(system, X):
-    """J1 + J2 (``gto.py:1500-1573``)."""
+    """J1 + J2 (``gto.py:1500-1573``, Padé; ``1684-1780``, B-spline)."""
     W, n_e, _ = X.shape
     J = np.zeros(W)
     if system.has_j2:
@@ -277,6 +302,24 @@ def jastrow_value(system, X):
         a = system.j1[:, 0][None, :, None]
         b = system.j1[:, 1][None, :, None]
         J += np.sum(a * r / (1.0 + b * r), axis=(1, 2))
+    bs2 = getattr(system, "bs2", None)
+    if bs2 is not None:
+        i, j = _pairs(n_e)
+        d = X[:, i] - X[:, j]
+        r = np.sqrt(np.sum(d * d, axis=-1))
+        same = (i % 2) == (j % 2)
+        u_l = bspline_vgl(bs2["like"], r, bs2["r_cut"])[0]
+        u_u = bspline_vgl(bs2["unlike"], r, bs2["r_cut"])[0]
+        J += np.sum(u_l * same, axis=-1) + np.sum(u_u * (~same), axis=-1)
+    bs1 = getattr(system, "bs1", None)
+    if bs1 is not None:
+        for I, entry in enumerate(bs1):
+            if entry is None:
+                continue
+            c, rc = entry
+            d = X - system.nuc[I][None, None, :]
+            r = np.sqrt(np.sum(d * d, axis=-1))
+            J += np.sum(bspline_vgl(c, r, rc)[0], axis=-1)
     return J
 
 
@@ -312,6 +355,34 @@ def jastrow_vgl(system, X):
         upp = -2.0 * a * b / (den * den * den)
         grad += np.sum((up / r)[..., None] * d, axis=2)
         lap += np.sum(upp + 2.0 * up / r, axis=2)
+    bs2 = getattr(system, "bs2", None)
+    if bs2 is not None:
+        i, j = _pairs(n_e)
+        d = X[:, i] - X[:, j]
+        r = np.sqrt(np.sum(d * d, axis=-1))
+        same = (i % 2) == (j % 2)
+        _, ul, ull = bspline_vgl(bs2["like"], r, bs2["r_cut"])
+        _, uu, uuu = bspline_vgl(bs2["unlike"], r, bs2["r_cut"])
+        up = np.where(same, ul, uu)
+        upp = np.where(same, ull, uuu)
+        gp = (up / r)[..., None] * d
+        lp = upp + 2.0 * up / r
+        for k in range(len(i)):
+            grad[:, i[k]] += gp[:, k]
+            grad[:, j[k]] -= gp[:, k]
+            lap[:, i[k]] += lp[:, k]
+            lap[:, j[k]] += lp[:, k]
+    bs1 = getattr(system, "bs1", None)
+    if bs1 is not None:
+        for I, entry in enumerate(bs1):
+            if entry is None:
+                continue
+            c, rc = entry
+            d = X - system.nuc[I][None, None, :]
+            r = np.sqrt(np.sum(d * d, axis=-1))
+            _, up, upp = bspline_vgl(c, r, rc)
+            grad += (up / r)[..., None] * d
+            lap += upp + 2.0 * up / r
     return grad, lap
 
 

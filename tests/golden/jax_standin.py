@@ -199,6 +199,7 @@ jnp.einsum = lambda eq, *ops: torch.einsum(eq, *[_f(o) for o in ops])
 jnp.dot = lambda a, b: _f(a) @ _f(b)
 jnp.outer = lambda a, b: torch.outer(_f(a), _f(b))
 jnp.take = lambda x, idx, axis=None: torch.index_select(_t(x), axis, _t(idx))
+jnp.clip = lambda x, a=None, b=None: torch.clamp(_t(x), a, b)
 
 
 def _triu(n, k=0, m=None):

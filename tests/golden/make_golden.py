@@ -178,6 +178,29 @@ CASES = {
                                            "unlike": np.array([0.5, 0.7])}},
                   0.8, 12),
     "nojastrow": (lambda: M.named_system("LiH"), False, lambda mol: {}, 1.0, 8),
+    # B-spline one- and two-body Jastrows with short cutoffs (walkers cross
+    # them), and B-spline summed with Padé at the default 10-bohr cutoff
+    "h2o_bspline": (lambda: M.named_system("H2O"), False,
+                    lambda mol: {"J1_bspline": {"O": np.array([0.3, -0.2, 0.1, 0.05, -0.02, 0.01]),
+                                                "H": np.array([0.1, 0.05, -0.03, 0.02])},
+                                 "J2_bspline": {"like": np.array([0.2, 0.1, 0.05, 0.02, 0.01]),
+                                                "unlike": np.array([0.4, 0.25, 0.1, 0.05, 0.02,
+                                                                    0.01])}},
+                    1.1, 24),
+    "lih_bspline_pade": (lambda: M.named_system("LiH"), True,
+                         lambda mol: {"J2_pade": {"like": np.array([0.25, 1.0]),
+                                                  "unlike": np.array([0.5, 1.0])},
+                                      "J2_bspline": {"like": np.array([0.1, 0.05, 0.02, 0.01]),
+                                                     "unlike": np.array([0.2, 0.1, 0.03])},
+                                      "J1_bspline": {"Li": np.array([-0.3, -0.1, 0.05]),
+                                                     "H": np.array([-0.1, 0.02])}},
+                         1.0, 16),
+}
+
+# B-spline cutoffs per case (jastrow_config of _PsiGTO, gto.py:948-968)
+JASTROW_CONFIG = {
+    "h2o_bspline": {"J2": {"r_cut": 4.0},
+                    "J1": {"O": {"r_cut": 3.5}, "H": {"r_cut": 3.0}}},
 }
 
 
@@ -189,9 +212,10 @@ def run_case(gto, name, seed):
     pcusp = M.synthetic_cusp_params(mol, seed=seed + 11) if cusp else None
     X = _walkers(mol, nw, sigma, seed + 101)
     rmf = _RefMF(mf)
+    jcfg = JASTROW_CONFIG.get(name)
     obj = gto._PsiGTO(rmf, params_cusp=(
         {s: {"q0": torch.tensor(v["q0"]), "coeff": torch.tensor(v["coeff"])}
-         for s, v in pcusp.items()} if cusp else None))
+         for s, v in pcusp.items()} if cusp else None), jastrow_config=jcfg)
     nuc = torch.tensor(mol.atom_coords())
     tp = {}
     for k, v in params.items():
@@ -216,6 +240,15 @@ def run_case(gto, name, seed):
                 g, L = obj._J2_pade_vgl(x, tp["J2_pade"])
                 grad = grad + g.reshape(-1)
                 lap = lap + L
+            if "J1_bspline" in tp:
+                g, L = obj._J1_bspline_vgl(x, nuc, tp["J1_bspline"])
+                grad = grad + g.reshape(-1)
+                lap = lap + L
+            if "J2_bspline" in tp:
+                for fn in (obj._J2_bspline_aa_vgl, obj._J2_bspline_ab_vgl):
+                    g, L = fn(x, tp["J2_bspline"])
+                    grad = grad + g.reshape(-1)
+                    lap = lap + L
         out["logpsi"].append(float(lp))
         out["e_ke"].append(float(ke))
         out["e_ee"].append(float(obj.local_energy_ee(x)))
@@ -231,7 +264,7 @@ def run_case(gto, name, seed):
             warnings.simplefilter("ignore")
             ke_h.append(float(obj._local_energy_ke_hessian(x, nuc, tp)))
     spec = {"atoms": mol._atom, "basis": mol._basis, "cusp": pcusp,
-            "params_corr": params}
+            "params_corr": params, "jastrow_config": jcfg}
     res = {k: np.array(v) for k, v in out.items()}
     res.update(X=X, mo_coeff=mf.mo_coeff, mo_occ=mf.mo_occ, e_nn=e_nn,
                e_ke_hessian=np.array(ke_h),
@@ -240,12 +273,21 @@ def run_case(gto, name, seed):
 
 
 def main():
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cases", nargs="*", default=None,
+                    help="generate only these cases (default: all, plus binning and cusp)")
+    args = ap.parse_args()
     gto, shell, utils = load_reference()
     os.makedirs(HERE, exist_ok=True)
     for k, name in enumerate(CASES):
+        if args.cases is not None and name not in args.cases:
+            continue
         res = run_case(gto, name, seed=k)
         np.savez_compressed(os.path.join(HERE, f"golden_{name}.npz"), **res)
         print(f"{name}: {len(res['logpsi'])} walkers, logpsi[0]={res['logpsi'][0]:.12f}")
+    if args.cases is not None:
+        return
     # binning analysis on a seeded AR(1) series
     rng = np.random.default_rng(42)
     x = np.zeros(2000)

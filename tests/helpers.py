@@ -51,7 +51,8 @@ def load_golden(name):
 
 def golden_system(name):
     mf, params, cusp, d = load_golden(name)
-    return build_system(mf, params, cusp), d
+    spec = json.loads(str(d["spec"]))
+    return build_system(mf, params, cusp, spec.get("jastrow_config")), d
 
 
 def seeded_walkers(system, n, sigma, seed):
