@@ -235,9 +235,10 @@ int oqmc_measure_peak(int kind, double* out_rate, void* stream);
 /* Jastrow-parameter derivatives per walker, the inputs of the linear-method
  * optimiser (compute_walker_derivs, OmegaQMC/vmcopt_gto_linear.py:686-703,
  * which differentiates log_trial_wavefunction and the local energy with
- * jax.grad).  Raw parameters, oqmc_param_count(ctx) = 4 + 2 natm of them:
- * J2 like a, like b, unlike a, unlike b, then J1 a_I, b_I for every atom
- * (terms absent from the context give zeros).  grad = the (W, n_e, 3)
+ * jax.grad).  Raw parameters, oqmc_param_count(ctx) of them: J2 like a,
+ * like b, unlike a, unlike b, then J1 a_I, b_I for every atom (Padé; absent
+ * terms give zeros), then the B-spline parameters: J2 like, J2 unlike, then
+ * J1 per element type (bs1_ncoef - 4 each, types in descriptor order).  grad = the (W, n_e, 3)
  * gradient of ln|psi| that oqmc_eval returns for the same walkers; outputs
  * dlogpsi, dEL are (W, count), FP64. */
 int oqmc_param_count(const oqmc_ctx* ctx);

@@ -95,20 +95,19 @@ def pack_system(system: System):
         d.bs2_rcut = float(bs2["r_cut"])
     bs1 = getattr(system, "bs1", None)
     if bs1 is not None:
-        # one table per distinct (coefficients, cutoff): the atoms of an element
-        types, tidx = [], []
-        for entry in bs1:
-            if entry is None:
-                tidx.append(-1)
-                continue
-            key = (tuple(np.asarray(entry[0]).tolist()), float(entry[1]))
-            if key not in types:
-                types.append(key)
-            tidx.append(types.index(key))
-        arr["bs1_type"] = np.array(tidx, dtype=np.int32)
-        arr["bs1_ncoef"] = np.array([len(t[0]) for t in types], dtype=np.int32)
-        arr["bs1_rcut"] = np.array([t[1] for t in types], dtype=np.float64)
-        arr["bs1_coef"] = np.concatenate([np.array(t[0], dtype=np.float64) for t in types])
+        # one table per element, in order of the element's first atom (the
+        # raw parameter order of oqmc_param_derivs)
+        syms = []
+        for ia, entry in enumerate(bs1):
+            if entry is not None and system.symbols[ia] not in syms:
+                syms.append(system.symbols[ia])
+        tables = [bs1[system.symbols.index(sym)] for sym in syms]
+        arr["bs1_type"] = np.array([syms.index(system.symbols[ia]) if e is not None else -1
+                                    for ia, e in enumerate(bs1)], dtype=np.int32)
+        arr["bs1_ncoef"] = np.array([len(t[0]) for t in tables], dtype=np.int32)
+        arr["bs1_rcut"] = np.array([t[1] for t in tables], dtype=np.float64)
+        arr["bs1_coef"] = np.concatenate([np.asarray(t[0], dtype=np.float64) for t in tables])
+        types = tables
         d.has_bs1 = 1
         d.bs1_ntype = len(types)
     for k, v in arr.items():

@@ -400,13 +400,93 @@ __device__ __forceinline__ void oq_pade_dp(double a, double b, double r, double 
   dL[1] = dupp1 + 2.0 * dup[1] / r;
 }
 
+// B-spline parameters: P_q is coefficient q+1 and coefficient 0 is
+// P_1 - 2 dr cusp, so a term at distance r in knot interval i touches the
+// parameters of coefficients i..i+3 (and P_1 through coefficient 0).
+__device__ __forceinline__ void oq_bs_param_add(const OqSystem& S, const double* c, int n,
+                                                double dinv, double rcut, double r, double gd,
+                                                bool half, double* dl, double* de) {
+  if (!(r < rcut)) return;
+  double t;
+  const int i = oq_bs_index<double>(r * dinv, n, t);
+  const double t2 = t * t, t3 = t2 * t, s6 = 1.0 / 6.0;
+  const double w[4] = {s6 * (-t3 + 3 * t2 - 3 * t + 1), s6 * (3 * t3 - 6 * t2 + 4),
+                       s6 * (-3 * t3 + 3 * t2 + 3 * t + 1), s6 * t3};
+  const double w1[4] = {s6 * dinv * (-3 * t2 + 6 * t - 3), s6 * dinv * (9 * t2 - 12 * t),
+                        s6 * dinv * (-9 * t2 + 6 * t + 3), s6 * dinv * 3 * t2};
+  const double w2[4] = {s6 * dinv * dinv * (-6 * t + 6), s6 * dinv * dinv * (18 * t - 12),
+                        s6 * dinv * dinv * (-18 * t + 6), s6 * dinv * dinv * 6 * t};
+  (void)c;
+  for (int k = 0; k < 4; ++k) {
+    const int idx = i + k;
+    const int q = idx == 0 ? 1 : idx - 1;      // coefficient 0 depends on P_1
+    if (q < 0 || q >= n) continue;
+    const double dL = w2[k] + 2.0 * w1[k] / r;
+    dl[q] += w[k];
+    de[q] -= half ? 0.5 * (dL + 2.0 * w1[k] * gd) : dL + w1[k] * gd;
+  }
+}
+
+__device__ void oq_param_derivs_bspline(const OqSystem& S, const double* x, const double* g,
+                                        int n_e, double* dl, double* de) {
+  int base = 4 + 2 * S.natm;
+  if (S.has_bs2) {
+    for (int i = 0; i < n_e; ++i)
+      for (int j = i + 1; j < n_e; ++j) {
+        const double dx = x[3 * i] - x[3 * j], dy = x[3 * i + 1] - x[3 * j + 1],
+                     dz = x[3 * i + 2] - x[3 * j + 2];
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        const double gd = ((g[3 * i] - g[3 * j]) * dx + (g[3 * i + 1] - g[3 * j + 1]) * dy +
+                           (g[3 * i + 2] - g[3 * j + 2]) * dz) / r;
+        const bool like = (i & 1) == (j & 1);
+        if (like)
+          oq_bs_param_add(S, S.bs2_like, S.bs2_n_like, S.bs2_dinv_like, S.bs2_rcut, r, gd, false,
+                          dl + base, de + base);
+        else
+          oq_bs_param_add(S, S.bs2_unlike, S.bs2_n_unlike, S.bs2_dinv_unlike, S.bs2_rcut, r, gd,
+                          false, dl + base + S.bs2_n_like, de + base + S.bs2_n_like);
+      }
+    base += S.bs2_n_like + S.bs2_n_unlike;
+  }
+  if (S.has_bs1) {
+    int tbase[OQ_MAX_BST];
+    for (int t = 0, b = base; t < OQ_MAX_BST; ++t) {
+      tbase[t] = b;
+      b += S.bs1_n[t];
+    }
+    for (int I = 0; I < S.natm; ++I) {
+      const int ty = S.bs1_type[I];
+      if (ty < 0) continue;
+      for (int e = 0; e < n_e; ++e) {
+        const double dx = x[3 * e] - S.nuc[I][0], dy = x[3 * e + 1] - S.nuc[I][1],
+                     dz = x[3 * e + 2] - S.nuc[I][2];
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        const double gd = (g[3 * e] * dx + g[3 * e + 1] * dy + g[3 * e + 2] * dz) / r;
+        oq_bs_param_add(S, S.bs1_c[ty], S.bs1_n[ty], S.bs1_dinv[ty], S.bs1_rcut[ty], r, gd, true,
+                        dl + tbase[ty], de + tbase[ty]);
+      }
+    }
+  }
+}
+
+static int param_count_of(const OqSystem& S) {
+  int n = 4 + 2 * S.natm;
+  if (S.has_bs2) n += S.bs2_n_like + S.bs2_n_unlike;
+  if (S.has_bs1)
+    for (int t = 0; t < OQ_MAX_BST; ++t) n += S.bs1_n[t];
+  return n;
+}
+
 __global__ void k_param_derivs(const OqSystem* __restrict__ gsys, const double* __restrict__ X,
                                const double* __restrict__ G, int W, int n_e,
                                double* __restrict__ dlog, double* __restrict__ del) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= W) return;
   const OqSystem& S = *gsys;
-  const int n_raw = 4 + 2 * S.natm;
+  int n_raw = 4 + 2 * S.natm;
+  if (S.has_bs2) n_raw += S.bs2_n_like + S.bs2_n_unlike;
+  if (S.has_bs1)
+    for (int t = 0; t < OQ_MAX_BST; ++t) n_raw += S.bs1_n[t];
   const double* x = X + (size_t)w * n_e * 3;
   const double* g = G + (size_t)w * n_e * 3;
   double* dl = dlog + (size_t)w * n_raw;
@@ -431,6 +511,7 @@ __global__ void k_param_derivs(const OqSystem* __restrict__ gsys, const double* 
       }
     for (int k = 0; k < 4; ++k) { dl[k] = al[k]; de[k] = ae[k]; }
   }
+  if (S.has_bs2 || S.has_bs1) oq_param_derivs_bspline(S, x, g, n_e, dl, de);
   if (S.has_j1) {
     for (int I = 0; I < S.natm; ++I) {
       double sl0 = 0, sl1 = 0, se0 = 0, se1 = 0;
@@ -451,7 +532,7 @@ __global__ void k_param_derivs(const OqSystem* __restrict__ gsys, const double* 
   }
 }
 
-int oqmc_param_count(const oqmc_ctx* ctx) { return ctx ? 4 + 2 * ctx->natm : OQ_ERR_ARG; }
+int oqmc_param_count(const oqmc_ctx* ctx) { return ctx ? param_count_of(ctx->hsys) : OQ_ERR_ARG; }
 
 int oqmc_param_derivs(oqmc_ctx* ctx, const double* X, int W, const double* grad, double* dlogpsi,
                       double* dEL, void* stream) {

@@ -40,15 +40,37 @@ def flatten_params(params_corr):
     return np.array(flat, dtype=np.float64), layout
 
 
-def raw_to_flat(raw, params_corr, atom_symbols, cusp):
+def raw_to_flat(raw, params_corr, system):
     """Map per-walker derivatives of the library's raw parameters (J2 like a,
-    like b, unlike a, unlike b, then J1 a_I, b_I per atom) onto the flat
-    parameter order; J1 entries collect the atoms of their element."""
+    like b, unlike a, unlike b, then J1 a_I, b_I per atom; then the B-spline
+    parameters: J2 like, J2 unlike, J1 per element in order of first atom)
+    onto the flat parameter order; Padé J1 entries collect the atoms of
+    their element."""
     raw = np.asarray(raw)
+    atom_symbols, cusp = list(system.symbols), system.cusp
     _, layout = flatten_params(params_corr)
     out = np.zeros((raw.shape[0], sum(n for _, _, n in layout)))
+    # offsets of the B-spline blocks in the raw layout
+    bs_off = {}
+    b = 4 + 2 * system.natm
+    if getattr(system, "bs2", None) is not None:
+        nl, nu = len(system.bs2["like"]) - 4, len(system.bs2["unlike"]) - 4
+        bs_off[("J2_bspline", "like")] = b
+        bs_off[("J2_bspline", "unlike")] = b + nl
+        b += nl + nu
+    seen = []
+    for ia, e in enumerate(getattr(system, "bs1", None) or []):
+        if e is not None and atom_symbols[ia] not in seen:
+            seen.append(atom_symbols[ia])
+            bs_off[("J1_bspline", atom_symbols[ia])] = b
+            b += len(e[0]) - 4
     o = 0
     for term, key, n in layout:
+        if term.endswith("_bspline"):
+            if (term, key) in bs_off:
+                out[:, o:o + n] = raw[:, bs_off[(term, key)]:bs_off[(term, key)] + n]
+            o += n
+            continue
         if term == "J2_pade":
             k = 0 if key == "like" else 2
             out[:, o] = raw[:, k]
@@ -70,9 +92,6 @@ def raw_to_flat(raw, params_corr, atom_symbols, cusp):
 def walker_derivatives(ctx: GTOContext, X, params_corr, stream=None):
     """(E_L (W,), d ln|psi|/dp (W, P), dE_L/dp (W, P)) in the flat parameter
     order, for walkers X (W, n_e, 3), evaluated in FP64 on the GPU."""
-    if getattr(ctx.system, "bs1", None) is not None or getattr(ctx.system, "bs2", None) is not None:
-        raise NotImplementedError("parameter derivatives cover the Padé terms only; "
-                                  "this trial has B-spline Jastrow terms")
     X = ctx.walkers_tensor(X)
     W = X.shape[0]
     ev = ctx.evaluate(X, want_grad=True, want_lap=False, stream=stream)
@@ -81,10 +100,8 @@ def walker_derivatives(ctx: GTOContext, X, params_corr, stream=None):
     de = torch.empty(W, n_raw, dtype=torch.float64, device=ctx.device)
     ctx._check(ctx.lib.oqmc_param_derivs(ctx._h, _dptr(X), W, _dptr(ev["grad"]), _dptr(dl),
                                          _dptr(de), _stream_ptr(stream)))
-    s = ctx.system
-    syms = list(s.symbols)
-    dl_f = raw_to_flat(dl.cpu().numpy(), params_corr, syms, s.cusp)
-    de_f = raw_to_flat(de.cpu().numpy(), params_corr, syms, s.cusp)
+    dl_f = raw_to_flat(dl.cpu().numpy(), params_corr, ctx.system)
+    de_f = raw_to_flat(de.cpu().numpy(), params_corr, ctx.system)
     return ev["e_loc"].cpu().numpy(), dl_f, de_f
 
 

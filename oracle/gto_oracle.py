@@ -476,9 +476,66 @@ def _pade_param_terms(a, b, r):
     return du, dup, dL
 
 
+def bspline_types(system):
+    """Element symbols with a one-body B-spline, in order of first atom: the
+    element types of the device tables and of the raw parameter layout."""
+    out = []
+    for ia, e in enumerate(getattr(system, "bs1", None) or []):
+        if e is not None and system.symbols[ia] not in out:
+            out.append(system.symbols[ia])
+    return out
+
+
+def _bspline_param_terms(c, r, r_cut):
+    """Coefficient indices (i..i+3) and the weights of u, u', u'' on them."""
+    n = len(c) - 4
+    dinv = (n + 1) / r_cut
+    x = r * dinv
+    i = np.clip(np.floor(x).astype(np.int64), 0, n)
+    t = x - i
+    t2, t3 = t * t, t * t * t
+    w = [(-t3 + 3 * t2 - 3 * t + 1) / 6, (3 * t3 - 6 * t2 + 4) / 6,
+         (-3 * t3 + 3 * t2 + 3 * t + 1) / 6, t3 / 6]
+    w1 = [v * dinv for v in ((-3 * t2 + 6 * t - 3) / 6, (9 * t2 - 12 * t) / 6,
+                             (-9 * t2 + 6 * t + 3) / 6, 3 * t2 / 6)]
+    w2 = [v * dinv * dinv for v in ((-6 * t + 6) / 6, (18 * t - 12) / 6, (-18 * t + 6) / 6,
+                                    6 * t / 6)]
+    m = r < r_cut
+    return i, w, w1, w2, m, n
+
+
+def _scatter_bspline(dl, de, base, n, i, w, w1, w2, m, r, gd, half):
+    """Add the parameter derivatives of spline terms at distances r
+    (flattened over walkers x terms, walker index wi) into dl/de rows.
+    Parameter P_q is coefficient q+1; coefficient 0 = P_1 - 2 dr cusp."""
+    W = dl.shape[0]
+    for k in range(4):
+        idx = i + k
+        dL = w2[k] + 2.0 * w1[k] / r
+        ce = (0.5 * (dL + 2.0 * w1[k] * gd)) if half else (dL + w1[k] * gd)
+        for q in range(n):
+            sel = ((idx == q + 1) | ((q == 1) & (idx == 0))) & m
+            dl[:, base + q] += np.sum(np.where(sel, w[k], 0.0), axis=-1)
+            de[:, base + q] -= np.sum(np.where(sel, ce, 0.0), axis=-1)
+
+
+def param_count(system):
+    """Raw parameters: Padé (4 + 2 natm), then the J2 B-spline like and
+    unlike parameters, then the J1 B-spline parameters per element type."""
+    n = 4 + 2 * system.natm
+    bs2 = getattr(system, "bs2", None)
+    if bs2 is not None:
+        n += len(bs2["like"]) - 4 + len(bs2["unlike"]) - 4
+    for sym in bspline_types(system):
+        ia = system.symbols.index(sym)
+        n += len(system.bs1[ia][0]) - 4
+    return n
+
+
 def param_derivatives(system, X, grad=None):
-    """Per-walker d log|psi| / dp and d E_L / dp for the raw Padé parameters
-    p = (J2 like a, like b, unlike a, unlike b, then J1 a_I, b_I per atom).
+    """Per-walker d log|psi| / dp and d E_L / dp for the raw parameters
+    (``param_count``): Padé p = (J2 like a, like b, unlike a, unlike b, then J1
+    a_I, b_I per atom), then the B-spline parameters.
 
     lnpsi depends on p only through J; E_L only through its kinetic part
     -1/2 sum_e (lap_e + |G_e|^2) with G_e the full gradient of ln|psi|
@@ -488,7 +545,7 @@ def param_derivatives(system, X, grad=None):
     W, n_e, _ = X.shape
     if grad is None:
         grad = evaluate(system, X)["grad"]
-    n_raw = 4 + 2 * system.natm
+    n_raw = param_count(system)
     dl = np.zeros((W, n_raw))
     de = np.zeros((W, n_raw))
     if system.has_j2:
@@ -514,4 +571,27 @@ def param_derivatives(system, X, grad=None):
             for q in range(2):
                 dl[:, 4 + 2 * I + q] = np.sum(du[q], axis=-1)
                 de[:, 4 + 2 * I + q] = -0.5 * np.sum(dL[q] + 2.0 * dup[q] * gdot, axis=-1)
+    base = 4 + 2 * system.natm
+    bs2 = getattr(system, "bs2", None)
+    if bs2 is not None:
+        i, j = _pairs(n_e)
+        d = X[:, i] - X[:, j]
+        r = np.sqrt(np.sum(d * d, axis=-1))
+        gd = np.sum((grad[:, i] - grad[:, j]) * d, axis=-1) / r
+        same = (i % 2) == (j % 2)
+        for key, mask in (("like", same), ("unlike", ~same)):
+            ii, w, w1, w2, m, n = _bspline_param_terms(bs2[key], r, bs2["r_cut"])
+            _scatter_bspline(dl, de, base, n, ii, w, w1, w2, m & mask[None, :], r, gd, False)
+            base += n
+    for sym in bspline_types(system):
+        for I, entry in enumerate(system.bs1):
+            if entry is None or system.symbols[I] != sym:
+                continue
+            c, rc = entry
+            d = X - system.nuc[I][None, None, :]
+            r = np.sqrt(np.sum(d * d, axis=-1))
+            gd = np.sum(grad * d, axis=-1) / r
+            ii, w, w1, w2, m, n = _bspline_param_terms(c, r, rc)
+            _scatter_bspline(dl, de, base, n, ii, w, w1, w2, m, r, gd, True)
+        base += len(system.bs1[system.symbols.index(sym)][0]) - 4
     return dl, de

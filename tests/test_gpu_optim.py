@@ -12,21 +12,34 @@ from omegaqmc_b200.system import build_system
 
 pytestmark = pytest.mark.gpu
 
-CASES = [("LiH", True), ("H2O", False), ("N2", False)]
+CASES = [("LiH", True, False), ("H2O", False, False), ("N2", False, False), ("H2O", False, True),
+         ("LiH", True, True)]
 
 
-@pytest.mark.parametrize("name,cusp", CASES)
-def test_param_derivatives_match_oracle(name, cusp):
+def _params(mol, cusp, bspline):
+    pc = M.default_params_corr(mol, cusp=cusp, j1=True)
+    if bspline:
+        pc["J2_bspline"] = {"like": np.array([0.2, 0.1, 0.05, 0.02]),
+                            "unlike": np.array([0.4, 0.25, 0.1, 0.05, 0.02])}
+        pc["J1_bspline"] = {s: np.array([-0.1, 0.05, 0.02]) for s in set(mol.elements)}
+    return pc
+
+
+@pytest.mark.filterwarnings("ignore::UserWarning")
+@pytest.mark.parametrize("name,cusp,bspline", CASES)
+def test_param_derivatives_match_oracle(name, cusp, bspline):
     mf = M.make_mf(name)
-    pc = M.default_params_corr(mf.mol, cusp=cusp, j1=True)
+    pc = _params(mf.mol, cusp, bspline)
     pcu = M.synthetic_cusp_params(mf.mol) if cusp else None
-    s = build_system(mf, pc, pcu)
+    cfg = ({"J2": {"r_cut": 3.5}, "J1": {e: {"r_cut": 3.0} for e in set(mf.mol.elements)}}
+           if bspline else None)
+    s = build_system(mf, pc, pcu, cfg)
     ctx = GTOContext(s)
     X = seeded_walkers(s, 257, 0.9, 11)          # ragged: 3 CTAs of 128
     e, dl, de = walker_derivatives(ctx, X, pc)
     ref_dl_raw, ref_de_raw = O.param_derivatives(s, X)
-    ref_dl = raw_to_flat(ref_dl_raw, pc, s.symbols, s.cusp)
-    ref_de = raw_to_flat(ref_de_raw, pc, s.symbols, s.cusp)
+    ref_dl = raw_to_flat(ref_dl_raw, pc, s)
+    ref_de = raw_to_flat(ref_de_raw, pc, s)
     sc_l = np.abs(ref_dl).max(axis=0) + 1.0
     sc_e = np.abs(ref_de).max(axis=0) + 1.0
     assert np.max(np.abs(dl - ref_dl) / sc_l) < 1e-10

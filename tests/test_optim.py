@@ -37,8 +37,8 @@ def test_flat_derivatives_match_finite_differences():
     s = build_system(mf, pc)
     X = seeded_walkers(s, 5, 0.8, 2)
     dl_raw, de_raw = O.param_derivatives(s, X)
-    dl = raw_to_flat(dl_raw, pc, s.symbols, s.cusp)
-    de = raw_to_flat(de_raw, pc, s.symbols, s.cusp)
+    dl = raw_to_flat(dl_raw, pc, s)
+    de = raw_to_flat(de_raw, pc, s)
     flat, _ = flatten_params(pc)
     for k in range(flat.size):
         h = 1e-5 * max(1.0, abs(flat[k]))
@@ -66,3 +66,31 @@ def test_build_matrices_definitions():
     dD = dl - dl.mean(axis=0)
     np.testing.assert_allclose(H[1:, 0], (dD * E[:, None]).mean(axis=0))
     np.testing.assert_allclose(H[1:, 1:], dD.T @ (de + dD * E[:, None]) / 200)
+
+
+def test_flat_bspline_derivatives_match_finite_differences():
+    mf = M.make_mf("H2O")
+    pc = {"J1_bspline": {"O": np.array([0.3, -0.2, 0.1]), "H": np.array([0.1, 0.05, -0.03])},
+          "J2_bspline": {"like": np.array([0.2, 0.1, 0.05]), "unlike": np.array([0.4, 0.25, 0.1])},
+          "J2_pade": {"like": [0.25, 3.0], "unlike": [0.5, 3.0]}}
+    cfg = {"J2": {"r_cut": 3.0}, "J1": {"O": {"r_cut": 2.5}, "H": {"r_cut": 2.0}}}
+    import warnings
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        s = build_system(mf, pc, None, cfg)
+        X = seeded_walkers(s, 4, 0.9, 5)
+        dl_raw, de_raw = O.param_derivatives(s, X)
+        dl = raw_to_flat(dl_raw, pc, s)
+        de = raw_to_flat(de_raw, pc, s)
+        flat, _ = flatten_params(pc)
+        for k in range(flat.size):
+            h = 1e-6
+            fp, fm = flat.copy(), flat.copy()
+            fp[k] += h
+            fm[k] -= h
+            sp = build_system(mf, _set_flat(pc, fp), None, cfg)
+            sm = build_system(mf, _set_flat(pc, fm), None, cfg)
+            fd_l = (O.log_psi(sp, X) - O.log_psi(sm, X)) / (2 * h)
+            fd_e = (O.evaluate(sp, X)["e_loc"] - O.evaluate(sm, X)["e_loc"]) / (2 * h)
+            np.testing.assert_allclose(dl[:, k], fd_l, rtol=1e-5, atol=1e-6)
+            np.testing.assert_allclose(de[:, k], fd_e, rtol=1e-4, atol=5e-5 * (1 + np.abs(fd_e).max()))

@@ -44,3 +44,32 @@ def test_param_derivatives_match_finite_differences(name):
         fd_e = (O.evaluate(sp, X)["e_loc"] - O.evaluate(sm, X)["e_loc"]) / (2 * h)
         np.testing.assert_allclose(dl[:, k], fd_l, rtol=1e-6, atol=1e-7)
         np.testing.assert_allclose(de[:, k], fd_e, rtol=1e-5, atol=1e-5 * (1 + np.abs(fd_e).max()))
+
+
+def test_bspline_param_derivatives_match_finite_differences():
+    mf = M.make_mf("H2O")
+    pc = {"J1_bspline": {"O": np.array([0.3, -0.2, 0.1, 0.05]), "H": np.array([0.1, 0.05, -0.03])},
+          "J2_bspline": {"like": np.array([0.2, 0.1, 0.05, 0.02]),
+                         "unlike": np.array([0.4, 0.25, 0.1, 0.05, 0.02])}}
+    cfg = {"J2": {"r_cut": 3.0}, "J1": {"O": {"r_cut": 2.5}, "H": {"r_cut": 2.0}}}
+    s = build_system(mf, pc, None, cfg)
+    X = seeded_walkers(s, 5, 0.9, 4)
+    dl, de = O.param_derivatives(s, X)
+    assert dl.shape[1] == O.param_count(s) == 4 + 6 + 4 + 5 + 4 + 3
+    keys = [("J2_bspline", "like", 4), ("J2_bspline", "unlike", 5), ("J1_bspline", "O", 4),
+            ("J1_bspline", "H", 3)]
+    col = 4 + 2 * s.natm
+    for term, key, n in keys:
+        for q in range(n):
+            pp, pm = copy.deepcopy(pc), copy.deepcopy(pc)
+            h = 1e-6
+            pp[term][key] = pc[term][key].copy()
+            pm[term][key] = pc[term][key].copy()
+            pp[term][key][q] += h
+            pm[term][key][q] -= h
+            sp, sm = build_system(mf, pp, None, cfg), build_system(mf, pm, None, cfg)
+            fd_l = (O.log_psi(sp, X) - O.log_psi(sm, X)) / (2 * h)
+            fd_e = (O.evaluate(sp, X)["e_loc"] - O.evaluate(sm, X)["e_loc"]) / (2 * h)
+            np.testing.assert_allclose(dl[:, col], fd_l, rtol=1e-6, atol=1e-7)
+            np.testing.assert_allclose(de[:, col], fd_e, rtol=1e-5, atol=2e-5 * (1 + np.abs(fd_e).max()))
+            col += 1
