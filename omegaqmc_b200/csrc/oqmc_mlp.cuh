@@ -419,6 +419,58 @@ __device__ __forceinline__ void oq_mlp_features(const SJ& J, PosF P, int ne, int
   f[31] = 1.0f;
 }
 
+// The same features for a compile-time electron count: the squared
+// distances to the other electrons are computed once and kept in
+// registers, the 8 nearest are selected with branch-free compare/selects
+// (same order and tie rule as oq_mlp_features) and only their coordinates
+// are read again.
+template <int NE, class SJ, class PosF>
+__device__ __forceinline__ void oq_mlp_features_ne(const SJ& J, PosF P, int e, double xe,
+                                                   double ye, double ze, float f[OQ_MLP_K0]) {
+  double d0 = 1e300, d1 = 1e300;
+  int i0 = 0, i1 = 0;
+  for (int I = 0; I < J.natm; ++I) {
+    const double ax = xe - J.nuc[I][0], ay = ye - J.nuc[I][1], az = ze - J.nuc[I][2];
+    const double r2 = ax * ax + ay * ay + az * az;
+    if (r2 < d0) {
+      d1 = d0; i1 = i0; d0 = r2; i0 = I;
+    } else if (r2 < d1) {
+      d1 = r2; i1 = I;
+    }
+  }
+  if (J.natm == 1) i1 = i0;
+  f[0] = (float)(xe - J.nuc[i0][0]); f[1] = (float)(ye - J.nuc[i0][1]); f[2] = (float)(ze - J.nuc[i0][2]);
+  f[3] = (float)(xe - J.nuc[i1][0]); f[4] = (float)(ye - J.nuc[i1][1]); f[5] = (float)(ze - J.nuc[i1][2]);
+  double r2[NE];
+#pragma unroll
+  for (int j = 0; j < NE; ++j) {
+    const double ax = P(j, 0) - xe, ay = P(j, 1) - ye, az = P(j, 2) - ze;
+    r2[j] = (j == e) ? 1e300 : ax * ax + ay * ay + az * az;
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    double best = 1e300;
+    int bj = -1;
+#pragma unroll
+    for (int j = 0; j < NE; ++j) {
+      const bool c = r2[j] < best;
+      best = c ? r2[j] : best;
+      bj = c ? j : bj;
+    }
+#pragma unroll
+    for (int j = 0; j < NE; ++j) r2[j] = (j == bj) ? 1e300 : r2[j];
+    if (bj < 0) {
+      f[6 + 3 * k] = 0.0f; f[7 + 3 * k] = 0.0f; f[8 + 3 * k] = 0.0f;
+    } else {
+      f[6 + 3 * k] = (float)(P(bj, 0) - xe);
+      f[7 + 3 * k] = (float)(P(bj, 1) - ye);
+      f[8 + 3 * k] = (float)(P(bj, 2) - ze);
+    }
+  }
+  f[30] = (e & 1) ? -1.0f : 1.0f;
+  f[31] = 1.0f;
+}
+
 // Write the 32 features of row r as BF16 into a K-major buffer (KC = 4).
 __device__ __forceinline__ void oq_mlp_store_features(unsigned char* act, int r,
                                                       const float f[OQ_MLP_K0]) {

@@ -136,7 +136,7 @@ k_moves_mlp(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gspli
       const float uc = ((float)rc.x + 0.5f) * 2.3283064365386963e-10f;
       const double ox = P(e, 0), oy = P(e, 1), oz = P(e, 2);
       float f[OQ_MLP_K0], out[OQ_MLP_NOUT];
-      oq_mlp_features(J, P, NE, e, ox, oy, oz, f);
+      oq_mlp_features_ne<NE>(J, P, e, ox, oy, oz, f);
       oq_mlp_store_features(act, r, f);
       ok = oq_mlp_forward_group(act, wreg, bias, tmem, bar, phase, r, bar_id, out);
       if (!ok) break;
@@ -144,7 +144,7 @@ k_moves_mlp(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gspli
       oq_mix_sample_f(out, uc, n3, d);
       const float lqf = oq_mix_logq_f(out, (float)d[0], (float)d[1], (float)d[2]);
       const double nx = ox + d[0], ny = oy + d[1], nz = oz + d[2];
-      oq_mlp_features(J, P, NE, e, nx, ny, nz, f);
+      oq_mlp_features_ne<NE>(J, P, e, nx, ny, nz, f);
       oq_mlp_store_features(act, r, f);
       ok = oq_mlp_forward_group(act, wreg, bias, tmem, bar, phase, r, bar_id, out);
       if (!ok) break;
