@@ -230,31 +230,50 @@ struct Gen {
             angular(g, k, false, "R" + ks, "", "");
           }
         } else {
+          // Radial factors: cusp groups always in FP64; groups with tight
+          // exponents in FP64 within their split radius, else in the working
+          // precision; other groups in the working precision only.
           bool cusp = false;
           for (int k = 0; k < nc; ++k) cusp = cusp || (s_shell && S.s_cusp[sh0 + k]);
+          const bool split = SP.r2[g] > 0.0;
           for (int k = 0; k < nc; ++k) {
             const std::string ks = std::to_string(k);
             add("    T RT" + ks + ", RpT" + ks + ", RlT" + ks + ";\n");
           }
-          add("    if (sizeof(T) == 8 || r2d < " + num(SP.r2[g]) + (cusp ? " || true" : "") +
-              ") {\n      {\n");
-          radial(g, true, "double", "r2d");
-          for (int k = 0; k < nc; ++k) {
-            const std::string ks = std::to_string(k);
-            if (s_shell && S.s_cusp[sh0 + k])
-              add("      oq_cusp_vgl(S, " + std::to_string(ia) + ", sqrt(r2d), R" + ks + ", Rp" + ks +
-                  ", Rl" + ks + ");\n");
-            add("      RT" + ks + " = (T)R" + ks + "; RpT" + ks + " = (T)Rp" + ks + "; RlT" + ks +
-                " = (T)Rl" + ks + ";\n");
+          auto fp64_inline = [&]() {
+            add("      {\n");
+            radial(g, true, "double", "r2d");
+            for (int k = 0; k < nc; ++k) {
+              const std::string ks = std::to_string(k);
+              if (s_shell && S.s_cusp[sh0 + k])
+                add("      oq_cusp_vgl(S, " + std::to_string(ia) + ", sqrt(r2d), R" + ks + ", Rp" +
+                    ks + ", Rl" + ks + ");\n");
+              add("      RT" + ks + " = (T)R" + ks + "; RpT" + ks + " = (T)Rp" + ks + "; RlT" + ks +
+                  " = (T)Rl" + ks + ";\n");
+            }
+            add("      }\n");
+          };
+          auto working = [&]() {
+            add("      {\n");
+            radial(g, true, "T", "r2");
+            for (int k = 0; k < nc; ++k) {
+              const std::string ks = std::to_string(k);
+              add("      RT" + ks + " = R" + ks + "; RpT" + ks + " = Rp" + ks + "; RlT" + ks +
+                  " = Rl" + ks + ";\n");
+            }
+            add("      }\n");
+          };
+          if (cusp) {
+            fp64_inline();
+          } else if (split) {
+            add("    if (sizeof(T) == 8 || r2d < " + num(SP.r2[g]) + ") {\n");
+            fp64_inline();
+            add("    } else {\n");
+            working();
+            add("    }\n");
+          } else {
+            working();
           }
-          add("      }\n    } else {\n      {\n");
-          radial(g, true, "T", "r2");
-          for (int k = 0; k < nc; ++k) {
-            const std::string ks = std::to_string(k);
-            add("      RT" + ks + " = R" + ks + "; RpT" + ks + " = Rp" + ks + "; RlT" + ks + " = Rl" +
-                ks + ";\n");
-          }
-          add("      }\n    }\n");
           for (int k = 0; k < nc; ++k) {
             const std::string ks = std::to_string(k);
             angular(g, k, true, "RT" + ks, "RpT" + ks, "RlT" + ks);
