@@ -256,16 +256,17 @@ def parse_params_corr(params_corr, mol, cusp):
     element carries ``[a, b]``; without them ``a = -Z`` and the entry is
     ``b`` (an ``[a, b]`` entry warns and its ``a`` is ignored; any other
     length raises ``ValueError``).  Keys other than ``J1_pade`` and
-    ``J2_pade`` raise ``NotImplementedError`` (B-spline and three-body
-    Jastrows are not part of this path).
+    ``J2_pade`` and the B-spline / J3_eeI terms (parsed by
+    :func:`parse_bspline` and :func:`parse_j3`) raise
+    ``NotImplementedError``.
     """
     params_corr = {} if params_corr is None else dict(params_corr)
     extra = [k for k in params_corr
-             if k not in ("J1_pade", "J2_pade", "J1_bspline", "J2_bspline")]
+             if k not in ("J1_pade", "J2_pade", "J1_bspline", "J2_bspline", "J3_eeI")]
     if extra:
         raise NotImplementedError(
-            f"Jastrow terms {extra} are not supported; J1/J2 Padé and B-spline "
-            "terms are implemented on this path")
+            f"Jastrow terms {extra} are not supported; J1/J2 Padé, B-spline "
+            "and J3_eeI terms are implemented on this path")
     natm = mol.natm
     Z = mol.atom_charges().astype(np.float64)
     j1 = np.zeros((natm, 2))
@@ -306,6 +307,190 @@ def parse_params_corr(params_corr, mol, cusp):
                 raise ValueError(f"J2_pade['{key}'] needs [a, b]")
             j2[k] = v[:2]
     return has_j1, j1, has_j2, j2
+
+
+# ---------------------------------------------------------------------------
+# Three-body electron-electron-nucleus Jastrow (J3_eeI)
+# ---------------------------------------------------------------------------
+J3_DEFAULT = {"N_eI": 3, "N_ee": 3, "r_cut": 5.0}     # _parse_eeI_cfg, gto.py:970-984
+J3_MAX_ORDER = 6
+
+
+def eeI_num_params(n_eI, n_ee):
+    """Free parameters of one J3_eeI polynomial block: unique gammas
+    (symmetric in the two electron-nucleus orders) minus the no-cusp
+    constraints (``_compute_eeI_num_params``, gto.py:243-251)."""
+    n_gamma = (n_eI + 1) * (n_eI + 2) // 2 * (n_ee + 1)
+    return n_gamma - ((2 * n_eI + 1) + (n_eI + n_ee + 1))
+
+
+def eeI_constraint_map(n_eI, n_ee, r_cut):
+    """Linear map from the free J3_eeI parameters to the unique gammas.
+
+    Returns ``(A, lmn)``: ``gamma_unique = A @ free`` and ``lmn[k]`` the
+    (l, m, n) powers of unique gamma k (l >= m; gamma(l, m, n) =
+    gamma(m, l, n)).  The constraints make the polynomial cusp-free at
+    r_ee = 0 and at r_eI = 0 given the (r_eI - L)^3 envelope; the free
+    parameters are the columns left without a pivot when the constraint
+    matrix is row-reduced with partial pivoting (QMCPACK
+    PolynomialFunctor3D; the same rows, pivot rule and 1e-6 threshold as
+    ``_build_eeI_constraint_map``, gto.py:321-463, so that the same
+    parameter vector means the same gammas).
+    """
+    if n_ee < 1:
+        raise ValueError("J3_eeI needs N_ee >= 1 (the e-e cusp row uses n = 1)")
+    half = 0.5 * r_cut
+    cont = 3.0                                  # envelope continuity order
+    lmn = [(l, m, n) for m in range(n_eI + 1) for l in range(m, n_eI + 1)
+           for n in range(n_ee + 1)]
+    slot = {}
+    for k, (l, m, n) in enumerate(lmn):
+        slot[(l, m, n)] = k
+        slot[(m, l, n)] = k
+    ng = len(lmn)
+    nrow = (2 * n_eI + 1) + (n_eI + n_ee + 1)
+    K = np.zeros((nrow, ng))
+    # r_ee cusp: the n = 1 gammas of each total order l + m
+    for tot in range(2 * n_eI + 1):
+        for m in range(tot + 1):
+            l = tot - m
+            if l <= n_eI and m <= n_eI and l >= m:
+                K[tot, slot[(l, m, 1)]] = 2.0 if l > m else 1.0
+    # r_eI cusp: one row per order l + n of the electron at the nucleus
+    base = 2 * n_eI + 1
+    for tot in range(n_eI + n_ee + 1):
+        if tot <= n_ee:
+            K[base + tot, slot[(0, 0, tot)]] = cont
+            if n_eI >= 1:
+                K[base + tot, slot[(0, 1, tot)]] = -half
+        for l in range(1, tot + 1):
+            n = tot - l
+            if 0 <= n <= n_ee and l <= n_eI:
+                K[base + tot, slot[(l, 0, n)]] = cont
+                if n_eI >= 1:
+                    K[base + tot, slot[(l, 1, n)]] = -half
+    free = np.zeros(ng, dtype=bool)
+    col = -1
+    for row in range(nrow):
+        col += 1
+        while col < ng:
+            piv = row + int(np.argmax(np.abs(K[row:, col])))
+            if abs(K[piv, col]) >= 1e-6:
+                break
+            free[col] = True
+            col += 1
+        if col >= ng:
+            break
+        K[[row, piv]] = K[[piv, row]]
+        K[row] /= K[row, col]
+        f = K[:, col].copy()
+        f[row] = 0.0
+        K -= f[:, None] * K[row][None, :]
+    free[col + 1:] = True
+    fcols = np.flatnonzero(free)
+    dcols = np.flatnonzero(~free)
+    if fcols.size != eeI_num_params(n_eI, n_ee):
+        raise ValueError("J3_eeI constraint system is rank deficient")
+    A = np.zeros((ng, fcols.size))
+    A[fcols, np.arange(fcols.size)] = 1.0
+    for r, dc in enumerate(dcols):
+        A[dc] = -K[r, fcols]
+    return A, lmn
+
+
+def eeI_gamma(params, n_eI, n_ee, r_cut):
+    """Full symmetric gamma array (n_eI+1, n_eI+1, n_ee+1) of one block
+    from its free parameters (``_vec_to_gamma_3d``, gto.py:466-478)."""
+    A, lmn = eeI_constraint_map(n_eI, n_ee, r_cut)
+    vec = A @ np.asarray(params, dtype=np.float64)
+    g = np.zeros((n_eI + 1, n_eI + 1, n_ee + 1))
+    for k, (l, m, n) in enumerate(lmn):
+        g[l, m, n] = vec[k]
+        g[m, l, n] = vec[k]
+    return g
+
+
+def parse_j3(params_corr, mol, jastrow_config=None):
+    """J3_eeI tables, or None without a ``J3_eeI`` entry.
+
+    ``params_corr["J3_eeI"]`` maps ``"like+<sym>"`` / ``"unlike+<sym>"`` to
+    free-parameter vectors (same-spin and opposite-spin electron pairs
+    around nuclei of element ``sym``).  Orders and cutoff come from
+    ``jastrow_config["J3"]`` (``N_eI``, ``N_ee``, ``r_cut``; defaults 3, 3,
+    5.0 bohr, gto.py:970-984).  Validation follows the driver
+    (vmc_gto.py:595-611: a non-dict raises ``TypeError``, a key without the
+    prefix ``ValueError``) and ``_sanitize_J3_eeI_params`` (gto.py:254-306:
+    an entry that is not a 1-D vector of the right length warns and becomes
+    zeros; the length is checked against the configured orders).  Keys of
+    elements absent from the molecule are ignored, as in ``J3_eeI_fn``
+    (gto.py:2011-2035), which sums over the molecule's elements.
+
+    Returns ``{"n_eI", "n_ee", "r_cut", "types": per-atom type (-1 none),
+    "elements": symbol per type, "gamma": (ntype, 2, n_eI+1, n_eI+1,
+    n_ee+1) with block 0 like and 1 unlike, "on": (ntype, 2) flags,
+    "params": the sanitised dict}``.
+    """
+    if not params_corr or "J3_eeI" not in params_corr:
+        return None
+    v = params_corr["J3_eeI"]
+    if not isinstance(v, dict):
+        raise TypeError(f"J3_eeI params must be a dict, got {type(v)}")
+    for k in v:
+        if not (k.startswith("like+") or k.startswith("unlike+")):
+            raise ValueError(f"J3_eeI sub-key '{k}' must start with 'like+' or 'unlike+'")
+    cfg = dict(J3_DEFAULT)
+    if jastrow_config is not None and "J3" in jastrow_config:
+        j = jastrow_config["J3"]
+        for k in ("N_eI", "N_ee"):
+            if k in j:
+                cfg[k] = int(j[k])
+        if "r_cut" in j:
+            cfg["r_cut"] = float(j["r_cut"])
+    n_eI, n_ee, r_cut = cfg["N_eI"], cfg["N_ee"], cfg["r_cut"]
+    if not (0 <= n_eI <= J3_MAX_ORDER and 1 <= n_ee <= J3_MAX_ORDER):
+        raise ValueError(f"J3 orders N_eI={n_eI}, N_ee={n_ee} out of range "
+                         f"(0..{J3_MAX_ORDER}, 1..{J3_MAX_ORDER})")
+    if not r_cut > 0.0:
+        raise ValueError("J3 r_cut must be positive")
+    npar = eeI_num_params(n_eI, n_ee)
+    clean = {}
+    for k, val in v.items():
+        try:
+            arr = np.asarray(val, dtype=np.float64)
+        except Exception:
+            warnings.warn(f"J3_eeI['{k}']: cannot convert to array; replacing with zeros",
+                          stacklevel=3)
+            clean[k] = np.zeros(npar)
+            continue
+        if arr.ndim != 1:
+            warnings.warn(f"J3_eeI['{k}']: expected 1-D array, got ndim={arr.ndim}; "
+                          "replacing with zeros", stacklevel=3)
+            clean[k] = np.zeros(npar)
+        elif arr.shape[0] != npar:
+            warnings.warn(f"J3_eeI['{k}']: expected {npar} params (for N_eI={n_eI}, "
+                          f"N_ee={n_ee}), got {arr.shape[0]}; replacing with zeros",
+                          stacklevel=3)
+            clean[k] = np.zeros(npar)
+        else:
+            clean[k] = arr.copy()
+    elements = []
+    for ia in range(mol.natm):
+        sym = mol.atom_symbol(ia)
+        if sym not in elements and ("like+" + sym in clean or "unlike+" + sym in clean):
+            elements.append(sym)
+    if not elements:
+        return None
+    types = [elements.index(mol.atom_symbol(ia)) if mol.atom_symbol(ia) in elements else -1
+             for ia in range(mol.natm)]
+    gamma = np.zeros((len(elements), 2, n_eI + 1, n_eI + 1, n_ee + 1))
+    on = np.zeros((len(elements), 2), dtype=np.int32)
+    for t, sym in enumerate(elements):
+        for b, prefix in enumerate(("like+", "unlike+")):
+            if prefix + sym in clean:
+                gamma[t, b] = eeI_gamma(clean[prefix + sym], n_eI, n_ee, r_cut)
+                on[t, b] = 1
+    return {"n_eI": n_eI, "n_ee": n_ee, "r_cut": r_cut, "types": types,
+            "elements": elements, "gamma": gamma, "on": on, "params": clean}
 
 
 def bspline_coefs(params, delta_r, cusp_val):
@@ -408,6 +593,7 @@ class System:
     symbols: list = field(default_factory=list)
     bs2: object = None         # B-spline J2: {"like", "unlike": coefs, "r_cut"}
     bs1: object = None         # B-spline J1: per atom (coefs, r_cut) or None
+    j3: object = None          # J3_eeI tables (see :func:`parse_j3`) or None
 
     @property
     def natm(self):
@@ -469,7 +655,8 @@ def build_system(mf, params_corr=None, params_cusp=None, jastrow_config=None):
             "J2_pade": {"like": [a, b], "unlike": [a, b]}}``.
         params_cusp: ``{sym: {"q0": float, "coeff": (8,)}}`` or None for no
             cusp correction (``gto.py:846-888``).
-        jastrow_config: B-spline cutoffs (see :func:`parse_bspline`).
+        jastrow_config: B-spline cutoffs (see :func:`parse_bspline`) and
+            the J3_eeI orders and cutoff (see :func:`parse_j3`).
     """
     mol = mf.mol
     n_e = mol.tot_electrons()
@@ -504,9 +691,11 @@ def build_system(mf, params_corr=None, params_cusp=None, jastrow_config=None):
             coeff[ia] = cf
     pc = {} if params_corr is None else params_corr
     has_j1, j1, has_j2, j2 = parse_params_corr(
-        {k: v for k, v in pc.items() if not k.endswith("_bspline")}, mol, cusp)
+        {k: v for k, v in pc.items() if not k.endswith("_bspline") and k != "J3_eeI"},
+        mol, cusp)
     bs2, bs1 = parse_bspline(pc, mol, cusp, jastrow_config)
+    j3 = parse_j3(pc, mol, jastrow_config)
     return System(nuc=mol.atom_coords(unit="Bohr"), Z=Z, shells=shells, C=C,
                   n_up=n_up, n_dn=n_dn, has_j1=has_j1, j1=j1, has_j2=has_j2,
                   j2=j2, cusp=cusp, cusp_rc=rc, cusp_q0=q0,
-                  cusp_coeff=coeff, symbols=mol.elements, bs2=bs2, bs1=bs1)
+                  cusp_coeff=coeff, symbols=mol.elements, bs2=bs2, bs1=bs1, j3=j3)

@@ -13,6 +13,7 @@ walkers, line by line from:
 * ``OmegaQMC/psi/gto.py:728-778``    Slater assembly (inverse, Gamma, lap)
 * ``OmegaQMC/psi/gto.py:1278-1290``  log|det| of the up and down blocks
 * ``OmegaQMC/psi/gto.py:1493-1649``  Padé J1/J2 value and VGL
+* ``OmegaQMC/psi/gto.py:243-604, 1933-2196``  J3_eeI three-body Jastrow
 * ``OmegaQMC/psi/gto.py:2220-2254``  log|psi| = log|det| + J
 * ``OmegaQMC/psi/gto.py:2406-2451``  eps-softened Coulomb terms
 * ``OmegaQMC/psi/gto.py:2506-2579``  analytic kinetic energy
@@ -282,8 +283,194 @@ def bspline_vgl(c, r, r_cut):
     return val * m, d1 * m, d2 * m
 
 
+# ---------------------------------------------------------------------------
+# J3_eeI (gto.py:243-604, 1933-2196)
+# ---------------------------------------------------------------------------
+def eeI_constraint_map(N_eI, N_ee, r_cut):
+    """gamma_unique = A @ free and the (l, m, n) of each unique gamma,
+    restating ``_build_eeI_constraint_map`` (gto.py:321-463) loop by loop."""
+    L = 0.5 * r_cut
+    index = {}
+    lmn = []
+    for m in range(N_eI + 1):
+        for l in range(m, N_eI + 1):
+            for n in range(N_ee + 1):
+                index[(l, m, n)] = index[(m, l, n)] = len(lmn)
+                lmn.append((l, m, n))
+    NG = len(lmn)
+    NC = (2 * N_eI + 1) + (N_eI + N_ee + 1)
+    Cm = np.zeros((NC, NG))
+    for k in range(2 * N_eI + 1):
+        for mi in range(k + 1):
+            li = k - mi
+            if li <= N_eI and mi <= N_eI:
+                if li > mi:
+                    Cm[k, index[(li, mi, 1)]] = 2.0
+                elif li == mi:
+                    Cm[k, index[(li, mi, 1)]] = 1.0
+    ro = 2 * N_eI + 1
+    for kp in range(N_eI + N_ee + 1):
+        if kp <= N_ee:
+            Cm[ro + kp, index[(0, 0, kp)]] = 3.0
+            if N_eI >= 1:
+                Cm[ro + kp, index[(0, 1, kp)]] = -L
+        for li in range(1, kp + 1):
+            ni = kp - li
+            if 0 <= ni <= N_ee and li <= N_eI:
+                Cm[ro + kp, index[(li, 0, ni)]] = 3.0
+                if N_eI >= 1:
+                    Cm[ro + kp, index[(li, 1, ni)]] = -L
+    indep = np.zeros(NG, dtype=bool)
+    col = -1
+    for row in range(NC):
+        while True:
+            col += 1
+            if col >= NG:
+                break
+            best, big = row, abs(Cm[row, col])
+            for ri in range(row + 1, NC):
+                if abs(Cm[ri, col]) > big:
+                    best, big = ri, abs(Cm[ri, col])
+            if big < 1e-6:
+                indep[col] = True
+                continue
+            break
+        if col >= NG:
+            break
+        Cm[[row, best]] = Cm[[best, row]]
+        Cm[row] /= Cm[row, col]
+        for ri in range(NC):
+            if ri != row:
+                Cm[ri] -= Cm[ri, col] * Cm[row]
+    for c in range(col + 1, NG):
+        indep[c] = True
+    ic = np.where(indep)[0]
+    dc = np.where(~indep)[0]
+    A = np.zeros((NG, len(ic)))
+    for p, j in enumerate(ic):
+        A[j, p] = 1.0
+    for c, i in enumerate(dc):
+        for p, j in enumerate(ic):
+            A[i, p] = -Cm[c, j]
+    return A, lmn
+
+
+def eeI_gamma3d(free, N_eI, N_ee, r_cut):
+    """Symmetric gamma(l, m, n) of one block (``_vec_to_gamma_3d``)."""
+    A, lmn = eeI_constraint_map(N_eI, N_ee, r_cut)
+    vec = A @ np.asarray(free, dtype=np.float64)
+    g = np.zeros((N_eI + 1, N_eI + 1, N_ee + 1))
+    for k, (l, m, n) in enumerate(lmn):
+        g[l, m, n] = g[m, l, n] = vec[k]
+    return g
+
+
+def _j3_blocks(system):
+    """(atom index, same-spin flag, gamma) for every populated block."""
+    j3 = getattr(system, "j3", None)
+    if j3 is None:
+        return []
+    syms = list(system.symbols)
+    out = []
+    for I in range(system.natm):
+        for prefix, same in (("like+", True), ("unlike+", False)):
+            key = prefix + syms[I]
+            if key in j3["params"]:
+                out.append((I, same, eeI_gamma3d(j3["params"][key], j3["n_eI"], j3["n_ee"],
+                                                 j3["r_cut"])))
+    return out
+
+
+def _eeI_poly_derivs(g, r12, r1, r2, L):
+    """u = P (r1-L)^3 (r2-L)^3 and its partials for particle 1
+    (``_eval_eeI_poly_vgl``, gto.py:508-604): u, u_1, u_12, u_11, u_1212,
+    u_1_12."""
+    nI, _, nE = g.shape
+    P = P1 = P11 = P12 = P112 = P1212 = 0.0
+    for l in range(nI):
+        for m in range(nI):
+            for n in range(nE):
+                c = g[l, m, n]
+                if c == 0.0:
+                    continue
+                a = r1 ** l
+                a1 = l * r1 ** (l - 1) if l >= 1 else 0.0
+                a2 = l * (l - 1) * r1 ** (l - 2) if l >= 2 else 0.0
+                b = r2 ** m
+                e = r12 ** n
+                e1 = n * r12 ** (n - 1) if n >= 1 else 0.0
+                e2 = n * (n - 1) * r12 ** (n - 2) if n >= 2 else 0.0
+                P = P + c * a * b * e
+                P1 = P1 + c * a1 * b * e
+                P11 = P11 + c * a2 * b * e
+                P12 = P12 + c * a * b * e1
+                P112 = P112 + c * a1 * b * e1
+                P1212 = P1212 + c * a * b * e2
+    s1, s2 = r1 - L, r2 - L
+    E = s1 ** 3 * s2 ** 3
+    E1 = 3.0 * s1 ** 2 * s2 ** 3
+    E11 = 6.0 * s1 * s2 ** 3
+    return (P * E, P1 * E + P * E1, P12 * E, P11 * E + 2.0 * P1 * E1 + P * E11, P1212 * E,
+            P112 * E + P12 * E1)
+
+
+def j3_value(system, X):
+    """J3_eeI = -sum over nuclei I and pairs i<j of the block's u, for
+    r_iI, r_jI < L (``J3_eeI_fn``, gto.py:1951-2040)."""
+    W, n_e, _ = X.shape
+    J = np.zeros(W)
+    blocks = _j3_blocks(system)
+    if not blocks:
+        return J
+    L = 0.5 * system.j3["r_cut"]
+    i, j = _pairs(n_e)
+    for I, same, g in blocks:
+        sel = ((i % 2) == (j % 2)) == same
+        for k in np.flatnonzero(sel):
+            a, b = i[k], j[k]
+            r12 = np.linalg.norm(X[:, a] - X[:, b], axis=-1)
+            r1 = np.linalg.norm(X[:, a] - system.nuc[I], axis=-1)
+            r2 = np.linalg.norm(X[:, b] - system.nuc[I], axis=-1)
+            m = (r1 < L) & (r2 < L)
+            u = _eeI_poly_derivs(g, r12, r1, r2, L)[0]
+            J -= np.where(m, u, 0.0)
+    return J
+
+
+def j3_vgl(system, X):
+    """Per-electron gradient and Laplacian of J3_eeI (``J3_eeI_vgl``,
+    gto.py:2042-2196): each electron of a triplet takes the partials with
+    itself as particle 1 (u is symmetric in the two electrons)."""
+    W, n_e, _ = X.shape
+    grad = np.zeros((W, n_e, 3))
+    lap = np.zeros((W, n_e))
+    blocks = _j3_blocks(system)
+    if not blocks:
+        return grad, lap
+    L = 0.5 * system.j3["r_cut"]
+    for I, same, g in blocks:
+        for a in range(n_e):
+            for b in range(n_e):
+                if a == b or ((a % 2) == (b % 2)) != same:
+                    continue
+                d12 = X[:, a] - X[:, b]
+                d1 = X[:, a] - system.nuc[I]
+                r12 = np.linalg.norm(d12, axis=-1)
+                r1 = np.linalg.norm(d1, axis=-1)
+                r2 = np.linalg.norm(X[:, b] - system.nuc[I], axis=-1)
+                m = ((r1 < L) & (r2 < L)).astype(np.float64)
+                _, u1, u12, u11, u1212, u112 = _eeI_poly_derivs(g, r12, r1, r2, L)
+                e1 = d1 / r1[:, None]
+                e12 = d12 / r12[:, None]
+                cos = np.sum(e1 * e12, axis=-1)
+                grad[:, a] -= m[:, None] * (u1[:, None] * e1 + u12[:, None] * e12)
+                lap[:, a] -= m * (u11 + 2.0 * u1 / r1 + u1212 + 2.0 * u12 / r12
+                                  + 2.0 * u112 * cos)
+    return grad, lap
+
+
 def jastrow_value(system, X):
-    """J1 + J2 (``gto.py:1500-1573``, Padé; ``1684-1780``, B-spline)."""
+    """J1 + J2 (``gto.py:1500-1573``, Padé; ``1684-1780``, B-spline) + J3_eeI."""
     W, n_e, _ = X.shape
     J = np.zeros(W)
     if system.has_j2:
@@ -320,6 +507,7 @@ def jastrow_value(system, X):
             d = X - system.nuc[I][None, None, :]
             r = np.sqrt(np.sum(d * d, axis=-1))
             J += np.sum(bspline_vgl(c, r, rc)[0], axis=-1)
+    J += j3_value(system, X)
     return J
 
 
@@ -383,7 +571,8 @@ def jastrow_vgl(system, X):
             _, up, upp = bspline_vgl(c, r, rc)
             grad += (up / r)[..., None] * d
             lap += upp + 2.0 * up / r
-    return grad, lap
+    g3, l3 = j3_vgl(system, X)
+    return grad + g3, lap + l3
 
 
 # ---------------------------------------------------------------------------

@@ -130,6 +130,13 @@ def _to_json(obj):
     return obj
 
 
+def _j3_params(syms, npar, seed):
+    """Seeded J3_eeI free parameters (scale 0.05, as the reference's test
+    ``_eeI_params``, tests/test_gto_jastrow.py:374-381)."""
+    rng = np.random.default_rng(seed)
+    return {p + s: rng.normal(size=npar) * 0.05 for s in syms for p in ("like+", "unlike+")}
+
+
 def fg_test_system():
     """Small system whose basis has f and g shells (am 3, 4)."""
     basis = {
@@ -195,13 +202,35 @@ CASES = {
                                       "J1_bspline": {"Li": np.array([-0.3, -0.1, 0.05]),
                                                      "H": np.array([-0.1, 0.02])}},
                          1.0, 16),
+    # J3_eeI three-body terms: default orders and cutoff (3, 3, 5 bohr) on
+    # H2O with both spin blocks of both elements; orders 2, 2 and a 4-bohr
+    # cutoff with only some blocks, on cusp-corrected LiH with Padé J1/J2
+    "h2o_j3": (lambda: M.named_system("H2O"), False,
+               lambda mol: {"J2_pade": {"like": np.array([0.25, 1.0]),
+                                        "unlike": np.array([0.5, 1.0])},
+                            "J3_eeI": _j3_params(("O", "H"), 26, seed=13)},
+               0.7, 24),
+    "lih_j3": (lambda: M.named_system("LiH"), True,
+               lambda mol: {"J1_pade": {"Li": np.array([-0.3, 0.8]),
+                                        "H": np.array([-0.1, 0.6])},
+                            "J2_pade": {"like": np.array([0.25, 0.8]),
+                                        "unlike": np.array([0.5, 0.8])},
+                            "J3_eeI": {k: v for k, v in
+                                       _j3_params(("Li", "H"), 8, seed=17).items()
+                                       if k != "unlike+H"}},
+               1.0, 16),
 }
 
-# B-spline cutoffs per case (jastrow_config of _PsiGTO, gto.py:948-968)
+# B-spline cutoffs and J3 orders per case (jastrow_config of _PsiGTO,
+# gto.py:948-984)
 JASTROW_CONFIG = {
     "h2o_bspline": {"J2": {"r_cut": 4.0},
                     "J1": {"O": {"r_cut": 3.5}, "H": {"r_cut": 3.0}}},
+    "lih_j3": {"J3": {"N_eI": 2, "N_ee": 2, "r_cut": 4.0}},
 }
+
+# (N_eI, N_ee, r_cut) of the stored J3_eeI constraint maps
+EEI_MAPS = [(3, 3, 5.0), (2, 2, 4.0), (2, 3, 6.0), (4, 3, 5.0), (1, 2, 3.0)]
 
 
 def run_case(gto, name, seed):
@@ -249,6 +278,10 @@ def run_case(gto, name, seed):
                     g, L = fn(x, tp["J2_bspline"])
                     grad = grad + g.reshape(-1)
                     lap = lap + L
+            if "J3_eeI" in tp:
+                g, L = obj._J3_eeI_vgl(x, nuc, tp["J3_eeI"])
+                grad = grad + g.reshape(-1)
+                lap = lap + L
         out["logpsi"].append(float(lp))
         out["e_ke"].append(float(ke))
         out["e_ee"].append(float(obj.local_energy_ee(x)))
@@ -286,6 +319,15 @@ def main():
         res = run_case(gto, name, seed=k)
         np.savez_compressed(os.path.join(HERE, f"golden_{name}.npz"), **res)
         print(f"{name}: {len(res['logpsi'])} walkers, logpsi[0]={res['logpsi'][0]:.12f}")
+    if args.cases is None or "eeI_map" in args.cases:
+        maps = {}
+        for n_ei, n_ee, rc in EEI_MAPS:
+            A, ls, ms, ns = gto._build_eeI_constraint_map(n_ei, n_ee, rc)
+            key = f"{n_ei}_{n_ee}_{rc:g}"
+            maps["A_" + key] = np.asarray(A)
+            maps["lmn_" + key] = np.stack([np.asarray(ls), np.asarray(ms), np.asarray(ns)], 1)
+        np.savez_compressed(os.path.join(HERE, "golden_eeI_map.npz"), **maps)
+        print("eeI maps:", ", ".join(sorted(k for k in maps if k.startswith("A_"))))
     if args.cases is not None:
         return
     # binning analysis on a seeded AR(1) series
