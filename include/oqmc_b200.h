@@ -97,6 +97,17 @@ typedef struct {
   const int* bs1_ncoef;                    /* ntype */
   const double* bs1_rcut;                  /* ntype */
   const double* bs1_coef;                  /* ntype blocks of ncoef values */
+  /* Three-body electron-electron-nucleus polynomial Jastrow (J3_eeI,
+   * psi/gto.py:243-604, 1933-2196): per element type a like-spin and an
+   * unlike-spin block of gammas g[l][m][n] (already expanded from the free
+   * parameters, symmetric in l, m), zero beyond r_eI = j3_rcut / 2. */
+  int has_j3;
+  int j3_n_ei, j3_n_ee;                    /* orders: 0..6 and 1..6 */
+  int j3_ntype;                            /* element types, at most 4 */
+  double j3_rcut;
+  const int* j3_type;                      /* natm: type of each atom, -1 none */
+  const int* j3_on;                        /* ntype x 2: like / unlike block present */
+  const double* j3_gamma;                  /* ntype x 2 x (n_ei+1)^2 x (n_ee+1) */
 } oqmc_system_desc;
 
 /* Library version string. */
@@ -238,9 +249,13 @@ int oqmc_measure_peak(int kind, double* out_rate, void* stream);
  * jax.grad).  Raw parameters, oqmc_param_count(ctx) of them: J2 like a,
  * like b, unlike a, unlike b, then J1 a_I, b_I for every atom (Padé; absent
  * terms give zeros), then the B-spline parameters: J2 like, J2 unlike, then
- * J1 per element type (bs1_ncoef - 4 each, types in descriptor order).  grad = the (W, n_e, 3)
- * gradient of ln|psi| that oqmc_eval returns for the same walkers; outputs
- * dlogpsi, dEL are (W, count), FP64. */
+ * J1 per element type (bs1_ncoef - 4 each, types in descriptor order), then
+ * the three-body gammas: per J3 element type in descriptor order, the like
+ * and then the unlike block when present, (n_ei+1)(n_ei+2)/2 (n_ee+1) unique
+ * gammas g[l][m][n], l >= m, ordered by m, then l, then n (the caller maps
+ * them onto the free parameters with the constraint matrix).  grad = the
+ * (W, n_e, 3) gradient of ln|psi| that oqmc_eval returns for the same
+ * walkers; outputs dlogpsi, dEL are (W, count), FP64. */
 int oqmc_param_count(const oqmc_ctx* ctx);
 int oqmc_param_derivs(oqmc_ctx* ctx, const double* walkers, int W, const double* grad,
                       double* dlogpsi, double* dEL, void* stream);

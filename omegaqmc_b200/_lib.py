@@ -49,6 +49,8 @@ class SystemDesc(ctypes.Structure):
         ("bs2_rcut", c_double), ("bs2_coef_like", P_double), ("bs2_coef_unlike", P_double),
         ("has_bs1", c_int), ("bs1_ntype", c_int), ("bs1_type", P_int), ("bs1_ncoef", P_int),
         ("bs1_rcut", P_double), ("bs1_coef", P_double),
+        ("has_j3", c_int), ("j3_n_ei", c_int), ("j3_n_ee", c_int), ("j3_ntype", c_int),
+        ("j3_rcut", c_double), ("j3_type", P_int), ("j3_on", P_int), ("j3_gamma", P_double),
     ]
 
 

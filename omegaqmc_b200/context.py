@@ -110,6 +110,16 @@ def pack_system(system: System):
         types = tables
         d.has_bs1 = 1
         d.bs1_ntype = len(types)
+    j3 = getattr(system, "j3", None)
+    if j3 is not None:
+        arr["j3_type"] = np.array(j3["types"], dtype=np.int32)
+        arr["j3_on"] = np.ascontiguousarray(j3["on"], dtype=np.int32).ravel()
+        arr["j3_gamma"] = np.ascontiguousarray(j3["gamma"], dtype=np.float64).ravel()
+        d.has_j3 = 1
+        d.j3_n_ei = int(j3["n_eI"])
+        d.j3_n_ee = int(j3["n_ee"])
+        d.j3_ntype = len(j3["elements"])
+        d.j3_rcut = float(j3["r_cut"])
     for k, v in arr.items():
         ct = ctypes.c_int if v.dtype == np.int32 else ctypes.c_double
         setattr(d, k, v.ctypes.data_as(ctypes.POINTER(ct)))

@@ -224,8 +224,34 @@ static int fill_system(const oqmc_system_desc* d, OqSystem& S) {
       S.bs1_type[i] = t;
     }
   }
+  for (int i = 0; i < OQ_MAX_NUC; ++i) S.j3_type[i] = -1;
+  if (d->has_j3) {
+    if (d->j3_n_ei < 0 || d->j3_n_ei > 6 || d->j3_n_ee < 1 || d->j3_n_ee > 6 ||
+        d->j3_ntype < 1 || d->j3_ntype > OQ_MAX_BST || !(d->j3_rcut > 0.0) || !d->j3_type ||
+        !d->j3_on || !d->j3_gamma)
+      return set_err(nullptr, OQ_ERR_ARG, "bad three-body Jastrow table%s");
+    S.has_j3 = 1;
+    S.j3_nI = d->j3_n_ei;
+    S.j3_nE = d->j3_n_ee;
+    S.j3_L = 0.5 * d->j3_rcut;
+    S.j3_gamma = d->j3_gamma;     // host table; oqmc_create points it at a device copy
+    for (int t = 0; t < d->j3_ntype; ++t)
+      for (int b = 0; b < 2; ++b) S.j3_on[t][b] = d->j3_on[2 * t + b] ? 1 : 0;
+    for (int i = 0; i < d->natm; ++i) {
+      const int t = d->j3_type[i];
+      if (t < -1 || t >= d->j3_ntype)
+        return set_err(nullptr, OQ_ERR_ARG, "bad three-body Jastrow atom type%s");
+      S.j3_type[i] = t;
+    }
+  }
   build_harm_table(S.harm);
   return OQ_OK;
+}
+
+// Doubles in the three-body Jastrow table of a descriptor.
+static size_t j3_table_len(const oqmc_system_desc* d) {
+  if (!d->has_j3) return 0;
+  return (size_t)d->j3_ntype * 2 * (d->j3_n_ei + 1) * (d->j3_n_ei + 1) * (d->j3_n_ee + 1);
 }
 
 static_assert(sizeof(OqSystem) % 16 == 0, "OqSystem is copied in 16-byte chunks");
@@ -308,6 +334,13 @@ extern "C" int oqmc_create(oqmc_ctx** out, const oqmc_system_desc* d) {
   e = (e == cudaSuccess) ? cudaMalloc(&ctx->d_C64, sizeof(double) * c32.size()) : e;
   e = (e == cudaSuccess) ? cudaMalloc(&ctx->d_C32, sizeof(float) * c32.size()) : e;
   e = (e == cudaSuccess) ? cudaMalloc(&ctx->d_flags, sizeof(unsigned)) : e;
+  if (S.has_j3) {
+    const size_t n3 = j3_table_len(d);
+    e = (e == cudaSuccess) ? cudaMalloc(&ctx->d_j3, sizeof(double) * n3) : e;
+    e = (e == cudaSuccess) ? cudaMemcpy(ctx->d_j3, d->j3_gamma, sizeof(double) * n3,
+                                        cudaMemcpyHostToDevice) : e;
+    S.j3_gamma = ctx->d_j3;
+  }
   e = (e == cudaSuccess) ? cudaMemcpy(ctx->d_sys, &S, sizeof(OqSystem), cudaMemcpyHostToDevice) : e;
   e = (e == cudaSuccess) ? cudaMemcpy(ctx->d_split, &ctx->hsplit, sizeof(OqSplit), cudaMemcpyHostToDevice) : e;
   e = (e == cudaSuccess) ? cudaMemcpy(ctx->d_C64, d->C, sizeof(double) * c32.size(), cudaMemcpyHostToDevice) : e;
@@ -333,6 +366,7 @@ int oqmc_destroy(oqmc_ctx* ctx) {
   cudaFree(ctx->d_C64);
   cudaFree(ctx->d_C32);
   cudaFree(ctx->d_flags);
+  cudaFree(ctx->d_j3);
   delete ctx;
   return OQ_OK;
 }
@@ -469,11 +503,119 @@ __device__ void oq_param_derivs_bspline(const OqSystem& S, const double* x, cons
   }
 }
 
+// Unique gammas of one three-body block: (l, m, n) with l >= m, ordered
+// m, then l, then n (the constraint map's order).
+__host__ __device__ static inline int j3_unique(const OqSystem& S) {
+  return (S.j3_nI + 1) * (S.j3_nI + 2) / 2 * (S.j3_nE + 1);
+}
+
+__device__ __forceinline__ double oq_ipow(double x, int k) {
+  double v = 1.0;
+  for (int i = 0; i < k; ++i) v *= x;
+  return v;
+}
+
+// phi = r1^l r2^m r12^n (+ r1^m r2^l r12^n for l != m) and its partials
+// with electron 1 moving: phi, d/dr1, d/dr12, d2/dr1^2, d2/dr12^2, d2/dr1dr12.
+__device__ __forceinline__ void oq_j3_basis(int l, int m, int n, double r1, double r2, double r12,
+                                            double f[6]) {
+  for (int k = 0; k < 6; ++k) f[k] = 0.0;
+  const double e0 = oq_ipow(r12, n), e1 = n >= 1 ? n * oq_ipow(r12, n - 1) : 0.0,
+               e2 = n >= 2 ? n * (n - 1) * oq_ipow(r12, n - 2) : 0.0;
+  for (int pass = 0; pass < (l != m ? 2 : 1); ++pass) {
+    const int a = pass ? m : l, b = pass ? l : m;
+    const double p0 = oq_ipow(r1, a), p1 = a >= 1 ? a * oq_ipow(r1, a - 1) : 0.0,
+                 p2 = a >= 2 ? a * (a - 1) * oq_ipow(r1, a - 2) : 0.0, q = oq_ipow(r2, b);
+    f[0] += p0 * q * e0;
+    f[1] += p1 * q * e0;
+    f[2] += p0 * q * e1;
+    f[3] += p2 * q * e0;
+    f[4] += p0 * q * e2;
+    f[5] += p1 * q * e1;
+  }
+}
+
+// d log|psi| / d gamma and d E_L / d gamma of the three-body Jastrow for the
+// unique gammas of every present block (types in order, like then unlike),
+// starting at raw slot `base`.  J3 = -sum u is linear in the gammas, so each
+// gamma's derivative is the J3 value, gradient and Laplacian with that
+// gamma's monomial in place of the polynomial.
+__device__ void oq_param_derivs_j3(const OqSystem& S, const double* x, const double* g, int n_e,
+                                   int base, double* dl, double* de) {
+  const int NG = j3_unique(S);
+  const double L = S.j3_L;
+  int boff[OQ_MAX_BST][2];
+  for (int t = 0, o = base; t < OQ_MAX_BST; ++t)
+    for (int b = 0; b < 2; ++b) {
+      boff[t][b] = S.j3_on[t][b] ? o : -1;
+      if (S.j3_on[t][b]) o += NG;
+    }
+  for (int I = 0; I < S.natm; ++I) {
+    const int ty = S.j3_type[I];
+    if (ty < 0) continue;
+    for (int i = 0; i < n_e; ++i)
+      for (int j = i + 1; j < n_e; ++j) {
+        const int blk = (i ^ j) & 1;
+        const int off = boff[ty][blk];
+        if (off < 0) continue;
+        double di[3], dj[3], dij[3];
+        for (int c = 0; c < 3; ++c) {
+          di[c] = x[3 * i + c] - S.nuc[I][c];
+          dj[c] = x[3 * j + c] - S.nuc[I][c];
+          dij[c] = x[3 * i + c] - x[3 * j + c];
+        }
+        const double ri = sqrt(di[0] * di[0] + di[1] * di[1] + di[2] * di[2]);
+        const double rj = sqrt(dj[0] * dj[0] + dj[1] * dj[1] + dj[2] * dj[2]);
+        if (!(ri < L) || !(rj < L)) continue;
+        const double r12 = sqrt(dij[0] * dij[0] + dij[1] * dij[1] + dij[2] * dij[2]);
+        // G_a . e_aI and G_a . e_ab for the two electrons, and the cosines
+        double gi1 = 0, gie = 0, gj1 = 0, gje = 0, ci = 0, cj = 0;
+        for (int c = 0; c < 3; ++c) {
+          const double ei = di[c] / ri, ej = dj[c] / rj, e = dij[c] / r12;
+          gi1 += g[3 * i + c] * ei;
+          gie += g[3 * i + c] * e;
+          gj1 += g[3 * j + c] * ej;
+          gje -= g[3 * j + c] * e;
+          ci += ei * e;
+          cj -= ej * e;
+        }
+        // envelope (r_1I - L)^3 (r_2I - L)^3 in each electron's frame
+        const double si = ri - L, sj = rj - L;
+        const double E = si * si * si * sj * sj * sj;
+        const double Ei1 = 3.0 * si * si * sj * sj * sj, Ei11 = 6.0 * si * sj * sj * sj;
+        const double Ej1 = 3.0 * sj * sj * si * si * si, Ej11 = 6.0 * sj * si * si * si;
+        int u = 0;
+        for (int m = 0; m <= S.j3_nI; ++m)
+          for (int l = m; l <= S.j3_nI; ++l)
+            for (int n = 0; n <= S.j3_nE; ++n, ++u) {
+              double fi[6], fj[6];
+              oq_j3_basis(l, m, n, ri, rj, r12, fi);
+              oq_j3_basis(l, m, n, rj, ri, r12, fj);
+              // partials of f = phi * E with each electron as particle 1
+              const double a1 = fi[1] * E + fi[0] * Ei1, ae = fi[2] * E;
+              const double a11 = fi[3] * E + 2.0 * fi[1] * Ei1 + fi[0] * Ei11, aee = fi[4] * E;
+              const double a1e = fi[5] * E + fi[2] * Ei1;
+              const double b1 = fj[1] * E + fj[0] * Ej1, be = fj[2] * E;
+              const double b11 = fj[3] * E + 2.0 * fj[1] * Ej1 + fj[0] * Ej11, bee = fj[4] * E;
+              const double b1e = fj[5] * E + fj[2] * Ej1;
+              // J3 = -sum f: d lap and G . dG of both electrons
+              const double dlap_i = -(a11 + 2.0 * a1 / ri + aee + 2.0 * ae / r12 + 2.0 * a1e * ci);
+              const double dlap_j = -(b11 + 2.0 * b1 / rj + bee + 2.0 * be / r12 + 2.0 * b1e * cj);
+              const double gdg = -(a1 * gi1 + ae * gie) - (b1 * gj1 + be * gje);
+              dl[off + u] -= fi[0] * E;
+              de[off + u] -= 0.5 * (dlap_i + dlap_j + 2.0 * gdg);
+            }
+      }
+  }
+}
+
 static int param_count_of(const OqSystem& S) {
   int n = 4 + 2 * S.natm;
   if (S.has_bs2) n += S.bs2_n_like + S.bs2_n_unlike;
   if (S.has_bs1)
     for (int t = 0; t < OQ_MAX_BST; ++t) n += S.bs1_n[t];
+  if (S.has_j3)
+    for (int t = 0; t < OQ_MAX_BST; ++t) n += j3_unique(S) * (S.j3_on[t][0] + S.j3_on[t][1]);
   return n;
 }
 
@@ -487,6 +629,9 @@ __global__ void k_param_derivs(const OqSystem* __restrict__ gsys, const double* 
   if (S.has_bs2) n_raw += S.bs2_n_like + S.bs2_n_unlike;
   if (S.has_bs1)
     for (int t = 0; t < OQ_MAX_BST; ++t) n_raw += S.bs1_n[t];
+  const int j3_base = n_raw;
+  if (S.has_j3)
+    for (int t = 0; t < OQ_MAX_BST; ++t) n_raw += j3_unique(S) * (S.j3_on[t][0] + S.j3_on[t][1]);
   const double* x = X + (size_t)w * n_e * 3;
   const double* g = G + (size_t)w * n_e * 3;
   double* dl = dlog + (size_t)w * n_raw;
@@ -512,6 +657,7 @@ __global__ void k_param_derivs(const OqSystem* __restrict__ gsys, const double* 
     for (int k = 0; k < 4; ++k) { dl[k] = al[k]; de[k] = ae[k]; }
   }
   if (S.has_bs2 || S.has_bs1) oq_param_derivs_bspline(S, x, g, n_e, dl, de);
+  if (S.has_j3) oq_param_derivs_j3(S, x, g, n_e, j3_base, dl, de);
   if (S.has_j1) {
     for (int I = 0; I < S.natm; ++I) {
       double sl0 = 0, sl1 = 0, se0 = 0, se1 = 0;
@@ -561,7 +707,7 @@ static uint16_t host_bf16(float f) {
 }
 
 int oqmc_use_tensor_cores(oqmc_ctx* ctx, int enable) {
-  if (ctx && enable && (ctx->hsys.has_bs1 || ctx->hsys.has_bs2))
+  if (ctx && enable && (ctx->hsys.has_bs1 || ctx->hsys.has_bs2 || ctx->hsys.has_j3))
     return set_err(ctx, OQ_ERR_UNSUPPORTED,
                    "the tensor-core local energy supports Pade Jastrow terms only%s");
   if (!ctx) return OQ_ERR_ARG;

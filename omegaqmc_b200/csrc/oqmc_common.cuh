@@ -66,6 +66,13 @@ struct OqSystem {
   int bs1_n[OQ_MAX_BST];
   double bs1_rcut[OQ_MAX_BST], bs1_dinv[OQ_MAX_BST];
   double bs1_c[OQ_MAX_BST][OQ_MAX_BSC];
+  // three-body electron-electron-nucleus polynomial Jastrow: gamma blocks
+  // [type][like 0 / unlike 1][nI + 1][nI + 1][nE + 1] in device memory
+  int has_j3, j3_nI, j3_nE, j3_pad;
+  double j3_L;                       // half cutoff: u = 0 unless r_1I, r_2I < L
+  const double* j3_gamma;
+  int j3_type[OQ_MAX_NUC];           // element type of each atom, -1: none
+  int j3_on[OQ_MAX_BST][2];          // block present
   OqHarmTable harm;
 };
 
@@ -221,6 +228,144 @@ __device__ __forceinline__ void oq_bs_vgl(const double* c, int n, T dinv, T rcut
                 (-(T)18 * t + (T)6) * c2 + (T)6 * t * c3);
   up_r = d1 * rinv;
   lap = d2 + (T)2 * up_r;
+}
+
+// ---------------------------------------------------------------------------
+// Three-body electron-electron-nucleus Jastrow (J3_eeI, psi/gto.py:474-604,
+// 1933-2196; QMCPACK PolynomialFunctor3D).  For electrons 1, 2 and nucleus I
+// with r_1I, r_2I < L = r_cut / 2,
+//   u = (r_1I - L)^3 (r_2I - L)^3 sum_lmn g[l][m][n] r_1I^l r_2I^m r_12^n,
+// and J3 = -(sum over nuclei and electron pairs of u).  g is the block of
+// the nucleus's element and the pair's spins, symmetric in (l, m), so u is
+// symmetric in the two electrons.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T oq_j3_u(const double* __restrict__ g, int nI, int nE, T L, T r12,
+                                     T r1, T r2) {
+  T P = (T)0;
+  for (int l = nI; l >= 0; --l) {
+    T a = (T)0;
+    for (int m = nI; m >= 0; --m) {
+      const double* gp = g + (l * (nI + 1) + m) * (nE + 1);
+      T q = (T)0;
+      for (int n = nE; n >= 0; --n) q = q * r12 + (T)gp[n];
+      a = a * r2 + q;
+    }
+    P = P * r1 + a;
+  }
+  const T e = (r1 - L) * (r2 - L);
+  return P * e * e * e;
+}
+
+// Partials of u with electron 1 as the moving particle (_eval_eeI_poly_vgl,
+// gto.py:508-604): u1 = du/dr_1I, ue = du/dr_12, u11, uee and the mixed u1e.
+// Horner in r_12, r_2I, r_1I carrying first and second derivatives.
+template <typename T>
+__device__ __forceinline__ void oq_j3_partials(const double* __restrict__ g, int nI, int nE, T L,
+                                               T r12, T r1, T r2, T& u1, T& ue, T& u11, T& uee,
+                                               T& u1e) {
+  T P = (T)0, P1 = (T)0, P11 = (T)0, Q = (T)0, Q1 = (T)0, R = (T)0;
+  for (int l = nI; l >= 0; --l) {
+    T a = (T)0, b = (T)0, c = (T)0;
+    for (int m = nI; m >= 0; --m) {
+      const double* gp = g + (l * (nI + 1) + m) * (nE + 1);
+      T q = (T)0, qd = (T)0, qdd = (T)0;
+      for (int n = nE; n >= 0; --n) {
+        qdd = qdd * r12 + (T)2 * qd;
+        qd = qd * r12 + q;
+        q = q * r12 + (T)gp[n];
+      }
+      a = a * r2 + q;
+      b = b * r2 + qd;
+      c = c * r2 + qdd;
+    }
+    P11 = P11 * r1 + (T)2 * P1;
+    P1 = P1 * r1 + P;
+    P = P * r1 + a;
+    Q1 = Q1 * r1 + Q;
+    Q = Q * r1 + b;
+    R = R * r1 + c;
+  }
+  const T s1 = r1 - L, s2 = r2 - L, s1s = s1 * s1, s2c = s2 * s2 * s2;
+  const T E = s1s * s1 * s2c, E1 = (T)3 * s1s * s2c, E11 = (T)6 * s1 * s2c;
+  u1 = P1 * E + P * E1;
+  ue = Q * E;
+  u11 = P11 * E + (T)2 * P1 * E1 + P * E11;
+  uee = R * E;
+  u1e = Q1 * E + Q * E1;
+}
+
+// Sum of u over the triplets of electron e at (x, y, z) with the electrons
+// j >= j0, j != e, whose coordinate c is pos[(3 j + c) * ps].
+template <typename T>
+__device__ __forceinline__ T oq_j3_electron(const OqSystem& S, const double* pos, size_t ps,
+                                            int ne, int e, int j0, double x, double y, double z) {
+  const int nI = S.j3_nI, nE = S.j3_nE, bsz = (nI + 1) * (nI + 1) * (nE + 1);
+  const T L = (T)S.j3_L;
+  T acc = (T)0;
+  for (int I = 0; I < S.natm; ++I) {
+    const int ty = S.j3_type[I];
+    if (ty < 0) continue;
+    const double ax = x - S.nuc[I][0], ay = y - S.nuc[I][1], az = z - S.nuc[I][2];
+    const T r1 = sqrt((T)(ax * ax + ay * ay + az * az));
+    if (!(r1 < L)) continue;
+    for (int j = j0; j < ne; ++j) {
+      if (j == e) continue;
+      const int blk = (e ^ j) & 1;
+      if (!S.j3_on[ty][blk]) continue;
+      const double xj = pos[(size_t)(3 * j) * ps], yj = pos[(size_t)(3 * j + 1) * ps],
+                   zj = pos[(size_t)(3 * j + 2) * ps];
+      const double bx = xj - S.nuc[I][0], by = yj - S.nuc[I][1], bz = zj - S.nuc[I][2];
+      const T r2 = sqrt((T)(bx * bx + by * by + bz * bz));
+      if (!(r2 < L)) continue;
+      const double dx = x - xj, dy = y - yj, dz = z - zj;
+      const T r12 = sqrt((T)(dx * dx + dy * dy + dz * dz));
+      acc += oq_j3_u<T>(S.j3_gamma + (size_t)(2 * ty + blk) * bsz, nI, nE, L, r12, r1, r2);
+    }
+  }
+  return acc;
+}
+
+// Gradient and Laplacian of J3 with respect to electron e at (x, y, z),
+// subtracted from (gx, gy, gz, lp) (J3 = -sum u; J3_eeI_vgl,
+// gto.py:2042-2196).
+template <typename T>
+__device__ __forceinline__ void oq_j3_vgl_electron(const OqSystem& S, const double* pos, size_t ps,
+                                                   int ne, int e, double x, double y, double z,
+                                                   T& gx, T& gy, T& gz, T& lp) {
+  const int nI = S.j3_nI, nE = S.j3_nE, bsz = (nI + 1) * (nI + 1) * (nE + 1);
+  const T L = (T)S.j3_L;
+  for (int I = 0; I < S.natm; ++I) {
+    const int ty = S.j3_type[I];
+    if (ty < 0) continue;
+    const T ax = (T)(x - S.nuc[I][0]), ay = (T)(y - S.nuc[I][1]), az = (T)(z - S.nuc[I][2]);
+    const T r1 = sqrt(ax * ax + ay * ay + az * az);
+    if (!(r1 < L)) continue;
+    const T i1 = (T)1 / r1;
+    const T e1x = ax * i1, e1y = ay * i1, e1z = az * i1;
+    for (int j = 0; j < ne; ++j) {
+      if (j == e) continue;
+      const int blk = (e ^ j) & 1;
+      if (!S.j3_on[ty][blk]) continue;
+      const double xj = pos[(size_t)(3 * j) * ps], yj = pos[(size_t)(3 * j + 1) * ps],
+                   zj = pos[(size_t)(3 * j + 2) * ps];
+      const T bx = (T)(xj - S.nuc[I][0]), by = (T)(yj - S.nuc[I][1]), bz = (T)(zj - S.nuc[I][2]);
+      const T r2 = sqrt(bx * bx + by * by + bz * bz);
+      if (!(r2 < L)) continue;
+      const T dx = (T)(x - xj), dy = (T)(y - yj), dz = (T)(z - zj);
+      const T r12 = sqrt(dx * dx + dy * dy + dz * dz);
+      const T i12 = (T)1 / r12;
+      const T ex = dx * i12, ey = dy * i12, ez = dz * i12;
+      T u1, ue, u11, uee, u1e;
+      oq_j3_partials<T>(S.j3_gamma + (size_t)(2 * ty + blk) * bsz, nI, nE, L, r12, r1, r2, u1, ue,
+                        u11, uee, u1e);
+      gx -= u1 * e1x + ue * ex;
+      gy -= u1 * e1y + ue * ey;
+      gz -= u1 * e1z + ue * ez;
+      lp -= u11 + (T)2 * u1 * i1 + uee + (T)2 * ue * i12 +
+            (T)2 * u1e * (e1x * ex + e1y * ey + e1z * ez);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -15,6 +15,7 @@ struct oqmc_ctx {
   double* d_C64;
   float* d_C32;
   unsigned* d_flags;
+  double* d_j3;            // three-body Jastrow gamma blocks (or null)
   double tight_alpha;
   int proposal;           // 0 fixed-width Gaussian, 1 nucleus-scaled width
   OqSpecModule* spec;     // run-time specialised kernels, or null

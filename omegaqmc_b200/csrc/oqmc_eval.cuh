@@ -49,7 +49,8 @@ __device__ bool oq_invert(double (&a)[N][N], double (&inv)[N][N], double& logdet
   return true;
 }
 
-// Jastrow value J1 + J2 for walker positions x[n_e][3] (in registers/local).
+// Jastrow value J1 + J2 (+ J3) for walker positions x[n_e][3] (in
+// registers/local).
 __device__ __forceinline__ double oq_jastrow_value(const OqSystem& S, const double* x,
                                                    int n_e) {
   double J = 0.0;
@@ -93,6 +94,10 @@ __device__ __forceinline__ double oq_jastrow_value(const OqSystem& S, const doub
         J += oq_bs_val<double>(S.bs1_c[ty], S.bs1_n[ty], S.bs1_dinv[ty], S.bs1_rcut[ty],
                                sqrt(dx * dx + dy * dy + dz * dz));
       }
+  }
+  if (S.has_j3) {
+    for (int i = 0; i < n_e; ++i)
+      J -= oq_j3_electron<double>(S, x, 1, n_e, i, i + 1, x[3 * i], x[3 * i + 1], x[3 * i + 2]);
   }
   return J;
 }
@@ -197,6 +202,9 @@ k_eval(const OqSystem* __restrict__ gsys, const double* __restrict__ gC,
         gx += upr * dx; gy += upr * dy; gz += upr * dz; lp += l;
       }
     }
+    if (S.has_j3)
+      oq_j3_vgl_electron<double>(S, x, 1, NE, e, x[3 * e], x[3 * e + 1], x[3 * e + 2], gx, gy, gz,
+                                 lp);
     if (grad) {
       double* gp = grad + (size_t)w * 3 * NE + 3 * e;
       gp[0] = gx; gp[1] = gy; gp[2] = gz;

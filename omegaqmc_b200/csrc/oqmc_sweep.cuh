@@ -366,6 +366,9 @@ __device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, cons
             oq_bs_val<T>(S.bs1_c[ty], S.bs1_n[ty], dinv, rc, ro2t * oq_rsqrt(ro2t));
     }
   }
+  if (S.has_j3)
+    dJ -= oq_j3_electron<T>(S, pos + tid, WPB, NE, e, 0, nx, ny, nz) -
+          oq_j3_electron<T>(S, pos + tid, WPB, NE, e, 0, ox, oy, oz);
   // new MO row and the ratio vector w_j = sum_m v_m A[m][j]; R = w_i
   T v[NOCC];
   B::template mo_val<T, Real>(S, SP, C, nx, ny, nz, v);
@@ -601,6 +604,7 @@ __device__ __forceinline__ void oq_eloc_electron(const SJ& J, const OqSystem& S,
       jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
     }
   }
+  if (S.has_j3) oq_j3_vgl_electron<T>(S, pos, ps, NE, e, xe, ye, ze, jx, jy, jz, jl);
   const double sgx = (double)gx, sgy = (double)gy, sgz = (double)gz;
   const double Gx = sgx + (double)jx, Gy = sgy + (double)jy, Gz = sgz + (double)jz;
   lp_tot += (double)lp - (sgx * sgx + sgy * sgy + sgz * sgz) + (double)jl;

@@ -23,6 +23,7 @@ import numpy as np
 import torch
 
 from .context import GTOContext, _dptr, _stream_ptr
+from .system import eeI_constraint_map
 
 __all__ = ["flatten_params", "raw_to_flat", "walker_derivatives", "build_matrices"]
 
@@ -43,9 +44,11 @@ def flatten_params(params_corr):
 def raw_to_flat(raw, params_corr, system):
     """Map per-walker derivatives of the library's raw parameters (J2 like a,
     like b, unlike a, unlike b, then J1 a_I, b_I per atom; then the B-spline
-    parameters: J2 like, J2 unlike, J1 per element in order of first atom)
+    parameters: J2 like, J2 unlike, J1 per element in order of first atom;
+    then the J3_eeI unique gammas per element type, like then unlike block)
     onto the flat parameter order; Padé J1 entries collect the atoms of
-    their element."""
+    their element, and J3 blocks go through the constraint matrix
+    (d/dp = A^T d/dgamma, gamma_unique = A p)."""
     raw = np.asarray(raw)
     atom_symbols, cusp = list(system.symbols), system.cusp
     _, layout = flatten_params(params_corr)
@@ -64,8 +67,23 @@ def raw_to_flat(raw, params_corr, system):
             seen.append(atom_symbols[ia])
             bs_off[("J1_bspline", atom_symbols[ia])] = b
             b += len(e[0]) - 4
+    j3 = getattr(system, "j3", None)
+    j3_off, A3 = {}, None
+    if j3 is not None:
+        A3, lmn = eeI_constraint_map(j3["n_eI"], j3["n_ee"], j3["r_cut"])
+        for t, sym in enumerate(j3["elements"]):
+            for blk, prefix in enumerate(("like+", "unlike+")):
+                if j3["on"][t][blk]:
+                    j3_off[prefix + sym] = b
+                    b += len(lmn)
     o = 0
     for term, key, n in layout:
+        if term == "J3_eeI":
+            if key in j3_off:
+                ng = A3.shape[0]
+                out[:, o:o + n] = raw[:, j3_off[key]:j3_off[key] + ng] @ A3
+            o += n
+            continue
         if term.endswith("_bspline"):
             if (term, key) in bs_off:
                 out[:, o:o + n] = raw[:, bs_off[(term, key)]:bs_off[(term, key)] + n]
@@ -96,6 +114,7 @@ def walker_derivatives(ctx: GTOContext, X, params_corr, stream=None):
     W = X.shape[0]
     ev = ctx.evaluate(X, want_grad=True, want_lap=False, stream=stream)
     n_raw = int(ctx.lib.oqmc_param_count(ctx._h))
+    ctx._check(min(n_raw, 0))
     dl = torch.empty(W, n_raw, dtype=torch.float64, device=ctx.device)
     de = torch.empty(W, n_raw, dtype=torch.float64, device=ctx.device)
     ctx._check(ctx.lib.oqmc_param_derivs(ctx._h, _dptr(X), W, _dptr(ev["grad"]), _dptr(dl),

@@ -414,37 +414,41 @@ def _eeI_poly_derivs(g, r12, r1, r2, L):
             P112 * E + P12 * E1)
 
 
-def j3_value(system, X):
+def j3_value(system, X, blocks=None):
     """J3_eeI = -sum over nuclei I and pairs i<j of the block's u, for
-    r_iI, r_jI < L (``J3_eeI_fn``, gto.py:1951-2040)."""
+    r_iI, r_jI < L (``J3_eeI_fn``, gto.py:1951-2040).  ``blocks`` replaces
+    the system's (atom, same-spin, gamma) blocks when given."""
     W, n_e, _ = X.shape
     J = np.zeros(W)
-    blocks = _j3_blocks(system)
+    blocks = _j3_blocks(system) if blocks is None else blocks
     if not blocks:
         return J
     L = 0.5 * system.j3["r_cut"]
     i, j = _pairs(n_e)
     for I, same, g in blocks:
         sel = ((i % 2) == (j % 2)) == same
-        for k in np.flatnonzero(sel):
-            a, b = i[k], j[k]
-            r12 = np.linalg.norm(X[:, a] - X[:, b], axis=-1)
-            r1 = np.linalg.norm(X[:, a] - system.nuc[I], axis=-1)
-            r2 = np.linalg.norm(X[:, b] - system.nuc[I], axis=-1)
-            m = (r1 < L) & (r2 < L)
-            u = _eeI_poly_derivs(g, r12, r1, r2, L)[0]
-            J -= np.where(m, u, 0.0)
+        a, b = i[sel], j[sel]
+        r12 = np.linalg.norm(X[:, a] - X[:, b], axis=-1)          # (W, pairs)
+        r1 = np.linalg.norm(X[:, a] - system.nuc[I], axis=-1)
+        r2 = np.linalg.norm(X[:, b] - system.nuc[I], axis=-1)
+        # power tables and the einsum of _eval_eeI_poly (gto.py:474-488)
+        p1 = np.stack([r1 ** k for k in range(g.shape[0])], axis=-1)
+        p2 = np.stack([r2 ** k for k in range(g.shape[0])], axis=-1)
+        p12 = np.stack([r12 ** k for k in range(g.shape[2])], axis=-1)
+        P = np.einsum("lmn,wpl,wpm,wpn->wp", g, p1, p2, p12)
+        u = P * ((r1 - L) * (r2 - L)) ** 3
+        J -= np.sum(np.where((r1 < L) & (r2 < L), u, 0.0), axis=-1)
     return J
 
 
-def j3_vgl(system, X):
+def j3_vgl(system, X, blocks=None):
     """Per-electron gradient and Laplacian of J3_eeI (``J3_eeI_vgl``,
     gto.py:2042-2196): each electron of a triplet takes the partials with
     itself as particle 1 (u is symmetric in the two electrons)."""
     W, n_e, _ = X.shape
     grad = np.zeros((W, n_e, 3))
     lap = np.zeros((W, n_e))
-    blocks = _j3_blocks(system)
+    blocks = _j3_blocks(system) if blocks is None else blocks
     if not blocks:
         return grad, lap
     L = 0.5 * system.j3["r_cut"]
@@ -710,7 +714,8 @@ def _scatter_bspline(dl, de, base, n, i, w, w1, w2, m, r, gd, half):
 
 def param_count(system):
     """Raw parameters: Padé (4 + 2 natm), then the J2 B-spline like and
-    unlike parameters, then the J1 B-spline parameters per element type."""
+    unlike parameters, then the J1 B-spline parameters per element type,
+    then the J3_eeI unique gammas per element type (like, unlike)."""
     n = 4 + 2 * system.natm
     bs2 = getattr(system, "bs2", None)
     if bs2 is not None:
@@ -718,7 +723,30 @@ def param_count(system):
     for sym in bspline_types(system):
         ia = system.symbols.index(sym)
         n += len(system.bs1[ia][0]) - 4
+    n += sum(len(lmn) for _, _, lmn in _j3_raw_blocks(system))
     return n
+
+
+def _j3_raw_blocks(system):
+    """(element, same-spin flag, unique (l, m, n) list) of the J3 raw
+    parameter blocks: element types in order of first atom, like then
+    unlike, present blocks only."""
+    j3 = getattr(system, "j3", None)
+    if j3 is None:
+        return []
+    syms = list(system.symbols)
+    elements = []
+    for sym in syms:
+        if sym not in elements and ("like+" + sym in j3["params"]
+                                    or "unlike+" + sym in j3["params"]):
+            elements.append(sym)
+    _, lmn = eeI_constraint_map(j3["n_eI"], j3["n_ee"], j3["r_cut"])
+    out = []
+    for sym in elements:
+        for prefix, same in (("like+", True), ("unlike+", False)):
+            if prefix + sym in j3["params"]:
+                out.append((sym, same, lmn))
+    return out
 
 
 def param_derivatives(system, X, grad=None):
@@ -783,4 +811,17 @@ def param_derivatives(system, X, grad=None):
             ii, w, w1, w2, m, n = _bspline_param_terms(c, r, rc)
             _scatter_bspline(dl, de, base, n, ii, w, w1, w2, m, r, gd, True)
         base += len(system.bs1[system.symbols.index(sym)][0]) - 4
+    # J3 is linear in the gammas: the derivative by one unique gamma is the
+    # J3 value / VGL with that gamma (and its (m, l, n) mirror) set to 1
+    j3 = getattr(system, "j3", None)
+    for sym, same, lmn in _j3_raw_blocks(system):
+        atoms = [I for I in range(system.natm) if system.symbols[I] == sym]
+        for (l, m, n) in lmn:
+            g = np.zeros((j3["n_eI"] + 1, j3["n_eI"] + 1, j3["n_ee"] + 1))
+            g[l, m, n] = g[m, l, n] = 1.0
+            blocks = [(I, same, g) for I in atoms]
+            dl[:, base] = j3_value(system, X, blocks)
+            dg, dlap = j3_vgl(system, X, blocks)
+            de[:, base] = -0.5 * np.sum(dlap + 2.0 * np.sum(grad * dg, axis=-1), axis=-1)
+            base += 1
     return dl, de

@@ -39,7 +39,8 @@ def test_validation_errors_and_warnings():
         build_system(mf, {"J2_pade": {"like": [0.25, 1.0], "unlike": [0.5, 1.0]},
                           "J2_bspline": {"like": [0.1, 0.2], "unlike": [0.3, 0.1]}})
     with pytest.raises(NotImplementedError):
-        build_system(mf, {"J3_eeI": {}})
+        build_system(mf, {"J4_unknown": {}})
+    assert build_system(mf, {"J3_eeI": {}}).j3 is None
     # an element without a configured cutoff has no one-body spline
     s = build_system(mf, {"J1_bspline": {"O": [0.1, 0.2], "H": [0.3, 0.4]}}, None,
                      {"J1": {"O": {"r_cut": 3.0}}})

@@ -12,27 +12,39 @@ from omegaqmc_b200.system import build_system
 
 pytestmark = pytest.mark.gpu
 
-CASES = [("LiH", True, False), ("H2O", False, False), ("N2", False, False), ("H2O", False, True),
-         ("LiH", True, True)]
+CASES = [("LiH", True, None), ("H2O", False, None), ("N2", False, None), ("H2O", False, "bspline"),
+         ("LiH", True, "bspline"), ("H2O", False, "j3"), ("LiH", True, "j3")]
 
 
-def _params(mol, cusp, bspline):
+def _params(mol, cusp, extra):
     pc = M.default_params_corr(mol, cusp=cusp, j1=True)
-    if bspline:
+    if extra == "bspline":
         pc["J2_bspline"] = {"like": np.array([0.2, 0.1, 0.05, 0.02]),
                             "unlike": np.array([0.4, 0.25, 0.1, 0.05, 0.02])}
         pc["J1_bspline"] = {s: np.array([-0.1, 0.05, 0.02]) for s in set(mol.elements)}
+    if extra == "j3":
+        rng = np.random.default_rng(6)
+        els = sorted(set(mol.elements))
+        pc["J3_eeI"] = {p + e: rng.normal(size=8) * 0.02 for e in els for p in ("like+", "unlike+")
+                        if p + e != "like+" + els[0]}
     return pc
 
 
+def _config(mol, extra):
+    if extra == "bspline":
+        return {"J2": {"r_cut": 3.5}, "J1": {e: {"r_cut": 3.0} for e in set(mol.elements)}}
+    if extra == "j3":
+        return {"J3": {"N_eI": 2, "N_ee": 2, "r_cut": 4.5}}
+    return None
+
+
 @pytest.mark.filterwarnings("ignore::UserWarning")
-@pytest.mark.parametrize("name,cusp,bspline", CASES)
-def test_param_derivatives_match_oracle(name, cusp, bspline):
+@pytest.mark.parametrize("name,cusp,extra", CASES)
+def test_param_derivatives_match_oracle(name, cusp, extra):
     mf = M.make_mf(name)
-    pc = _params(mf.mol, cusp, bspline)
+    pc = _params(mf.mol, cusp, extra)
     pcu = M.synthetic_cusp_params(mf.mol) if cusp else None
-    cfg = ({"J2": {"r_cut": 3.5}, "J1": {e: {"r_cut": 3.0} for e in set(mf.mol.elements)}}
-           if bspline else None)
+    cfg = _config(mf.mol, extra)
     s = build_system(mf, pc, pcu, cfg)
     ctx = GTOContext(s)
     X = seeded_walkers(s, 257, 0.9, 11)          # ragged: 3 CTAs of 128

@@ -73,3 +73,38 @@ def test_bspline_param_derivatives_match_finite_differences():
             np.testing.assert_allclose(dl[:, col], fd_l, rtol=1e-6, atol=1e-7)
             np.testing.assert_allclose(de[:, col], fd_e, rtol=1e-5, atol=2e-5 * (1 + np.abs(fd_e).max()))
             col += 1
+
+
+def test_j3_param_derivatives_match_finite_differences():
+    """J3_eeI: the oracle's unique-gamma derivatives, mapped onto the free
+    parameters through the constraint matrix (optim.raw_to_flat), against
+    central differences in each free parameter."""
+    from omegaqmc_b200.optim import flatten_params, raw_to_flat
+    mf = M.make_mf("LiH")
+    rng = np.random.default_rng(4)
+    pc = {"J2_pade": {"like": np.array([0.25, 1.0]), "unlike": np.array([0.5, 1.0])},
+          "J3_eeI": {"like+Li": rng.normal(size=8) * 0.02, "unlike+Li": rng.normal(size=8) * 0.02,
+                     "unlike+H": rng.normal(size=8) * 0.02}}
+    cfg = {"J3": {"N_eI": 2, "N_ee": 2, "r_cut": 5.0}}
+    s = build_system(mf, pc, None, cfg)
+    X = seeded_walkers(s, 4, 0.9, 5)
+    dl, de = O.param_derivatives(s, X)
+    assert dl.shape[1] == O.param_count(s) == 4 + 2 * s.natm + 3 * 18
+    fl, fe = raw_to_flat(dl, pc, s), raw_to_flat(de, pc, s)
+    _, layout = flatten_params(pc)
+    col = 0
+    for term, key, n in layout:
+        if term != "J3_eeI":
+            col += n
+            continue
+        for q in range(n):
+            pp, pm = copy.deepcopy(pc), copy.deepcopy(pc)
+            h = 1e-6
+            pp[term][key][q] += h
+            pm[term][key][q] -= h
+            sp, sm = build_system(mf, pp, None, cfg), build_system(mf, pm, None, cfg)
+            fd_l = (O.log_psi(sp, X) - O.log_psi(sm, X)) / (2 * h)
+            fd_e = (O.evaluate(sp, X)["e_loc"] - O.evaluate(sm, X)["e_loc"]) / (2 * h)
+            np.testing.assert_allclose(fl[:, col], fd_l, rtol=1e-6, atol=1e-7)
+            np.testing.assert_allclose(fe[:, col], fd_e, rtol=1e-5, atol=2e-5 * (1 + np.abs(fd_e).max()))
+            col += 1
