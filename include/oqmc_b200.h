@@ -206,6 +206,24 @@ int oqmc_sweeps_noalloc(oqmc_ctx* ctx, double* walkers, int W, int precision,
  * exact proposal-density ratio, so the stationary distribution is unchanged
  * while core electrons move with core-sized steps. */
 int oqmc_set_proposal(oqmc_ctx* ctx, int kind, double r0, double fmin_frac);
+/* Multi-determinant trial (the `trial` dict of get_psi_fun /
+ * get_vmc_gto_func, OmegaQMC/psi/gto.py:846-863, 1312-1488):
+ *   psi_S = sum_d coef[d] det(Phi_up[:, occ_up[d]]) det(Phi_dn[:, occ_dn[d]])
+ * with Phi the orbitals of the ncol columns of C (nbf x ncol, row-major;
+ * for UHF trials the alpha and beta columns side by side, occ_dn indexing
+ * the beta half).  occ_up, occ_dn: ndet x nocc column indices in
+ * determinant order.  At most 16 distinct columns and 64 distinct
+ * determinants per spin.  Evaluation (oqmc_eval, oqmc_log_psi) and
+ * sampling (oqmc_refresh, oqmc_sweeps, oqmc_basin) then use the expansion,
+ * in FP64 only (oqmc_sweeps_noalloc included); the batched, learned-proposal
+ * and tensor-core paths refuse it.  ndet = 0 returns to the single determinant
+ * of the descriptor.  Sampler state sizes (oqmc_state_bytes) change with the
+ * expansion. */
+int oqmc_set_multidet(oqmc_ctx* ctx, int ndet, int ncol, const double* C, const double* coef,
+                      const int* occ_up, const int* occ_dn);
+/* Terms, distinct up / down determinants and padded orbital columns of the
+ * context's expansion (all 0 for a single determinant). */
+int oqmc_multidet_info(const oqmc_ctx* ctx, int* ndet, int* nu_up, int* nu_dn, int* ncol);
 
 /* Mixed-precision local energy with the MO contraction (the GEMM
  * AO(5 components) x C of get_psi_mo_vgl, OmegaQMC/psi/gto.py:1188-1214) on

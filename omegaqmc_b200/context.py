@@ -143,6 +143,8 @@ class GTOContext:
             code = self.lib.oqmc_create(ctypes.byref(h), ctypes.byref(desc))
         L.check(code, None)
         self._h = h
+        if getattr(system, "md", None) is not None:
+            self.set_multidet(system.md)
 
     # -- lifetime --------------------------------------------------------
     def close(self):
@@ -246,6 +248,31 @@ class GTOContext:
     def use_tensor_cores(self, enable=True):
         """Mixed-precision local energy with the MO contraction on tcgen05."""
         self._check(self.lib.oqmc_use_tensor_cores(self._h, int(enable)))
+
+    def set_multidet(self, md):
+        """Use a multi-determinant Slater part (``md`` from
+        :func:`~omegaqmc_b200.system.parse_trial`, or None for the single
+        determinant).  Evaluation and FP64 sampling follow the expansion."""
+        if md is None:
+            self._check(self.lib.oqmc_set_multidet(self._h, 0, 0, None, None, None, None))
+            self._md_keep = None
+            return
+        C = np.ascontiguousarray(md["C"], dtype=np.float64)
+        ci = np.ascontiguousarray(md["ci"], dtype=np.float64)
+        up = np.ascontiguousarray(md["occ_up"], dtype=np.int32)
+        dn = np.ascontiguousarray(md["occ_dn"], dtype=np.int32)
+        pd, pi = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+        self._md_keep = (C, ci, up, dn)
+        self._check(self.lib.oqmc_set_multidet(
+            self._h, ci.shape[0], C.shape[1], C.ctypes.data_as(pd), ci.ctypes.data_as(pd),
+            up.ctypes.data_as(pi), dn.ctypes.data_as(pi)))
+
+    def multidet_info(self):
+        """(terms, distinct up determinants, distinct down determinants,
+        padded orbital columns); zeros for a single determinant."""
+        v = [ctypes.c_int() for _ in range(4)]
+        self._check(self.lib.oqmc_multidet_info(self._h, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
 
     def set_proposal(self, kind, r0=1.0, fmin_frac=0.05):
         """0: fixed-width Gaussian (reference); 1: nucleus-scaled width."""

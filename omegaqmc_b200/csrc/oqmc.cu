@@ -5,6 +5,7 @@
 #include <cstring>
 #include <cmath>
 #include <string>
+#include <map>
 #include <vector>
 #include <cuda_runtime.h>
 
@@ -248,6 +249,19 @@ static int fill_system(const oqmc_system_desc* d, OqSystem& S) {
   return OQ_OK;
 }
 
+// Release a context's multi-determinant expansion.
+static void md_free(oqmc_ctx* ctx) {
+  OqMdHost* m = ctx->md;
+  if (!m) return;
+  cudaFree(m->d_C);
+  cudaFree(m->d_coef);
+  cudaFree(m->d_det);
+  cudaFree(m->d_occ);
+  cudaFree(m->d_scratch);
+  delete m;
+  ctx->md = nullptr;
+}
+
 // Doubles in the three-body Jastrow table of a descriptor.
 static size_t j3_table_len(const oqmc_system_desc* d) {
   if (!d->has_j3) return 0;
@@ -367,7 +381,107 @@ int oqmc_destroy(oqmc_ctx* ctx) {
   cudaFree(ctx->d_C32);
   cudaFree(ctx->d_flags);
   cudaFree(ctx->d_j3);
+  md_free(ctx);
   delete ctx;
+  return OQ_OK;
+}
+
+int oqmc_set_multidet(oqmc_ctx* ctx, int ndet, int ncol, const double* C, const double* coef,
+                      const int* occ_up, const int* occ_dn) {
+  if (!ctx) return OQ_ERR_ARG;
+  md_free(ctx);
+  if (ndet == 0) return OQ_OK;
+  const int N = ctx->nocc, nbf = ctx->nbf;
+  if (ndet < 0 || ncol < N || !C || !coef || !occ_up || !occ_dn)
+    return set_err(ctx, OQ_ERR_ARG, "bad multi-determinant arguments%s");
+  // the orbital columns the expansion uses, in increasing order
+  std::vector<int> slot(ncol, -1);
+  for (int d = 0; d < ndet; ++d)
+    for (int sp = 0; sp < 2; ++sp) {
+      const int* o = (sp ? occ_dn : occ_up) + (size_t)d * N;
+      for (int k = 0; k < N; ++k) {
+        if (o[k] < 0 || o[k] >= ncol)
+          return set_err(ctx, OQ_ERR_ARG, "orbital index out of range%s");
+        for (int q = 0; q < k; ++q)
+          if (o[q] == o[k])
+            return set_err(ctx, OQ_ERR_ARG, "orbital repeated within a determinant%s");
+        slot[o[k]] = 0;
+      }
+      if (!std::isfinite(coef[d]))
+        return set_err(ctx, OQ_ERR_ARG, "non-finite CI coefficient%s");
+    }
+  int nused = 0;
+  for (int c = 0; c < ncol; ++c)
+    if (slot[c] == 0) slot[c] = nused++;
+  if (nused > 16)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED,
+                   "multi-determinant expansions may use at most 16 orbitals%s");
+  const int M = (nused <= 8 && N <= 8) ? 8 : 16;
+  // unique spin determinants (orbital slots in the listed order)
+  std::map<std::vector<int>, int> uniq[2];
+  std::vector<std::vector<int>> lists[2];
+  std::vector<int> det(2 * (size_t)ndet);
+  for (int d = 0; d < ndet; ++d)
+    for (int sp = 0; sp < 2; ++sp) {
+      const int* o = (sp ? occ_dn : occ_up) + (size_t)d * N;
+      std::vector<int> key(N);
+      for (int k = 0; k < N; ++k) key[k] = slot[o[k]];
+      auto it = uniq[sp].find(key);
+      int idx;
+      if (it == uniq[sp].end()) {
+        idx = (int)lists[sp].size();
+        uniq[sp][key] = idx;
+        lists[sp].push_back(key);
+      } else {
+        idx = it->second;
+      }
+      det[2 * (size_t)d + sp] = idx;
+    }
+  const int nu0 = (int)lists[0].size(), nu1 = (int)lists[1].size();
+  if (nu0 > OQ_MD_MAXU || nu1 > OQ_MD_MAXU)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED,
+                   "at most 64 distinct determinants per spin%s");
+  for (int d = 0; d < ndet; ++d) det[2 * (size_t)d + 1] += nu0;
+  std::vector<int> occ((size_t)(nu0 + nu1) * N);
+  for (int u = 0; u < nu0; ++u)
+    for (int k = 0; k < N; ++k) occ[(size_t)u * N + k] = lists[0][u][k];
+  for (int u = 0; u < nu1; ++u)
+    for (int k = 0; k < N; ++k) occ[(size_t)(nu0 + u) * N + k] = lists[1][u][k];
+  std::vector<double> Cp((size_t)nbf * M, 0.0);
+  for (int a = 0; a < nbf; ++a)
+    for (int c = 0; c < ncol; ++c)
+      if (slot[c] >= 0) Cp[(size_t)a * M + slot[c]] = C[(size_t)a * ncol + c];
+  OqMdHost* m = new (std::nothrow) OqMdHost();
+  if (!m) return set_err(ctx, OQ_ERR_NOMEM, "out of host memory%s");
+  m->ndet = ndet; m->nu0 = nu0; m->nu1 = nu1; m->M = M;
+  ctx->md = m;
+  cudaError_t e = cudaSuccess;
+  e = (e == cudaSuccess) ? cudaMalloc(&m->d_C, sizeof(double) * Cp.size()) : e;
+  e = (e == cudaSuccess) ? cudaMalloc(&m->d_coef, sizeof(double) * ndet) : e;
+  e = (e == cudaSuccess) ? cudaMalloc(&m->d_det, sizeof(int) * det.size()) : e;
+  e = (e == cudaSuccess) ? cudaMalloc(&m->d_occ, sizeof(int) * occ.size()) : e;
+  e = (e == cudaSuccess) ? cudaMemcpy(m->d_C, Cp.data(), sizeof(double) * Cp.size(),
+                                      cudaMemcpyHostToDevice) : e;
+  e = (e == cudaSuccess) ? cudaMemcpy(m->d_coef, coef, sizeof(double) * ndet,
+                                      cudaMemcpyHostToDevice) : e;
+  e = (e == cudaSuccess) ? cudaMemcpy(m->d_det, det.data(), sizeof(int) * det.size(),
+                                      cudaMemcpyHostToDevice) : e;
+  e = (e == cudaSuccess) ? cudaMemcpy(m->d_occ, occ.data(), sizeof(int) * occ.size(),
+                                      cudaMemcpyHostToDevice) : e;
+  if (e != cudaSuccess) {
+    md_free(ctx);
+    return set_err(ctx, OQ_ERR_CUDA, "CUDA error in set_multidet: %s", cudaGetErrorString(e));
+  }
+  return OQ_OK;
+}
+
+int oqmc_multidet_info(const oqmc_ctx* ctx, int* ndet, int* nu_up, int* nu_dn, int* ncol) {
+  if (!ctx) return OQ_ERR_ARG;
+  const OqMdHost* m = ctx->md;
+  if (ndet) *ndet = m ? m->ndet : 0;
+  if (nu_up) *nu_up = m ? m->nu0 : 0;
+  if (nu_dn) *nu_dn = m ? m->nu1 : 0;
+  if (ncol) *ncol = m ? m->M : 0;
   return OQ_OK;
 }
 
@@ -707,6 +821,9 @@ static uint16_t host_bf16(float f) {
 }
 
 int oqmc_use_tensor_cores(oqmc_ctx* ctx, int enable) {
+  if (ctx && enable && ctx->md)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED,
+                   "the tensor-core local energy supports single determinants only%s");
   if (ctx && enable && (ctx->hsys.has_bs1 || ctx->hsys.has_bs2 || ctx->hsys.has_j3))
     return set_err(ctx, OQ_ERR_UNSUPPORTED,
                    "the tensor-core local energy supports Pade Jastrow terms only%s");
@@ -788,11 +905,18 @@ static size_t smem_sys_c64(const oqmc_ctx* ctx) {
   return sizeof(OqSystem) + sizeof(double) * ctx->nbf * ctx->nocc;
 }
 
+static cudaError_t to_soa(const oqmc_ctx* ctx, const double* X, double* pos, int W,
+                          cudaStream_t s);
+
+static int md_eval(oqmc_ctx* ctx, const double* X, int W, double* logpsi, double* grad,
+                   double* lap, double* eparts, void* stream);
+
 int oqmc_eval(oqmc_ctx* ctx, const double* X, int W, double* logpsi, double* grad,
               double* lap, double* eparts, void* stream) {
   if (!ctx) return OQ_ERR_ARG;
   if (W < 0 || (W > 0 && (!X || !logpsi))) return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
   if (W == 0) return OQ_OK;
+  if (ctx->md) return md_eval(ctx, X, W, logpsi, grad, lap, eparts, stream);
   const OqLaunch L = make_launch(ctx, stream, smem_sys_c64(ctx));
   cudaError_t err = cudaSuccess;
 #define OQ_X(N) err = oq_eval_##N(L, X, W, logpsi, grad, lap, eparts)
@@ -806,6 +930,7 @@ int oqmc_log_psi(oqmc_ctx* ctx, const double* X, int W, double* logpsi, void* st
   if (!ctx) return OQ_ERR_ARG;
   if (W < 0 || (W > 0 && (!X || !logpsi))) return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
   if (W == 0) return OQ_OK;
+  if (ctx->md) return md_eval(ctx, X, W, logpsi, nullptr, nullptr, nullptr, stream);
   const OqLaunch L = make_launch(ctx, stream, smem_sys_c64(ctx));
   cudaError_t err = cudaSuccess;
 #define OQ_X(N) err = oq_logpsi_##N(L, X, W, logpsi)
@@ -841,8 +966,75 @@ static size_t real_size(int precision) {
   return precision == OQ_PREC_MIXED ? sizeof(float) : sizeof(double);
 }
 
+// Multi-determinant sampler state: [pos SoA][inverses (nu0+nu1) nocc^2 W]
+// [log|det| (nu0+nu1) W][signs (nu0+nu1) W], all FP64.
+static size_t md_state_bytes(const oqmc_ctx* ctx, int W) {
+  const size_t nu = (size_t)ctx->md->nu0 + ctx->md->nu1;
+  return align256((size_t)3 * ctx->n_e * W * sizeof(double)) +
+         align256(nu * ctx->nocc * ctx->nocc * W * sizeof(double)) +
+         2 * align256(nu * W * sizeof(double));
+}
+
+static OqMdState md_state(const oqmc_ctx* ctx, void* state, int W) {
+  const size_t nu = (size_t)ctx->md->nu0 + ctx->md->nu1;
+  OqMdState st;
+  char* b = static_cast<char*>(state);
+  st.pos = reinterpret_cast<double*>(b);
+  b += align256((size_t)3 * ctx->n_e * W * sizeof(double));
+  st.ainv = reinterpret_cast<double*>(b);
+  b += align256(nu * ctx->nocc * ctx->nocc * W * sizeof(double));
+  st.ldet = reinterpret_cast<double*>(b);
+  b += align256(nu * W * sizeof(double));
+  st.sgn = reinterpret_cast<double*>(b);
+  st.W = W;
+  st.pad = 0;
+  return st;
+}
+
+static OqMdTables md_tables(const oqmc_ctx* ctx) {
+  const OqMdHost* m = ctx->md;
+  OqMdTables T;
+  T.C = m->d_C; T.coef = m->d_coef; T.det = m->d_det; T.occ = m->d_occ;
+  T.ndet = m->ndet; T.nu0 = m->nu0; T.nu1 = m->nu1; T.pad = 0;
+  return T;
+}
+
+// Multi-determinant evaluation from scratch: FP64 refresh of a scratch state,
+// then the local-energy kernel with the per-walker outputs.
+static int md_eval(oqmc_ctx* ctx, const double* X, int W, double* logpsi, double* grad,
+                   double* lap, double* eparts, void* stream) {
+  OqMdHost* m = ctx->md;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (m->scratch_w < W) {
+    OQ_CUDA(ctx, cudaStreamSynchronize(s));
+    cudaFree(m->d_scratch);
+    m->d_scratch = nullptr;
+    m->scratch_w = 0;
+    OQ_CUDA(ctx, cudaMalloc(&m->d_scratch, md_state_bytes(ctx, W)));
+    m->scratch_w = W;
+  }
+  const OqMdState st = md_state(ctx, m->d_scratch, W);
+  const OqMdTables T = md_tables(ctx);
+  OQ_CUDA(ctx, to_soa(ctx, X, st.pos, W, s));
+  const OqLaunch L = make_launch(ctx, stream, sizeof(OqSystem));
+  OqElocArgs a;
+  memset(&a, 0, sizeof(a));
+  a.pos = st.pos; a.W = W; a.eparts = eparts; a.flags = ctx->d_flags;
+  cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_md_refresh_##N(L, T, st, m->M)
+  OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+  OQ_CUDA(ctx, err);
+#define OQ_X(N) err = oq_md_local_##N(L, T, st, a, logpsi, grad, lap, m->M)
+  OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+  OQ_CUDA(ctx, err);
+  return OQ_OK;
+}
+
 size_t oqmc_state_bytes(const oqmc_ctx* ctx, int W, int precision) {
   if (!ctx || W < 0) return 0;
+  if (ctx->md) return md_state_bytes(ctx, W);
   return align256((size_t)3 * ctx->n_e * W * sizeof(double)) +
          align256((size_t)2 * ctx->nocc * ctx->nocc * W * real_size(precision)) +
          align256((size_t)W * sizeof(double));
@@ -898,8 +1090,23 @@ int oqmc_refresh(oqmc_ctx* ctx, const double* X, int W, void* state, int precisi
   if (W < 0 || (W > 0 && (!X || !state)) || !valid_prec(precision))
     return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
   if (W == 0) return OQ_OK;
-  const OqStatePtrs st = state_ptrs(ctx, state, W, precision);
   cudaStream_t s = (cudaStream_t)stream;
+  if (ctx->md) {
+    if (precision != OQ_PREC_FP64)
+      return set_err(ctx, OQ_ERR_UNSUPPORTED,
+                     "multi-determinant trials are sampled in FP64 only%s");
+    const OqMdState st = md_state(ctx, state, W);
+    OQ_CUDA(ctx, to_soa(ctx, X, st.pos, W, s));
+    const OqLaunch L = make_launch(ctx, stream, sizeof(OqSystem));
+    const OqMdTables T = md_tables(ctx);
+    cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_md_refresh_##N(L, T, st, ctx->md->M)
+    OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+    OQ_CUDA(ctx, err);
+    return OQ_OK;
+  }
+  const OqStatePtrs st = state_ptrs(ctx, state, W, precision);
   OQ_CUDA(ctx, to_soa(ctx, X, st.pos, W, s));
   const OqLaunch L = make_launch(ctx, stream, smem_sys_c64(ctx));
   const int mixed = precision == OQ_PREC_MIXED;
@@ -969,6 +1176,69 @@ static int launch_moves(oqmc_ctx* ctx, const OqMoveArgs& m, int wpb, size_t sm, 
   return OQ_OK;
 }
 
+static int md_moves(oqmc_ctx* ctx, const OqMoveArgs& m, double* sgn, void* stream) {
+  const OqLaunch L = make_launch(ctx, stream, sizeof(OqSystem));
+  const OqMdTables T = md_tables(ctx);
+  cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_md_moves_##N(L, T, m, sgn, ctx->md->M)
+  OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+  OQ_CUDA(ctx, err);
+  return OQ_OK;
+}
+
+// Sweeps with a multi-determinant Slater part (FP64; the same measurement
+// layout as the single-determinant sweeps).
+static int md_sweeps(oqmc_ctx* ctx, double* X, int W, void* state, int precision, int n_sweeps,
+                     int measure_every, double step, uint64_t seed, uint64_t step_base,
+                     double* sums, double* el_trace, double* eparts_last, void* stream) {
+  if (precision != OQ_PREC_FP64)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED, "multi-determinant trials are sampled in FP64 only%s");
+  if (ctx->mlp)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED,
+                   "the learned proposal does not support multi-determinant trials%s");
+  cudaStream_t s = (cudaStream_t)stream;
+  const OqMdState st = md_state(ctx, state, W);
+  const OqMdTables T = md_tables(ctx);
+  OQ_CUDA(ctx, to_soa(ctx, X, st.pos, W, s));
+  OqMoveArgs m;
+  memset(&m, 0, sizeof(m));
+  m.pos = st.pos; m.ainv = st.ainv; m.logdet = st.ldet; m.W = W; m.mode = 0;
+  m.step = step; m.seed = seed; m.flags = ctx->d_flags;
+  m.proposal = ctx->proposal; m.scale_r0 = ctx->scale_r0; m.scale_fmin = ctx->scale_fmin;
+  OqElocArgs el;
+  memset(&el, 0, sizeof(el));
+  el.pos = st.pos; el.W = W; el.flags = ctx->d_flags;
+  const OqLaunch Le = make_launch(ctx, stream, sizeof(OqSystem));
+  const int n_meas = n_sweeps / measure_every;
+  int done = 0;
+  for (int k = 0; k < n_meas; ++k) {
+    m.n_steps = measure_every;
+    m.step_base = step_base + done;
+    m.acc_sum = sums + (size_t)k * OQ_NSUM + 5;
+    int rc = md_moves(ctx, m, st.sgn, stream);
+    if (rc != OQ_OK) return rc;
+    done += measure_every;
+    el.sums = sums + (size_t)k * OQ_NSUM;
+    el.el_trace = el_trace ? el_trace + (size_t)k * W : nullptr;
+    el.eparts = (k == n_meas - 1) ? eparts_last : nullptr;
+    cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_md_local_##N(Le, T, st, el, nullptr, nullptr, nullptr, ctx->md->M)
+    OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+    OQ_CUDA(ctx, err);
+  }
+  if (done < n_sweeps) {
+    m.n_steps = n_sweeps - done;
+    m.step_base = step_base + done;
+    m.acc_sum = nullptr;
+    int rc = md_moves(ctx, m, st.sgn, stream);
+    if (rc != OQ_OK) return rc;
+  }
+  OQ_CUDA(ctx, to_aos(ctx, st.pos, X, W, s));
+  return OQ_OK;
+}
+
 int oqmc_sweeps(oqmc_ctx* ctx, double* X, int W, void* state, int precision, int n_sweeps,
                 int measure_every, double step, uint64_t seed, uint64_t step_base,
                 double* sums, double* el_trace, double* eparts_last, int wpb,
@@ -981,6 +1251,9 @@ int oqmc_sweeps(oqmc_ctx* ctx, double* X, int W, void* state, int precision, int
     return set_err(ctx, OQ_ERR_ARG, "null buffer%s");
   if (ctx->mlp && precision != OQ_PREC_MIXED)
     return set_err(ctx, OQ_ERR_UNSUPPORTED, "the learned proposal runs in mixed precision only%s");
+  if (ctx->md)
+    return md_sweeps(ctx, X, W, state, precision, n_sweeps, measure_every, step, seed, step_base,
+                     sums, el_trace, eparts_last, stream);
   size_t sm;
   wpb = pick_wpb(ctx, wpb, precision, &sm);
   if (wpb == -1) return set_err(ctx, OQ_ERR_ARG, "walkers_per_block must be 32, 64 or 128%s");
@@ -1053,6 +1326,23 @@ int oqmc_basin(oqmc_ctx* ctx, double* X, int W, void* state, int precision, int 
     return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
   if (W == 0 || n_steps == 0) return OQ_OK;
   if (!X || !state) return set_err(ctx, OQ_ERR_ARG, "null buffer%s");
+  if (ctx->md) {
+    if (precision != OQ_PREC_FP64)
+      return set_err(ctx, OQ_ERR_UNSUPPORTED,
+                     "multi-determinant trials are sampled in FP64 only%s");
+    cudaStream_t s = (cudaStream_t)stream;
+    const OqMdState st = md_state(ctx, state, W);
+    OQ_CUDA(ctx, to_soa(ctx, X, st.pos, W, s));
+    OqMoveArgs m;
+    memset(&m, 0, sizeof(m));
+    m.pos = st.pos; m.ainv = st.ainv; m.logdet = st.ldet; m.W = W; m.mode = 1;
+    m.n_steps = n_steps; m.step = sigma; m.seed = seed; m.step_base = step_base;
+    m.acc_sum = acc_sum; m.flags = ctx->d_flags;
+    int rc = md_moves(ctx, m, st.sgn, stream);
+    if (rc != OQ_OK) return rc;
+    OQ_CUDA(ctx, to_aos(ctx, st.pos, X, W, s));
+    return OQ_OK;
+  }
   size_t sm;
   const int wpb = pick_wpb(ctx, 0, precision, &sm);
   if (wpb < 0)

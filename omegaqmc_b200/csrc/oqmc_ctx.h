@@ -5,6 +5,18 @@
 
 struct OqSpecModule;
 
+// Multi-determinant expansion of a context (device tables and the scratch
+// state the evaluation entry points use).
+struct OqMdHost {
+  int ndet, nu0, nu1, M;
+  double* d_C;          // nbf x M
+  double* d_coef;
+  int* d_det;
+  int* d_occ;
+  void* d_scratch;      // evaluation state for up to scratch_w walkers
+  int scratch_w;
+};
+
 struct oqmc_ctx {
   int device;
   int nocc, n_e, nbf, natm;
@@ -27,6 +39,7 @@ struct oqmc_ctx {
   void* mlp_mod;                // its specialised sweep kernels (module; 2 and 4 groups)
   void* mlp_fn[2];
   int mlp_groups;               // walker groups per CTA of the learned-proposal sweep
+  OqMdHost* md;                 // multi-determinant expansion, or null
   char err[512];
 };
 

@@ -13,8 +13,11 @@
 
 // Gauss-Jordan inverse with partial pivoting of the N x N matrix a
 // (destroyed); returns false if a pivot is exactly zero or not finite.
+// logdet = log|det a|; *sign (when given) = the sign of det a.
 template <int N>
-__device__ bool oq_invert(double (&a)[N][N], double (&inv)[N][N], double& logdet) {
+__device__ bool oq_invert(double (&a)[N][N], double (&inv)[N][N], double& logdet,
+                          double* sign = nullptr) {
+  double sg = 1.0;
 #pragma unroll
   for (int i = 0; i < N; ++i)
 #pragma unroll
@@ -29,6 +32,7 @@ __device__ bool oq_invert(double (&a)[N][N], double (&inv)[N][N], double& logdet
     }
     if (!(best > 0.0) || !isfinite(best)) return false;
     if (piv != k) {
+      sg = -sg;
       for (int j = 0; j < N; ++j) {
         double t = a[k][j]; a[k][j] = a[piv][j]; a[piv][j] = t;
         t = inv[k][j]; inv[k][j] = inv[piv][j]; inv[piv][j] = t;
@@ -36,6 +40,7 @@ __device__ bool oq_invert(double (&a)[N][N], double (&inv)[N][N], double& logdet
     }
     const double d = a[k][k];
     logdet += log(fabs(d));
+    if (d < 0.0) sg = -sg;
     const double rd = 1.0 / d;
     for (int j = 0; j < N; ++j) { a[k][j] *= rd; inv[k][j] *= rd; }
     for (int i = 0; i < N; ++i) {
@@ -46,6 +51,7 @@ __device__ bool oq_invert(double (&a)[N][N], double (&inv)[N][N], double& logdet
       }
     }
   }
+  if (sign) *sign = sg;
   return true;
 }
 

@@ -116,3 +116,56 @@ cudaError_t OQ_FN(oq_eloc_tc)(const OqLaunch& L, const OqElocArgs& a, const void
                                                 static_cast<const unsigned char*>(Bpack), a);
   return cudaGetLastError();
 }
+
+// Multi-determinant kernels: M = 8 or 16 orbital columns (M >= OQ_N).
+template <int M>
+static cudaError_t md_refresh_m(const OqLaunch& L, const OqMdTables& T, const OqMdState& st) {
+  cudaError_t e = oq_smem_attr(k_md_refresh<OQ_N, M>, L.smem);
+  if (e != cudaSuccess) return e;
+  k_md_refresh<OQ_N, M><<<(st.W + 127) / 128, 128, L.smem, L.stream>>>(L.sys, T, st, L.flags);
+  return cudaGetLastError();
+}
+
+template <int M>
+static cudaError_t md_moves_m(const OqLaunch& L, const OqMdTables& T, const OqMoveArgs& a,
+                              double* sgn) {
+  cudaError_t e = oq_smem_attr(k_md_moves<OQ_N, M>, L.smem);
+  if (e != cudaSuccess) return e;
+  k_md_moves<OQ_N, M><<<(a.W + 127) / 128, 128, L.smem, L.stream>>>(L.sys, T, a, sgn);
+  return cudaGetLastError();
+}
+
+template <int M>
+static cudaError_t md_local_m(const OqLaunch& L, const OqMdTables& T, const OqMdState& st,
+                              const OqElocArgs& a, double* logpsi, double* grad, double* lap) {
+  cudaError_t e = oq_smem_attr(k_md_local<OQ_N, M>, L.smem);
+  if (e != cudaSuccess) return e;
+  k_md_local<OQ_N, M><<<(st.W + 127) / 128, 128, L.smem, L.stream>>>(L.sys, T, st, a, logpsi,
+                                                                       grad, lap);
+  return cudaGetLastError();
+}
+
+cudaError_t OQ_FN(oq_md_refresh)(const OqLaunch& L, const OqMdTables& T, const OqMdState& st,
+                                 int M) {
+  if constexpr (OQ_N <= 8) {
+    if (M == 8) return md_refresh_m<8>(L, T, st);
+  }
+  return M == 16 ? md_refresh_m<16>(L, T, st) : cudaErrorInvalidValue;
+}
+
+cudaError_t OQ_FN(oq_md_moves)(const OqLaunch& L, const OqMdTables& T, const OqMoveArgs& a,
+                               double* sgn, int M) {
+  if constexpr (OQ_N <= 8) {
+    if (M == 8) return md_moves_m<8>(L, T, a, sgn);
+  }
+  return M == 16 ? md_moves_m<16>(L, T, a, sgn) : cudaErrorInvalidValue;
+}
+
+cudaError_t OQ_FN(oq_md_local)(const OqLaunch& L, const OqMdTables& T, const OqMdState& st,
+                               const OqElocArgs& a, double* logpsi, double* grad, double* lap,
+                               int M) {
+  if constexpr (OQ_N <= 8) {
+    if (M == 8) return md_local_m<8>(L, T, st, a, logpsi, grad, lap);
+  }
+  return M == 16 ? md_local_m<16>(L, T, st, a, logpsi, grad, lap) : cudaErrorInvalidValue;
+}

@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "oqmc_eloc_tc.cuh"
+#include "oqmc_multidet.cuh"
 
 struct OqLaunch {
   const OqSystem* sys;
@@ -25,7 +26,14 @@ struct OqLaunch {
   cudaError_t oq_moves_##N(const OqLaunch& L, const OqMoveArgs& a, int wpb, int mixed); \
   cudaError_t oq_eloc_##N(const OqLaunch& L, const OqElocArgs& a, int mixed);           \
   cudaError_t oq_eloc_tc_##N(const OqLaunch& L, const OqElocArgs& a, const void* Bpack, \
-                             int nbf);
+                             int nbf);                                                \
+  cudaError_t oq_md_refresh_##N(const OqLaunch& L, const OqMdTables& T,                \
+                                const OqMdState& st, int M);                           \
+  cudaError_t oq_md_moves_##N(const OqLaunch& L, const OqMdTables& T,                  \
+                              const OqMoveArgs& a, double* sgn, int M);                \
+  cudaError_t oq_md_local_##N(const OqLaunch& L, const OqMdTables& T,                  \
+                              const OqMdState& st, const OqElocArgs& a, double* logpsi, \
+                              double* grad, double* lap, int M);
 
 #define OQ_NOCC_LIST(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(10) X(12) X(14) X(16)
 

@@ -301,31 +301,21 @@ __device__ __forceinline__ double oq_scaled_width(const SJ& S, double x, double 
   return step * fmin(1.0, fmax(fmn, f));
 }
 
-// One single-electron Metropolis move of electron e to (nx, ny, nz) against
-// shared-memory state; log_extra is the log proposal-density ratio
-// log q(old)/q(new) (0 for symmetric proposals).  Returns acceptance.
-// J supplies the nuclei and Jastrow constants (natm, nuc, has_j1, j1a, j1b,
-// has_j2, j2): the system struct itself or a compact copy of those fields;
-// S is handed to the basis policy.
-template <int NOCC, typename T, typename Real, class B, class SJ>
-__device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, const OqSplit& SP,
-                                            const Real* __restrict__ C, double* pos,
-                                            Real* Ai, int WPB, int tid, int e,
-                                            double nx, double ny, double nz,
-                                            double log_extra, double u, double& logdet) {
-  constexpr int NE = 2 * NOCC;
-  constexpr int NN = NOCC * NOCC;
-  const int s = e & 1, i = e >> 1;
+// Change of the Jastrow factor (arithmetic in T) when electron e moves from
+// (ox, oy, oz) to (nx, ny, nz), and the MIN_DIST_THRESHOLD test of the new
+// position (FP64; OmegaQMC/constants.py:23): valid is cleared when an
+// electron-electron or electron-nucleus distance falls below 1e-4.  The
+// other electrons' coordinate c is pos[(3 j + c) * ps].
+template <int NE, typename T, class SJ>
+__device__ __forceinline__ T oq_jastrow_delta(const SJ& J, const OqSystem& S, const double* pos,
+                                              int ps, int e, double ox, double oy, double oz,
+                                              double nx, double ny, double nz, bool& valid) {
   const double thr2 = 1e-4 * 1e-4;
-  const double ox = pos[(3 * e) * WPB + tid], oy = pos[(3 * e + 1) * WPB + tid],
-               oz = pos[(3 * e + 2) * WPB + tid];
-  // Jastrow change (arithmetic in T) and the MIN_DIST_THRESHOLD test (FP64)
   T dJ = (T)0;
-  bool valid = true;
+  valid = true;
   for (int j = 0; j < NE; ++j) {
     if (j == e) continue;
-    const double xj = pos[(3 * j) * WPB + tid], yj = pos[(3 * j + 1) * WPB + tid],
-                 zj = pos[(3 * j + 2) * WPB + tid];
+    const double xj = pos[(3 * j) * ps], yj = pos[(3 * j + 1) * ps], zj = pos[(3 * j + 2) * ps];
     const double ax = nx - xj, ay = ny - yj, az = nz - zj;
     const double rn2 = ax * ax + ay * ay + az * az;
     valid = valid && (rn2 >= thr2);
@@ -367,8 +357,31 @@ __device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, cons
     }
   }
   if (S.has_j3)
-    dJ -= oq_j3_electron<T>(S, pos + tid, WPB, NE, e, 0, nx, ny, nz) -
-          oq_j3_electron<T>(S, pos + tid, WPB, NE, e, 0, ox, oy, oz);
+    dJ -= oq_j3_electron<T>(S, pos, (size_t)ps, NE, e, 0, nx, ny, nz) -
+          oq_j3_electron<T>(S, pos, (size_t)ps, NE, e, 0, ox, oy, oz);
+  return dJ;
+}
+
+// One single-electron Metropolis move of electron e to (nx, ny, nz) against
+// shared-memory state; log_extra is the log proposal-density ratio
+// log q(old)/q(new) (0 for symmetric proposals).  Returns acceptance.
+// J supplies the nuclei and Jastrow constants (natm, nuc, has_j1, j1a, j1b,
+// has_j2, j2): the system struct itself or a compact copy of those fields;
+// S is handed to the basis policy.
+template <int NOCC, typename T, typename Real, class B, class SJ>
+__device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, const OqSplit& SP,
+                                            const Real* __restrict__ C, double* pos,
+                                            Real* Ai, int WPB, int tid, int e,
+                                            double nx, double ny, double nz,
+                                            double log_extra, double u, double& logdet) {
+  constexpr int NE = 2 * NOCC;
+  constexpr int NN = NOCC * NOCC;
+  const int s = e & 1, i = e >> 1;
+  const double ox = pos[(3 * e) * WPB + tid], oy = pos[(3 * e + 1) * WPB + tid],
+               oz = pos[(3 * e + 2) * WPB + tid];
+  // Jastrow change (arithmetic in T) and the MIN_DIST_THRESHOLD test (FP64)
+  bool valid;
+  const T dJ = oq_jastrow_delta<NE, T>(J, S, pos + tid, WPB, e, ox, oy, oz, nx, ny, nz, valid);
   // new MO row and the ratio vector w_j = sum_m v_m A[m][j]; R = w_i
   T v[NOCC];
   B::template mo_val<T, Real>(S, SP, C, nx, ny, nz, v);
@@ -413,6 +426,45 @@ __device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, cons
     logdet += log(fabs(Rd));
   }
   return acc;
+}
+
+// Basin relocation proposal (basin_move_1w, OmegaQMC/vmc_gto.py:925-957):
+// one random electron to N(R_J, sigma^2) around a random nucleus J.  Returns
+// the electron; sets its proposed position, the log proposal ratio
+// log q(old) - log q(new) with q(x) = sum_J exp(-|x - R_J|^2 / 2 sigma^2)
+// (computed as a log-sum-exp) and the acceptance uniform u.
+template <int NE>
+__device__ __forceinline__ int oq_basin_propose(const OqSystem& S, const double* pos, int ps,
+                                                uint64_t seed, uint32_t w, uint32_t gstep,
+                                                double sg, double& nx, double& ny, double& nz,
+                                                double& log_qratio, double& u) {
+  double n3[3];
+  oq_move_randoms(seed, w, gstep, 0xB0000000u, n3, u);
+  const OqU4 c = {w, gstep, 0xB0000001u, 2u};
+  const OqU4 r = oq_philox(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const int e = (int)(((uint64_t)r.x * NE) >> 32);
+  const int J = (int)(((uint64_t)r.y * S.natm) >> 32);
+  const double inv2s2 = 1.0 / (2.0 * sg * sg);
+  nx = S.nuc[J][0] + sg * n3[0];
+  ny = S.nuc[J][1] + sg * n3[1];
+  nz = S.nuc[J][2] + sg * n3[2];
+  const double ox = pos[(3 * e) * ps], oy = pos[(3 * e + 1) * ps], oz = pos[(3 * e + 2) * ps];
+  double mo = -INFINITY, mn = -INFINITY;
+  for (int I = 0; I < S.natm; ++I) {
+    const double dox = ox - S.nuc[I][0], doy = oy - S.nuc[I][1], doz = oz - S.nuc[I][2];
+    const double dnx = nx - S.nuc[I][0], dny = ny - S.nuc[I][1], dnz = nz - S.nuc[I][2];
+    mo = fmax(mo, -(dox * dox + doy * doy + doz * doz) * inv2s2);
+    mn = fmax(mn, -(dnx * dnx + dny * dny + dnz * dnz) * inv2s2);
+  }
+  double so = 0.0, sn = 0.0;
+  for (int I = 0; I < S.natm; ++I) {
+    const double dox = ox - S.nuc[I][0], doy = oy - S.nuc[I][1], doz = oz - S.nuc[I][2];
+    const double dnx = nx - S.nuc[I][0], dny = ny - S.nuc[I][1], dnz = nz - S.nuc[I][2];
+    so += exp(-(dox * dox + doy * doy + doz * doz) * inv2s2 - mo);
+    sn += exp(-(dnx * dnx + dny * dny + dnz * dnz) * inv2s2 - mn);
+  }
+  log_qratio = (mo + log(so)) - (mn + log(sn));
+  return e;
 }
 
 // Metropolis moves, one thread per walker, state resident in shared memory
@@ -491,33 +543,9 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
                                            log_extra, u, logdet);
       }
     } else {
-      double n3[3], u;
-      oq_move_randoms(a.seed, (uint32_t)w, gstep, 0xB0000000u, n3, u);
-      const OqU4 c = {(uint32_t)w, gstep, 0xB0000001u, 2u};
-      const OqU4 r = oq_philox(c, (uint32_t)a.seed, (uint32_t)(a.seed >> 32));
-      const int e = (int)(((uint64_t)r.x * NE) >> 32);
-      const int J = (int)(((uint64_t)r.y * S.natm) >> 32);
-      const double sg = a.step, inv2s2 = 1.0 / (2.0 * sg * sg);
-      const double nx = S.nuc[J][0] + sg * n3[0], ny = S.nuc[J][1] + sg * n3[1],
-                   nz = S.nuc[J][2] + sg * n3[2];
-      const double ox = pos[(3 * e) * WPB + tid], oy = pos[(3 * e + 1) * WPB + tid],
-                   oz = pos[(3 * e + 2) * WPB + tid];
-      // log q(x) = logsumexp_J(-|x - R_J|^2 / 2 sigma^2)
-      double mo = -INFINITY, mn = -INFINITY;
-      for (int I = 0; I < S.natm; ++I) {
-        const double dox = ox - S.nuc[I][0], doy = oy - S.nuc[I][1], doz = oz - S.nuc[I][2];
-        const double dnx = nx - S.nuc[I][0], dny = ny - S.nuc[I][1], dnz = nz - S.nuc[I][2];
-        mo = fmax(mo, -(dox * dox + doy * doy + doz * doz) * inv2s2);
-        mn = fmax(mn, -(dnx * dnx + dny * dny + dnz * dnz) * inv2s2);
-      }
-      double so = 0.0, sn = 0.0;
-      for (int I = 0; I < S.natm; ++I) {
-        const double dox = ox - S.nuc[I][0], doy = oy - S.nuc[I][1], doz = oz - S.nuc[I][2];
-        const double dnx = nx - S.nuc[I][0], dny = ny - S.nuc[I][1], dnz = nz - S.nuc[I][2];
-        so += exp(-(dox * dox + doy * doy + doz * doz) * inv2s2 - mo);
-        sn += exp(-(dnx * dnx + dny * dny + dnz * dnz) * inv2s2 - mn);
-      }
-      const double log_qratio = (mo + log(so)) - (mn + log(sn));
+      double u, nx, ny, nz, log_qratio;
+      const int e = oq_basin_propose<NE>(S, pos + tid, WPB, a.seed, (uint32_t)w, gstep, a.step,
+                                         nx, ny, nz, log_qratio, u);
       nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
                                          log_qratio, u, logdet);
     }
@@ -535,33 +563,17 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
   }
 }
 
-// Local-energy contributions of electron e of one walker: its Coulomb terms
-// (e-e counted once, for partners j > e; gto.py:2406-2451), the Laplacian
-// term lap_e = sum_m A[m][i] L[i][m] - |Gamma_e|^2 + lap J_e and the squared
-// total gradient |Gamma_e + grad J_e|^2 (_slater_det_assemble, gto.py:728-778;
-// Padé VGL, gto.py:1575-1649).  pos points at the walker's x of electron 0
-// with stride ps between coordinates; A at its inverse entry (0,0,0) with
-// stride as between entries.  The four outputs are accumulated (+=).
-template <int NOCC, typename T, typename Real, class B, class SJ>
-__device__ __forceinline__ void oq_eloc_electron(const SJ& J, const OqSystem& S,
-                                                 const OqSplit& SP, const Real* __restrict__ C,
-                                                 const double* pos, size_t ps, const Real* A,
-                                                 size_t as, int e, double& ee, double& en,
-                                                 double& lp_tot, double& g2) {
-  constexpr int NE = 2 * NOCC;
-  const int s = e & 1, i = e >> 1;
-  const double xe = pos[(size_t)(3 * e) * ps], ye = pos[(size_t)(3 * e + 1) * ps],
-               ze = pos[(size_t)(3 * e + 2) * ps];
-  T mv[NOCC], mg[NOCC][3], ml[NOCC];
-  B::template mo_vgl<T, Real>(S, SP, C, xe, ye, ze, mv, mg, ml);
-  T gx = 0, gy = 0, gz = 0, lp = 0;
-#pragma unroll
-  for (int m = 0; m < NOCC; ++m) {
-    const T am = (T)A[(size_t)((s * NOCC + m) * NOCC + i) * as];
-    gx += am * mg[m][0]; gy += am * mg[m][1]; gz += am * mg[m][2];
-    lp += am * ml[m];
-  }
-  T jx = (T)0, jy = (T)0, jz = (T)0, jl = (T)0;
+// Jastrow gradient and Laplacian of electron e at (xe, ye, ze) (Padé,
+// B-spline and three-body terms; gto.py:1575-1649, 1657-1931, 2042-2196),
+// accumulated into (jx, jy, jz, jl), and its Coulomb terms (e-e counted once,
+// for partners j > e; e-n; gto.py:2406-2451) into ee, en.  The other
+// electrons' coordinate c is pos[(3 j + c) * ps].
+template <int NE, typename T, class SJ>
+__device__ __forceinline__ void oq_jastrow_vgl_coulomb(const SJ& J, const OqSystem& S,
+                                                       const double* pos, size_t ps, int e,
+                                                       double xe, double ye, double ze, T& jx,
+                                                       T& jy, T& jz, T& jl, double& ee,
+                                                       double& en) {
   for (int j = 0; j < NE; ++j) {
     if (j == e) continue;
     const double dx = xe - pos[(size_t)(3 * j) * ps], dy = ye - pos[(size_t)(3 * j + 1) * ps],
@@ -605,6 +617,36 @@ __device__ __forceinline__ void oq_eloc_electron(const SJ& J, const OqSystem& S,
     }
   }
   if (S.has_j3) oq_j3_vgl_electron<T>(S, pos, ps, NE, e, xe, ye, ze, jx, jy, jz, jl);
+}
+
+// Local-energy contributions of electron e of one walker: its Coulomb terms
+// (e-e counted once, for partners j > e; gto.py:2406-2451), the Laplacian
+// term lap_e = sum_m A[m][i] L[i][m] - |Gamma_e|^2 + lap J_e and the squared
+// total gradient |Gamma_e + grad J_e|^2 (_slater_det_assemble, gto.py:728-778;
+// Padé VGL, gto.py:1575-1649).  pos points at the walker's x of electron 0
+// with stride ps between coordinates; A at its inverse entry (0,0,0) with
+// stride as between entries.  The four outputs are accumulated (+=).
+template <int NOCC, typename T, typename Real, class B, class SJ>
+__device__ __forceinline__ void oq_eloc_electron(const SJ& J, const OqSystem& S,
+                                                 const OqSplit& SP, const Real* __restrict__ C,
+                                                 const double* pos, size_t ps, const Real* A,
+                                                 size_t as, int e, double& ee, double& en,
+                                                 double& lp_tot, double& g2) {
+  constexpr int NE = 2 * NOCC;
+  const int s = e & 1, i = e >> 1;
+  const double xe = pos[(size_t)(3 * e) * ps], ye = pos[(size_t)(3 * e + 1) * ps],
+               ze = pos[(size_t)(3 * e + 2) * ps];
+  T mv[NOCC], mg[NOCC][3], ml[NOCC];
+  B::template mo_vgl<T, Real>(S, SP, C, xe, ye, ze, mv, mg, ml);
+  T gx = 0, gy = 0, gz = 0, lp = 0;
+#pragma unroll
+  for (int m = 0; m < NOCC; ++m) {
+    const T am = (T)A[(size_t)((s * NOCC + m) * NOCC + i) * as];
+    gx += am * mg[m][0]; gy += am * mg[m][1]; gz += am * mg[m][2];
+    lp += am * ml[m];
+  }
+  T jx = (T)0, jy = (T)0, jz = (T)0, jl = (T)0;
+  oq_jastrow_vgl_coulomb<NE, T>(J, S, pos, ps, e, xe, ye, ze, jx, jy, jz, jl, ee, en);
   const double sgx = (double)gx, sgy = (double)gy, sgz = (double)gz;
   const double Gx = sgx + (double)jx, Gy = sgy + (double)jy, Gz = sgz + (double)jz;
   lp_tot += (double)lp - (sgx * sgx + sgy * sgy + sgz * sgz) + (double)jl;

@@ -14,8 +14,9 @@ tensors.  Jastrow parameters (``curr_params``) and nuclear coordinates are
 call-time arguments as in the reference; a device context is built (and
 cached) for each distinct set.
 
-Not on this path: multi-determinant trials, B-spline/three-body Jastrows and
-the MO-coefficient (CPHF/force) variants, which raise ``NotImplementedError``.
+Multi-determinant ``trial`` dicts evaluate through the library's FP64
+multi-determinant kernels.  Not on this path: the MO-coefficient
+(CPHF/force) variants, which raise ``NotImplementedError``.
 """
 from __future__ import annotations
 
@@ -75,9 +76,7 @@ class PsiGTO:
     """Per-walker GTO Slater-Jastrow functions backed by the CUDA kernels."""
 
     def __init__(self, mf, params_cusp=None, trial=None, jastrow_config=None):
-        if trial is not None:
-            raise NotImplementedError(
-                "multi-determinant trials are not supported on this path")
+        self.trial = trial
         self.mf = mf
         self.params_cusp = params_cusp
         self.jastrow_config = jastrow_config
@@ -98,7 +97,7 @@ class PsiGTO:
             for kk, v in p.items():
                 if isinstance(v, dict):
                     p[kk] = {a: _np(b) for a, b in v.items()}
-            system = build_system(mf, p, self.params_cusp, self.jastrow_config)
+            system = build_system(mf, p, self.params_cusp, self.jastrow_config, self.trial)
             ctx = GTOContext(system)
             if len(self._ctx) > 16:
                 self._ctx.clear()

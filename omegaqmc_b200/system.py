@@ -594,6 +594,7 @@ class System:
     bs2: object = None         # B-spline J2: {"like", "unlike": coefs, "r_cut"}
     bs1: object = None         # B-spline J1: per atom (coefs, r_cut) or None
     j3: object = None          # J3_eeI tables (see :func:`parse_j3`) or None
+    md: object = None          # multi-determinant trial (see :func:`parse_trial`) or None
 
     @property
     def natm(self):
@@ -645,7 +646,45 @@ class System:
         return sum(sh.nprim for sh in self.shells)
 
 
-def build_system(mf, params_corr=None, params_cusp=None, jastrow_config=None):
+def parse_trial(trial, n_up, n_dn):
+    """Multi-determinant expansion of a ``trial`` dict (``_parse_mol``,
+    gto.py:846-863; format of ``OmegaQMC/psi/trial.py``): ``mo_coeff``
+    (nao, nmo) for restricted orbitals or (2, nao, nmo) for UHF ones (alpha
+    and beta columns side by side, the down occupations shifted by nmo),
+    ``ci_coeffs`` (ndet,), ``occ_up`` (ndet, n_up), ``occ_dn`` (ndet, n_dn).
+
+    Returns ``{"C": (nao, ncol), "ci", "occ_up", "occ_dn"}``."""
+    def arr(x, dt):
+        if torch_like(x):
+            x = x.detach().cpu().numpy()
+        return np.asarray(x, dtype=dt)
+
+    mo = arr(trial["mo_coeff"], np.float64)
+    ci = np.ravel(arr(trial["ci_coeffs"], np.float64))
+    occ_up = np.atleast_2d(arr(trial["occ_up"], np.int64))
+    occ_dn = np.atleast_2d(arr(trial["occ_dn"], np.int64))
+    if mo.ndim == 3:
+        if mo.shape[0] != 2:
+            raise ValueError("UHF trial mo_coeff must have shape (2, nao, nmo)")
+        occ_dn = occ_dn + mo.shape[2]
+        mo = np.concatenate(list(mo), axis=1)
+    if mo.ndim != 2:
+        raise ValueError("trial mo_coeff must have shape (nao, nmo) or (2, nao, nmo)")
+    if not (ci.shape[0] == occ_up.shape[0] == occ_dn.shape[0]) or ci.shape[0] < 1:
+        raise ValueError("ci_coeffs, occ_up and occ_dn must list the same determinants")
+    if occ_up.shape[1] != n_up or occ_dn.shape[1] != n_dn:
+        raise ValueError(f"trial occupations have {occ_up.shape[1]} up and {occ_dn.shape[1]} "
+                         f"down orbitals, the molecule {n_up} and {n_dn} electrons")
+    if occ_up.min() < 0 or occ_dn.min() < 0 or max(occ_up.max(), occ_dn.max()) >= mo.shape[1]:
+        raise ValueError("trial occupation index out of range of mo_coeff")
+    return {"C": np.ascontiguousarray(mo), "ci": ci, "occ_up": occ_up, "occ_dn": occ_dn}
+
+
+def torch_like(x):
+    return hasattr(x, "detach") and hasattr(x, "cpu")
+
+
+def build_system(mf, params_corr=None, params_cusp=None, jastrow_config=None, trial=None):
     """Build a :class:`System` from a PySCF-style mean-field object.
 
     Args:
@@ -657,6 +696,9 @@ def build_system(mf, params_corr=None, params_cusp=None, jastrow_config=None):
             cusp correction (``gto.py:846-888``).
         jastrow_config: B-spline cutoffs (see :func:`parse_bspline`) and
             the J3_eeI orders and cutoff (see :func:`parse_j3`).
+        trial: multi-determinant trial dict (see :func:`parse_trial`); the
+            single-determinant orbitals are then the first determinant's up
+            orbitals (``mo_occ_coeff``, gto.py:860-862).
     """
     mol = mf.mol
     n_e = mol.tot_electrons()
@@ -665,14 +707,20 @@ def build_system(mf, params_corr=None, params_cusp=None, jastrow_config=None):
         raise NotImplementedError(
             "only closed-shell single determinants are supported "
             f"(n_up={n_up}, n_dn={n_dn})")
-    nocc = int(np.count_nonzero(np.asarray(mf.mo_occ) > 0))
-    if nocc != n_up:
-        raise ValueError(f"mo_occ marks {nocc} occupied orbitals, expected "
-                         f"{n_up} for {n_e} electrons")
+    md = None
+    if trial is not None:
+        md = parse_trial(trial, n_up, n_dn)
+        nocc = n_up
+        C = np.ascontiguousarray(md["C"][:, md["occ_up"][0]])
+    else:
+        nocc = int(np.count_nonzero(np.asarray(mf.mo_occ) > 0))
+        if nocc != n_up:
+            raise ValueError(f"mo_occ marks {nocc} occupied orbitals, expected "
+                             f"{n_up} for {n_e} electrons")
+        C = np.ascontiguousarray(np.asarray(mf.mo_coeff, dtype=np.float64)[:, :nocc])
     cusp = params_cusp is not None
     shells = build_shells(mol, cusp=cusp)
     nbf = shells[-1].isgs + shells[-1].nsgs
-    C = np.ascontiguousarray(np.asarray(mf.mo_coeff, dtype=np.float64)[:, :nocc])
     if C.shape[0] != nbf:
         raise ValueError(f"mo_coeff has {C.shape[0]} rows, basis has {nbf}")
     natm = mol.natm
@@ -698,4 +746,4 @@ def build_system(mf, params_corr=None, params_cusp=None, jastrow_config=None):
     return System(nuc=mol.atom_coords(unit="Bohr"), Z=Z, shells=shells, C=C,
                   n_up=n_up, n_dn=n_dn, has_j1=has_j1, j1=j1, has_j2=has_j2,
                   j2=j2, cusp=cusp, cusp_rc=rc, cusp_q0=q0,
-                  cusp_coeff=coeff, symbols=mol.elements, bs2=bs2, bs1=bs1, j3=j3)
+                  cusp_coeff=coeff, symbols=mol.elements, bs2=bs2, bs1=bs1, j3=j3, md=md)

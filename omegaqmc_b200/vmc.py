@@ -105,9 +105,10 @@ def get_vmc_gto_func(mf, params_corr, cusp_scheme="Quady2025", gr_scheme="scheme
     constants instead of fitting them; ``precision`` is ``"fp64"`` or
     ``"mixed"``; ``proposal`` is ``"plain"`` (fixed-width Gaussian) or
     ``"scaled"`` (nucleus-scaled width); ``specialize`` compiles kernels for
-    this molecule (NVRTC) when available."""
-    if trial is not None:
-        raise NotImplementedError("multi-determinant trials are not supported on this path")
+    this molecule (NVRTC) when available.  A multi-determinant ``trial``
+    samples in FP64 through the library's multi-determinant kernels."""
+    if trial is not None and precision != "fp64":
+        raise ValueError("multi-determinant trials are sampled in precision='fp64'")
     if symmop_list not in (None, "E", ["E"]):
         raise NotImplementedError("symmetry-adapted (correlated-sampling) operations are "
                                   "not supported on this path")
@@ -126,20 +127,21 @@ def get_vmc_gto_func(mf, params_corr, cusp_scheme="Quady2025", gr_scheme="scheme
     print("Begin time: {}".format(timestamp_init))
     return VMCDriverGTO(mf, params_corr, params_cusp, prefix, timestamp_init,
                         precision=precision, proposal=proposal, specialize=specialize,
-                        jastrow_config=jastrow_config)
+                        jastrow_config=jastrow_config, trial=trial)
 
 
 class VMCDriverGTO:
     """Runs VMC sampling of one trial wavefunction (``vmc_gto.py:672-1617``)."""
 
     def __init__(self, mf, params_corr, params_cusp, prefix, timestamp_init,
-                 precision="fp64", proposal="plain", specialize=True, jastrow_config=None):
+                 precision="fp64", proposal="plain", specialize=True, jastrow_config=None,
+                 trial=None):
         self.mf = mf
         self.params_corr = params_corr
         self.params_cusp = params_cusp
-        self.system = build_system(mf, params_corr, params_cusp, jastrow_config)
+        self.system = build_system(mf, params_corr, params_cusp, jastrow_config, trial)
         self.ctx = GTOContext(self.system)
-        if specialize:
+        if specialize and trial is None:
             try:
                 self.ctx.specialize()
             except NotImplementedError as e:

@@ -12,6 +12,7 @@ walkers, line by line from:
 * ``OmegaQMC/psi/gto.py:1101-1214``  AO/MO value-gradient-Laplacian
 * ``OmegaQMC/psi/gto.py:728-778``    Slater assembly (inverse, Gamma, lap)
 * ``OmegaQMC/psi/gto.py:1278-1290``  log|det| of the up and down blocks
+* ``OmegaQMC/psi/gto.py:1319-1480``  multi-determinant Slater part
 * ``OmegaQMC/psi/gto.py:1493-1649``  Padé J1/J2 value and VGL
 * ``OmegaQMC/psi/gto.py:243-604, 1933-2196``  J3_eeI three-body Jastrow
 * ``OmegaQMC/psi/gto.py:2220-2254``  log|psi| = log|det| + J
@@ -224,7 +225,10 @@ def mo_vgl(system, X):
 # Slater determinant
 # ---------------------------------------------------------------------------
 def log_slater(system, X):
-    """log|det up| + log|det down| (``gto.py:1278-1290``)."""
+    """log|det up| + log|det down| (``gto.py:1278-1290``), or the
+    multi-determinant log|sum_d c_d D_up D_dn| with a trial."""
+    if getattr(system, "md", None) is not None:
+        return multidet_assemble(system, X)[0]
     mo = mo_value(system, X)
     _, la = np.linalg.slogdet(mo[:, 0::2, :])
     _, lb = np.linalg.slogdet(mo[:, 1::2, :])
@@ -249,6 +253,48 @@ def slater_assemble(mo_val, mo_grad, mo_lap):
         grad[:, off::2] = Gam
         lap[:, off::2] = lp
     return logv, grad, lap
+
+
+def multidet_assemble(system, X):
+    """(log|psi_S|, grad_e, lap_e) of a multi-determinant Slater part,
+    restating ``log_slater_multidet`` and ``log_slater_multidet_analytic``
+    (gto.py:1319-1480): per term the up and down slogdet, inverses, Gamma
+    and ell; signed log-sum-exp weights w_d summing to 1; grad = sum_d w_d
+    Gamma_d, lap = sum_d w_d (|Gamma_d|^2 + ell_d) - |grad|^2."""
+    md = system.md
+    C = md["C"]
+    v, g, l = ao_vgl(system, X)
+    mv = v @ C
+    mg = np.einsum("...ax,am->...mx", g, C)
+    ml = l @ C
+    W, n_e, _ = X.shape
+    nd = len(md["ci"])
+    logs = np.zeros((W, nd))
+    phase = np.zeros((W, nd))
+    gam = np.zeros((W, nd, n_e, 3))
+    sec = np.zeros((W, nd, n_e))
+    for d in range(nd):
+        for off, occ in ((0, md["occ_up"][d]), (1, md["occ_dn"][d])):
+            S = mv[:, off::2][:, :, occ]
+            G = mg[:, off::2][:, :, occ, :]
+            L = ml[:, off::2][:, :, occ]
+            sgn, ld = np.linalg.slogdet(S)
+            A = np.linalg.inv(S)
+            Gam = np.einsum("wji,wijx->wix", A, G)
+            ell = np.einsum("wji,wij->wi", A, L) - np.sum(Gam * Gam, axis=-1)
+            logs[:, d] += ld
+            phase[:, d] = (sgn if off == 0 else phase[:, d] * sgn)
+            gam[:, d, off::2] = Gam
+            sec[:, d, off::2] = np.sum(Gam * Gam, axis=-1) + ell
+        phase[:, d] *= np.sign(md["ci"][d])
+    contrib = np.log(np.abs(md["ci"]))[None, :] + logs
+    lmax = np.max(contrib, axis=1)
+    shifted = phase * np.exp(contrib - lmax[:, None])
+    total = np.sum(shifted, axis=1)
+    w = shifted / total[:, None]
+    grad = np.einsum("wd,wdix->wix", w, gam)
+    lap = np.einsum("wd,wdi->wi", w, sec) - np.sum(grad * grad, axis=-1)
+    return np.log(np.abs(total)) + lmax, grad, lap
 
 
 # ---------------------------------------------------------------------------
@@ -612,8 +658,11 @@ def evaluate(system, X):
     ``local_energy_ke`` (``gto.py:2506-2579``) and ``_local_energy_batch``
     (``OmegaQMC/vmc_gto.py:801-812``)."""
     X = np.asarray(X, dtype=np.float64)
-    mv, mg, ml = mo_vgl(system, X)
-    _, gs, ls = slater_assemble(mv, mg, ml)
+    if getattr(system, "md", None) is not None:
+        _, gs, ls = multidet_assemble(system, X)
+    else:
+        mv, mg, ml = mo_vgl(system, X)
+        _, gs, ls = slater_assemble(mv, mg, ml)
     gj, lj = jastrow_vgl(system, X)
     grad = gs + gj
     lap = ls + lj

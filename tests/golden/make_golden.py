@@ -219,6 +219,15 @@ CASES = {
                                        _j3_params(("Li", "H"), 8, seed=17).items()
                                        if k != "unlike+H"}},
                1.0, 16),
+    "h2o_md": (lambda: M.named_system("H2O"), False,
+               lambda mol: {"J1_pade": {"O": np.array(0.9), "H": np.array(0.4)},
+                            "J2_pade": {"like": np.array([0.25, 0.6]),
+                                        "unlike": np.array([0.5, 0.4])}},
+               0.6, 24),
+    "lih_md_uhf": (lambda: M.named_system("LiH"), True,
+                   lambda mol: {"J2_pade": {"like": np.array([0.25, 0.8]),
+                                            "unlike": np.array([0.5, 0.8])}},
+                   1.0, 16),
 }
 
 # B-spline cutoffs and J3 orders per case (jastrow_config of _PsiGTO,
@@ -228,6 +237,37 @@ JASTROW_CONFIG = {
                     "J1": {"O": {"r_cut": 3.5}, "H": {"r_cut": 3.0}}},
     "lih_j3": {"J3": {"N_eI": 2, "N_ee": 2, "r_cut": 4.0}},
 }
+
+# multi-determinant trials (trial dicts of OmegaQMC/psi/trial.py): a
+# restricted expansion on H2O (6 terms, 8 orbitals) and a UHF expansion on
+# cusp-corrected LiH (alpha and beta orbitals differ)
+def _trial_h2o(mf, seed):
+    rng = np.random.default_rng(seed)
+    C = np.asarray(mf.mo_coeff)
+    mo = np.concatenate([C, rng.normal(size=(C.shape[0], 3)) * 0.3], axis=1)
+    g, s1, s2, s3 = [0, 1, 2, 3, 4], [0, 1, 2, 3, 5], [0, 1, 2, 4, 6], [0, 1, 2, 3, 7]
+    up = [g, s1, g, s2, s1, g]
+    dn = [g, g, s1, s2, s2, s3]
+    ci = [0.95, -0.12, -0.12, 0.08, 0.05, 0.03]
+    return {"mo_coeff": mo, "ci_coeffs": np.array(ci), "occ_up": np.array(up),
+            "occ_dn": np.array(dn), "ndet": len(ci)}
+
+
+def _trial_lih_uhf(mf, seed):
+    rng = np.random.default_rng(seed)
+    C = np.asarray(mf.mo_coeff)
+    n = C.shape[0]
+    a = np.concatenate([C, rng.normal(size=(n, 2)) * 0.3], axis=1)
+    b = np.concatenate([C + rng.normal(size=C.shape) * 0.02, rng.normal(size=(n, 2)) * 0.3],
+                       axis=1)
+    up = [[0, 1], [0, 2], [0, 3], [0, 1]]
+    dn = [[0, 1], [0, 1], [0, 2], [1, 3]]
+    ci = [0.9, 0.2, -0.15, 0.1]
+    return {"mo_coeff": np.stack([a, b]), "ci_coeffs": np.array(ci), "occ_up": np.array(up),
+            "occ_dn": np.array(dn), "ndet": len(ci)}
+
+
+TRIALS = {"h2o_md": _trial_h2o, "lih_md_uhf": _trial_lih_uhf}
 
 # (N_eI, N_ee, r_cut) of the stored J3_eeI constraint maps
 EEI_MAPS = [(3, 3, 5.0), (2, 2, 4.0), (2, 3, 6.0), (4, 3, 5.0), (1, 2, 3.0)]
@@ -242,9 +282,17 @@ def run_case(gto, name, seed):
     X = _walkers(mol, nw, sigma, seed + 101)
     rmf = _RefMF(mf)
     jcfg = JASTROW_CONFIG.get(name)
+    trial = TRIALS[name](mf, seed + 31) if name in TRIALS else None
+    ref_trial = None
+    if trial is not None:
+        ref_trial = {"mo_coeff": trial["mo_coeff"],
+                     "ci_coeffs": torch.tensor(trial["ci_coeffs"]),
+                     "occ_up": torch.tensor(trial["occ_up"], dtype=torch.int64),
+                     "occ_dn": torch.tensor(trial["occ_dn"], dtype=torch.int64),
+                     "ndet": trial["ndet"]}
     obj = gto._PsiGTO(rmf, params_cusp=(
         {s: {"q0": torch.tensor(v["q0"]), "coeff": torch.tensor(v["coeff"])}
-         for s, v in pcusp.items()} if cusp else None), jastrow_config=jcfg)
+         for s, v in pcusp.items()} if cusp else None), trial=ref_trial, jastrow_config=jcfg)
     nuc = torch.tensor(mol.atom_coords())
     tp = {}
     for k, v in params.items():
@@ -302,6 +350,9 @@ def run_case(gto, name, seed):
     res.update(X=X, mo_coeff=mf.mo_coeff, mo_occ=mf.mo_occ, e_nn=e_nn,
                e_ke_hessian=np.array(ke_h),
                spec=np.array(json.dumps(_to_json(spec))))
+    if trial is not None:
+        res.update(trial_mo_coeff=trial["mo_coeff"], trial_ci=trial["ci_coeffs"],
+                   trial_occ_up=trial["occ_up"], trial_occ_dn=trial["occ_dn"])
     return res
 
 

@@ -49,10 +49,18 @@ def load_golden(name):
     return mf, params, cusp, d
 
 
+def golden_trial(d):
+    """The multi-determinant trial dict stored with a golden case, or None."""
+    if "trial_ci" not in d:
+        return None
+    return {"mo_coeff": d["trial_mo_coeff"], "ci_coeffs": d["trial_ci"],
+            "occ_up": d["trial_occ_up"], "occ_dn": d["trial_occ_dn"]}
+
+
 def golden_system(name):
     mf, params, cusp, d = load_golden(name)
     spec = json.loads(str(d["spec"]))
-    return build_system(mf, params, cusp, spec.get("jastrow_config")), d
+    return build_system(mf, params, cusp, spec.get("jastrow_config"), golden_trial(d)), d
 
 
 def seeded_walkers(system, n, sigma, seed):
