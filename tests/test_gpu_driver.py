@@ -67,5 +67,8 @@ def test_get_psi_fun_error_conventions():
     with pytest.warns(UserWarning, match="a is fixed at -Z"):
         log_psi(x, mf.mol.atom_coords(), {"J1_pade": {"O": np.array([-0.05, 0.9]),
                                                      "H": np.array(0.4)}})
-    with pytest.raises(NotImplementedError):
+    # without jastrow_config every element gets the 10-bohr one-body spline,
+    # and an element missing from J1_bspline raises KeyError as in the
+    # reference's J1_bspline_fn (gto.py:1752-1756)
+    with pytest.raises(KeyError):
         log_psi(x, mf.mol.atom_coords(), {"J1_bspline": {"O": np.zeros(4)}})
