@@ -110,8 +110,15 @@ struct Gen {
     return s;
   }
 
-  // declare R<k> (and Rp<k>, Rl<k>) of type ty and accumulate group g
-  void radial(int g, bool vgl, const std::string& ty, const char* r2) {
+  // Primitive p of group g is tight when its own split radius 25 / alpha
+  // is within the group's (the largest over its tight primitives).
+  bool tight(int g, int p) const {
+    return SP.r2[g] > 0.0 && S.alpha[S.g_off[g] + p] * SP.r2[g] >= 25.0 * (1.0 - 1e-12);
+  }
+
+  // declare R<k> (and Rp<k>, Rl<k>) of type ty and accumulate group g's
+  // primitives (sel 0: all, 1: tight only, 2: all but the tight ones)
+  void radial(int g, bool vgl, const std::string& ty, const char* r2, int sel = 0) {
     const int np = S.g_n[g], nc = S.g_ncol[g], off = S.g_off[g], sh0 = S.g_shell0[g];
     for (int k = 0; k < nc; ++k) {
       const std::string ks = std::to_string(k);
@@ -121,6 +128,7 @@ struct Gen {
     }
     const std::string ex = (ty == "double") ? "exp" : "oq_exp<T>";
     for (int p = 0; p < np; ++p) {
+      if ((sel == 1 && !tight(g, p)) || (sel == 2 && tight(g, p))) continue;
       const std::string al = "((" + ty + ")" + num(S.alpha[off + p]) + ")";
       add("      { const " + ty + " e = " + ex + "(-" + al + " * " + r2 + ");\n");
       if (vgl) {
@@ -230,9 +238,10 @@ struct Gen {
             angular(g, k, false, "R" + ks, "", "");
           }
         } else {
-          // Radial factors: cusp groups always in FP64; groups with tight
-          // exponents in FP64 within their split radius, else in the working
-          // precision; other groups in the working precision only.
+          // Radial factors: cusp groups always in FP64; the tight exponents
+          // of a split group in FP64 within its split radius (the group's
+          // other exponents and every exponent outside the radius in the
+          // working precision); other groups in the working precision.
           bool cusp = false;
           for (int k = 0; k < nc; ++k) cusp = cusp || (s_shell && S.s_cusp[sh0 + k]);
           const bool split = SP.r2[g] > 0.0;
@@ -266,11 +275,30 @@ struct Gen {
           if (cusp) {
             fp64_inline();
           } else if (split) {
-            add("    if (sizeof(T) == 8 || r2d < " + num(SP.r2[g]) + ") {\n");
-            fp64_inline();
-            add("    } else {\n");
-            working();
-            add("    }\n");
+            // the group's other primitives in the working precision for
+            // every lane; the tight ones in FP64 within the split radius
+            add("      {\n");
+            radial(g, true, "T", "r2", 2);
+            for (int k = 0; k < nc; ++k) {
+              const std::string ks = std::to_string(k);
+              add("      RT" + ks + " = R" + ks + "; RpT" + ks + " = Rp" + ks + "; RlT" + ks +
+                  " = Rl" + ks + ";\n");
+            }
+            add("      }\n    if (sizeof(T) == 8 || r2d < " + num(SP.r2[g]) + ") {\n      {\n");
+            radial(g, true, "double", "r2d", 1);
+            for (int k = 0; k < nc; ++k) {
+              const std::string ks = std::to_string(k);
+              add("      RT" + ks + " += (T)R" + ks + "; RpT" + ks + " += (T)Rp" + ks + "; RlT" +
+                  ks + " += (T)Rl" + ks + ";\n");
+            }
+            add("      }\n    } else {\n      {\n");
+            radial(g, true, "T", "r2", 1);
+            for (int k = 0; k < nc; ++k) {
+              const std::string ks = std::to_string(k);
+              add("      RT" + ks + " += R" + ks + "; RpT" + ks + " += Rp" + ks + "; RlT" + ks +
+                  " += Rl" + ks + ";\n");
+            }
+            add("      }\n    }\n");
           } else {
             working();
           }
