@@ -108,6 +108,17 @@ typedef struct {
   const int* j3_type;                      /* natm: type of each atom, -1 none */
   const int* j3_on;                        /* ntype x 2: like / unlike block present */
   const double* j3_gamma;                  /* ntype x 2 x (n_ei+1)^2 x (n_ee+1) */
+  /* Quintic radial splines of the AO transform (psi/gto.py:141-240): table
+   * t holds knots in s = r^2 (spl_npts, knot 0 at s = 0, then a log grid
+   * from spl_smin) and spl_npts - 1 segments of 6 power-form coefficients
+   * (highest power first).  spl_shell: per shell (descriptor order) its
+   * table, -1 for the analytic radial. */
+  int has_spl;
+  int spl_npts, spl_ntab;
+  double spl_smin;
+  const int* spl_shell;
+  const double* spl_knots;                 /* ntab x npts */
+  const double* spl_coef;                  /* ntab x (npts - 1) x 6 */
 } oqmc_system_desc;
 
 /* Library version string. */

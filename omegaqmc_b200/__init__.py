@@ -33,11 +33,14 @@ def __getattr__(name):
 
 
 def generate_molecular_orbitals(astr, units="Bohr", basis="cc-pvdz-shaped", spin=0,
-                                charge=0, **kw):
+                                charge=0, ao_splines=None, **kw):
     """RHF mean-field object for ``astr`` (``OmegaQMC/vmc_gto.py:217-452`` runs
     PySCF; here the package's own RHF).  ``basis`` is a PySCF-format dict
     ``{element: [[am, [alpha, c...], ...], ...]}`` or one of the generated
-    sets ``"cc-pvdz-shaped"`` / ``"sto-3g"`` (H only)."""
+    sets ``"cc-pvdz-shaped"`` / ``"sto-3g"`` (H only).  ``ao_splines``
+    (True or a dict of grid options) switches on the quintic radial-spline
+    AO transform, stored on ``mf.mol.ao_radial_transform`` as in the
+    reference (``vmc_gto.py:278-290, 415``)."""
     from . import molecules as M
     from .rhf import run_rhf
     if spin != 0:
@@ -53,4 +56,5 @@ def generate_molecular_orbitals(astr, units="Bohr", basis="cc-pvdz-shaped", spin
         else:
             raise ValueError(f"unknown basis {basis!r}; pass a PySCF-format dict")
     mol = Mole(astr, basis, unit=units, charge=charge, basis_name="gen")
+    mol.ao_radial_transform = ao_splines
     return run_rhf(mol, **kw)

@@ -51,6 +51,8 @@ class SystemDesc(ctypes.Structure):
         ("bs1_rcut", P_double), ("bs1_coef", P_double),
         ("has_j3", c_int), ("j3_n_ei", c_int), ("j3_n_ee", c_int), ("j3_ntype", c_int),
         ("j3_rcut", c_double), ("j3_type", P_int), ("j3_on", P_int), ("j3_gamma", P_double),
+        ("has_spl", c_int), ("spl_npts", c_int), ("spl_ntab", c_int), ("spl_smin", c_double),
+        ("spl_shell", P_int), ("spl_knots", P_double), ("spl_coef", P_double),
     ]
 
 

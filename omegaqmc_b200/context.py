@@ -120,6 +120,21 @@ def pack_system(system: System):
         d.j3_n_ee = int(j3["n_ee"])
         d.j3_ntype = len(j3["elements"])
         d.j3_rcut = float(j3["r_cut"])
+    spl = getattr(system, "spl", None)
+    if spl is not None and spl["tables"]:
+        index = {id(sh): i for i, sh in enumerate(system.shells)}
+        ids = sorted(spl["tables"])
+        tab_of = {i: t for t, i in enumerate(ids)}
+        arr["spl_shell"] = np.array([tab_of.get(index[id(sh)], -1) for sh in order],
+                                    dtype=np.int32)
+        arr["spl_knots"] = np.ascontiguousarray(
+            np.stack([spl["tables"][i][0] for i in ids]), dtype=np.float64).ravel()
+        arr["spl_coef"] = np.ascontiguousarray(
+            np.stack([spl["tables"][i][1] for i in ids]), dtype=np.float64).ravel()
+        d.has_spl = 1
+        d.spl_npts = int(spl["npts"])
+        d.spl_ntab = len(ids)
+        d.spl_smin = float(spl["smin"])
     for k, v in arr.items():
         ct = ctypes.c_int if v.dtype == np.int32 else ctypes.c_double
         setattr(d, k, v.ctypes.data_as(ctypes.POINTER(ct)))

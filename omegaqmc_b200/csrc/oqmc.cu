@@ -245,6 +245,23 @@ static int fill_system(const oqmc_system_desc* d, OqSystem& S) {
       S.j3_type[i] = t;
     }
   }
+  for (int i = 0; i < OQ_MAX_SHELL; ++i) S.s_spl[i] = -1;
+  if (d->has_spl) {
+    if (d->spl_npts < 3 || d->spl_ntab < 1 || !(d->spl_smin > 0.0) || !d->spl_shell ||
+        !d->spl_knots || !d->spl_coef)
+      return set_err(nullptr, OQ_ERR_ARG, "bad radial spline table%s");
+    S.has_spl = 1;
+    S.spl_npts = d->spl_npts;
+    S.spl_smin = d->spl_smin;
+    S.spl_knots = d->spl_knots;   // host tables; oqmc_create points them at device copies
+    S.spl_coef = d->spl_coef;
+    for (int i = 0; i < S.nshell; ++i) {
+      const int t = d->spl_shell[i];
+      if (t < -1 || t >= d->spl_ntab || (t >= 0 && S.s_cusp[i]))
+        return set_err(nullptr, OQ_ERR_ARG, "bad radial spline shell table%s");
+      S.s_spl[i] = t;
+    }
+  }
   build_harm_table(S.harm);
   return OQ_OK;
 }
@@ -355,6 +372,18 @@ extern "C" int oqmc_create(oqmc_ctx** out, const oqmc_system_desc* d) {
                                         cudaMemcpyHostToDevice) : e;
     S.j3_gamma = ctx->d_j3;
   }
+  if (S.has_spl) {
+    const size_t nk = (size_t)d->spl_ntab * d->spl_npts;
+    const size_t nc = (size_t)d->spl_ntab * (d->spl_npts - 1) * 6;
+    e = (e == cudaSuccess) ? cudaMalloc(&ctx->d_spl_knots, sizeof(double) * nk) : e;
+    e = (e == cudaSuccess) ? cudaMalloc(&ctx->d_spl_coef, sizeof(double) * nc) : e;
+    e = (e == cudaSuccess) ? cudaMemcpy(ctx->d_spl_knots, d->spl_knots, sizeof(double) * nk,
+                                        cudaMemcpyHostToDevice) : e;
+    e = (e == cudaSuccess) ? cudaMemcpy(ctx->d_spl_coef, d->spl_coef, sizeof(double) * nc,
+                                        cudaMemcpyHostToDevice) : e;
+    S.spl_knots = ctx->d_spl_knots;
+    S.spl_coef = ctx->d_spl_coef;
+  }
   e = (e == cudaSuccess) ? cudaMemcpy(ctx->d_sys, &S, sizeof(OqSystem), cudaMemcpyHostToDevice) : e;
   e = (e == cudaSuccess) ? cudaMemcpy(ctx->d_split, &ctx->hsplit, sizeof(OqSplit), cudaMemcpyHostToDevice) : e;
   e = (e == cudaSuccess) ? cudaMemcpy(ctx->d_C64, d->C, sizeof(double) * c32.size(), cudaMemcpyHostToDevice) : e;
@@ -381,6 +410,8 @@ int oqmc_destroy(oqmc_ctx* ctx) {
   cudaFree(ctx->d_C32);
   cudaFree(ctx->d_flags);
   cudaFree(ctx->d_j3);
+  cudaFree(ctx->d_spl_knots);
+  cudaFree(ctx->d_spl_coef);
   md_free(ctx);
   delete ctx;
   return OQ_OK;
@@ -824,6 +855,9 @@ int oqmc_use_tensor_cores(oqmc_ctx* ctx, int enable) {
   if (ctx && enable && ctx->md)
     return set_err(ctx, OQ_ERR_UNSUPPORTED,
                    "the tensor-core local energy supports single determinants only%s");
+  if (ctx && enable && ctx->hsys.has_spl)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED,
+                   "the tensor-core local energy uses analytic radial functions only%s");
   if (ctx && enable && (ctx->hsys.has_bs1 || ctx->hsys.has_bs2 || ctx->hsys.has_j3))
     return set_err(ctx, OQ_ERR_UNSUPPORTED,
                    "the tensor-core local energy supports Pade Jastrow terms only%s");
@@ -860,6 +894,10 @@ int oqmc_specialize(oqmc_ctx* ctx, int enable) {
   oq_spec_destroy(ctx->spec);
   ctx->spec = nullptr;
   if (!enable) return OQ_OK;
+  if (ctx->hsys.has_spl)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED,
+                   "specialised kernels use analytic radial functions; the radial-spline "
+                   "transform runs on the table-driven kernels%s");
   std::string err;
   OqSpecModule* m = nullptr;
   if (oq_spec_build(ctx->hsys, ctx->hsplit, ctx->h_C, ctx->nocc, &m, &err) != 0)

@@ -29,6 +29,14 @@ __device__ __forceinline__ void oq_mo_val(const OqSystem& S, const TC* __restric
       for (int k = 0; k < OQ_MAX_COL; ++k)
         if (k < ncol) R[k] += S.norm[S.s_norm[sh0 + k] + p] * e;
     }
+    if (S.has_spl) {
+#pragma unroll
+      for (int k = 0; k < OQ_MAX_COL; ++k)
+        if (k < ncol && S.s_spl[sh0 + k] >= 0) {
+          double gp, gpp;
+          oq_spline_gdd(S, S.s_spl[sh0 + k], r2, R[k], gp, gpp);
+        }
+    }
     const int am = S.g_am[g];
 #pragma unroll
     for (int k = 0; k < OQ_MAX_COL; ++k) {
@@ -97,6 +105,18 @@ __device__ __forceinline__ void oq_mo_vgl(const OqSystem& S, const TC* __restric
           R[k] += n * e;
           Rp[k] += n * fp;
           Rl[k] += n * fl;
+        }
+    }
+    if (S.has_spl) {
+      // spline triple (g, 2 g', 6 g' + 4 s g''), _radial_vgl_spline (gto.py:226-240)
+#pragma unroll
+      for (int k = 0; k < OQ_MAX_COL; ++k)
+        if (k < ncol && S.s_spl[sh0 + k] >= 0) {
+          double gv, gp, gpp;
+          oq_spline_gdd(S, S.s_spl[sh0 + k], r2, gv, gp, gpp);
+          R[k] = gv;
+          Rp[k] = 2.0 * gp;
+          Rl[k] = 6.0 * gp + 4.0 * r2 * gpp;
         }
     }
     const int am = S.g_am[g];

@@ -303,6 +303,10 @@ int oqmc_batch_bind(oqmc_batch* b, const oqmc_batch_system* sys) {
         (in.cap > 0 && !in.sums) || (in.proposal != 0 && in.proposal != 1) ||
         (in.proposal == 1 && !(in.scale_r0 > 0.0 && in.scale_fmin > 0.0)))
       return berr(b, OQ_ERR_ARG, "bad system entry " + std::to_string(k));
+    if (c->hsys.has_spl)
+      return berr(b, OQ_ERR_UNSUPPORTED,
+                  "system " + std::to_string(k) + " uses the radial-spline AO transform; the "
+                  "batched kernel evaluates analytic radial functions");
     if (c->md)
       return berr(b, OQ_ERR_UNSUPPORTED,
                   "system " + std::to_string(k) + " has a multi-determinant trial; the "

@@ -73,6 +73,12 @@ struct OqSystem {
   const double* j3_gamma;
   int j3_type[OQ_MAX_NUC];           // element type of each atom, -1: none
   int j3_on[OQ_MAX_BST][2];          // block present
+  // quintic radial splines in s = r^2 (tables in device memory)
+  int has_spl, spl_npts, spl_pad0, spl_pad1;
+  double spl_smin, spl_pad2;
+  const double* spl_knots;           // [table][npts]
+  const double* spl_coef;            // [table][npts - 1][6]
+  int s_spl[OQ_MAX_SHELL];           // table of each shell, -1: analytic radial
   OqHarmTable harm;
 };
 
@@ -228,6 +234,36 @@ __device__ __forceinline__ void oq_bs_vgl(const double* c, int n, T dinv, T rcut
                 (-(T)18 * t + (T)6) * c2 + (T)6 * t * c3);
   up_r = d1 * rinv;
   lap = d2 + (T)2 * up_r;
+}
+
+// ---------------------------------------------------------------------------
+// Quintic radial spline of table id at s = r^2 (_locate_and_horner,
+// psi/gto.py:200-217): g(s), g'(s), g''(s); zero from the last knot on.  The
+// segment is the one searchsorted(knots, s, 'right') - 1 picks: a first guess
+// from the log grid, then corrected against the knots.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void oq_spline_gdd(const OqSystem& S, int id, double s, double& g,
+                                              double& gp, double& gpp) {
+  const int n = S.spl_npts;
+  const double* kn = S.spl_knots + (size_t)id * n;
+  const double send = kn[n - 1];
+  if (!(s < send)) {
+    g = gp = gpp = 0.0;
+    return;
+  }
+  int j = 0;
+  if (s >= kn[1]) {
+    const double f = log(s / S.spl_smin) / log(send / S.spl_smin);
+    j = 1 + (int)floor(f * (double)(n - 2));
+    j = j < 1 ? 1 : (j > n - 2 ? n - 2 : j);
+    while (j < n - 2 && kn[j + 1] <= s) ++j;
+    while (j > 0 && kn[j] > s) --j;
+  }
+  const double* c = S.spl_coef + ((size_t)id * (n - 1) + j) * 6;
+  const double d = s - kn[j];
+  g = ((((c[0] * d + c[1]) * d + c[2]) * d + c[3]) * d + c[4]) * d + c[5];
+  gp = (((5.0 * c[0] * d + 4.0 * c[1]) * d + 3.0 * c[2]) * d + 2.0 * c[3]) * d + c[4];
+  gpp = ((20.0 * c[0] * d + 12.0 * c[1]) * d + 6.0 * c[2]) * d + 2.0 * c[3];
 }
 
 // ---------------------------------------------------------------------------

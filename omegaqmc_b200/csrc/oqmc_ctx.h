@@ -28,6 +28,8 @@ struct oqmc_ctx {
   float* d_C32;
   unsigned* d_flags;
   double* d_j3;            // three-body Jastrow gamma blocks (or null)
+  double* d_spl_knots;     // radial spline tables (or null)
+  double* d_spl_coef;
   double tight_alpha;
   int proposal;           // 0 fixed-width Gaussian, 1 nucleus-scaled width
   OqSpecModule* spec;     // run-time specialised kernels, or null

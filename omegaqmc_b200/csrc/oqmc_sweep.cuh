@@ -56,6 +56,15 @@ __device__ __forceinline__ void oq_mo_val_t(const OqSystem& S, const OqSplit& SP
       for (int k = 0; k < OQ_MAX_COL; ++k)
         if (k < ncol) R[k] += (T)S.norm[S.s_norm[sh0 + k] + p] * e;
     }
+    if (S.has_spl) {
+#pragma unroll
+      for (int k = 0; k < OQ_MAX_COL; ++k)
+        if (k < ncol && S.s_spl[sh0 + k] >= 0) {
+          double gv, gp, gpp;
+          oq_spline_gdd(S, S.s_spl[sh0 + k], r2d, gv, gp, gpp);
+          R[k] = (T)gv;
+        }
+    }
     const int am = S.g_am[g];
 #pragma unroll
     for (int k = 0; k < OQ_MAX_COL; ++k) {
@@ -153,6 +162,17 @@ __device__ __forceinline__ void oq_mo_vgl_t(const OqSystem& S, const OqSplit& SP
             R[k] += n * e; Rp[k] += n * fp; Rl[k] += n * fl;
           }
       }
+    }
+    if (S.has_spl) {
+#pragma unroll
+      for (int k = 0; k < OQ_MAX_COL; ++k)
+        if (k < ncol && S.s_spl[sh0 + k] >= 0) {
+          double gv, gp, gpp;
+          oq_spline_gdd(S, S.s_spl[sh0 + k], r2d, gv, gp, gpp);
+          R[k] = (T)gv;
+          Rp[k] = (T)(2.0 * gp);
+          Rl[k] = (T)(6.0 * gp + 4.0 * r2d * gpp);
+        }
     }
     const int am = S.g_am[g];
 #pragma unroll

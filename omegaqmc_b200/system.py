@@ -595,6 +595,7 @@ class System:
     bs1: object = None         # B-spline J1: per atom (coefs, r_cut) or None
     j3: object = None          # J3_eeI tables (see :func:`parse_j3`) or None
     md: object = None          # multi-determinant trial (see :func:`parse_trial`) or None
+    spl: object = None         # quintic radial splines (see :func:`ao_spline_tables`) or None
 
     @property
     def natm(self):
@@ -644,6 +645,62 @@ class System:
         """Exponentials per position as the reference evaluates them
         (one set per contraction column)."""
         return sum(sh.nprim for sh in self.shells)
+
+
+def build_quintic_radial_spline(alpha, norm, smin=1.0e-6, tol=1.0e-7, npts=1001,
+                                rmax_cap=100.0):
+    """Quintic Hermite spline of a contracted radial g(s) = sum_p norm_p
+    exp(-alpha_p s) in s = r^2 (QMCPACK's numerical-orbital transform,
+    ``_build_quintic_radial_spline``, gto.py:141-198).
+
+    Knots: s = 0 and a log grid from smin to smax = rmax^2, rmax the last
+    radius on a 20001-point scan of [0, rmax_cap] where |g| > tol.  Each
+    segment is the quintic matching (g, g', g'') at both ends (scipy
+    ``BPoly.from_derivatives``, converted to power form ``PPoly``).
+    Returns ``(knots (npts,), coefs (npts - 1, 6))``, coefficients of
+    segment j in powers of (s - knots[j]), highest first."""
+    from scipy.interpolate import BPoly, PPoly
+    a = np.asarray(alpha, dtype=np.float64)
+    c = np.asarray(norm, dtype=np.float64)
+
+    def derivs(sv):
+        sv = np.asarray(sv, dtype=np.float64)
+        e = np.exp(-a[None, :] * sv[:, None])
+        return np.stack([np.sum(c[None, :] * e, axis=1),
+                         np.sum((-a * c)[None, :] * e, axis=1),
+                         np.sum((a * a * c)[None, :] * e, axis=1)], axis=1)
+
+    r_scan = np.linspace(0.0, rmax_cap, 20001)
+    big = np.abs(derivs(r_scan ** 2)[:, 0]) > tol
+    rmax = float(r_scan[np.max(np.nonzero(big))]) if big.any() else 1.0
+    smax = max(rmax ** 2, 100.0 * smin)
+    grid = np.concatenate([[0.0], np.logspace(np.log10(smin), np.log10(smax), npts - 1)])
+    pp = PPoly.from_bernstein_basis(BPoly.from_derivatives(grid, derivs(grid)))
+    return np.asarray(pp.x, dtype=np.float64), np.ascontiguousarray(np.asarray(pp.c).T)
+
+
+def ao_spline_tables(shells, transform):
+    """Spline tables of the shells the AO radial transform replaces (every
+    shell but the cusp-corrected s ones, gto.py:905-936), or None when
+    ``transform`` is falsy.  ``transform`` True uses the default grid; a
+    dict overrides ``smin``, ``tol``, ``npts``, ``rmax_cap``.
+
+    Returns ``{"npts", "smin", "tables": {shell index: (knots, coefs)}}``."""
+    if not transform:
+        return None
+    kw = dict(transform) if isinstance(transform, dict) else {}
+    unknown = set(kw) - {"smin", "tol", "npts", "rmax_cap"}
+    if unknown:
+        raise TypeError(f"unknown AO spline options {sorted(unknown)}")
+    npts = int(kw.get("npts", 1001))
+    if npts < 3:
+        raise ValueError("AO spline npts must be at least 3")
+    tables = {}
+    for i, sh in enumerate(shells):
+        if sh.is_cusp:
+            continue
+        tables[i] = build_quintic_radial_spline(sh.alpha, sh.norm, **kw)
+    return {"npts": npts, "smin": float(kw.get("smin", 1.0e-6)), "tables": tables, "cfg": kw}
 
 
 def parse_trial(trial, n_up, n_dn):
@@ -743,7 +800,9 @@ def build_system(mf, params_corr=None, params_cusp=None, jastrow_config=None, tr
         mol, cusp)
     bs2, bs1 = parse_bspline(pc, mol, cusp, jastrow_config)
     j3 = parse_j3(pc, mol, jastrow_config)
+    spl = ao_spline_tables(shells, getattr(mol, "ao_radial_transform", None))
     return System(nuc=mol.atom_coords(unit="Bohr"), Z=Z, shells=shells, C=C,
                   n_up=n_up, n_dn=n_dn, has_j1=has_j1, j1=j1, has_j2=has_j2,
                   j2=j2, cusp=cusp, cusp_rc=rc, cusp_q0=q0,
-                  cusp_coeff=coeff, symbols=mol.elements, bs2=bs2, bs1=bs1, j3=j3, md=md)
+                  cusp_coeff=coeff, symbols=mol.elements, bs2=bs2, bs1=bs1, j3=j3, md=md,
+                  spl=spl)

@@ -13,6 +13,7 @@ walkers, line by line from:
 * ``OmegaQMC/psi/gto.py:728-778``    Slater assembly (inverse, Gamma, lap)
 * ``OmegaQMC/psi/gto.py:1278-1290``  log|det| of the up and down blocks
 * ``OmegaQMC/psi/gto.py:1319-1480``  multi-determinant Slater part
+* ``OmegaQMC/psi/gto.py:141-240``    quintic radial splines of the AO transform
 * ``OmegaQMC/psi/gto.py:1493-1649``  Padé J1/J2 value and VGL
 * ``OmegaQMC/psi/gto.py:243-604, 1933-2196``  J3_eeI three-body Jastrow
 * ``OmegaQMC/psi/gto.py:2220-2254``  log|psi| = log|det| + J
@@ -155,6 +156,59 @@ def cusp_s_vgl(r, rc, Z, R, Rp_r, Rlap, q0, coeff):
 # ---------------------------------------------------------------------------
 # AO evaluation
 # ---------------------------------------------------------------------------
+# ---------------------------------------------------------------------------
+# Quintic radial splines of the AO transform (gto.py:141-240)
+# ---------------------------------------------------------------------------
+def quintic_radial_spline(alpha, norm, smin=1.0e-6, tol=1.0e-7, npts=1001, rmax_cap=100.0):
+    """(knots, coefs) of ``_build_quintic_radial_spline`` (gto.py:141-198):
+    Hermite quintics matching g, g', g'' of g(s) = sum_p norm_p
+    exp(-alpha_p s) at s = 0 and on a log grid up to the tol cutoff."""
+    from scipy.interpolate import BPoly, PPoly
+    a = np.asarray(alpha, dtype=np.float64)
+    c = np.asarray(norm, dtype=np.float64)
+
+    def ders(sv):
+        e = np.exp(-a[None, :] * np.asarray(sv, dtype=np.float64)[:, None])
+        return np.stack([(c * e).sum(1), (-a * c * e).sum(1), (a * a * c * e).sum(1)], axis=1)
+
+    rs = np.linspace(0.0, rmax_cap, 20001)
+    big = np.abs(ders(rs ** 2)[:, 0]) > tol
+    rmax = float(rs[np.max(np.nonzero(big))]) if big.any() else 1.0
+    smax = max(rmax ** 2, 100.0 * smin)
+    sg = np.concatenate([[0.0], np.logspace(np.log10(smin), np.log10(smax), npts - 1)])
+    pp = PPoly.from_bernstein_basis(BPoly.from_derivatives(sg, ders(sg)))
+    return np.asarray(pp.x), np.asarray(pp.c).T
+
+
+def spline_gdd(knots, coefs, s):
+    """(g, g', g'') at s and the inside mask (``_locate_and_horner``,
+    gto.py:200-217)."""
+    seg = np.clip(np.searchsorted(knots, s, side="right") - 1, 0, coefs.shape[0] - 1)
+    d = s - knots[seg]
+    c = coefs[seg]
+    g = ((((c[..., 0] * d + c[..., 1]) * d + c[..., 2]) * d + c[..., 3]) * d + c[..., 4]) * d \
+        + c[..., 5]
+    gp = (((5 * c[..., 0] * d + 4 * c[..., 1]) * d + 3 * c[..., 2]) * d + 2 * c[..., 3]) * d \
+        + c[..., 4]
+    gpp = ((20 * c[..., 0] * d + 12 * c[..., 1]) * d + 6 * c[..., 2]) * d + 2 * c[..., 3]
+    inside = s < knots[-1]
+    return np.where(inside, g, 0.0), np.where(inside, gp, 0.0), np.where(inside, gpp, 0.0)
+
+
+_SPL_CACHE = {}
+
+
+def _shell_spline(system, i, sh):
+    """The spline of shell i when the system's AO transform splines it."""
+    spl = getattr(system, "spl", None)
+    if spl is None or i not in spl["tables"]:
+        return None
+    key = (tuple(sh.alpha), tuple(sh.norm), tuple(sorted(spl["cfg"].items())))
+    if key not in _SPL_CACHE:
+        _SPL_CACHE[key] = quintic_radial_spline(sh.alpha, sh.norm, **spl["cfg"])
+    return _SPL_CACHE[key]
+
+
 def _shell_disp(system, sh, x):
     dr = x - system.nuc[sh.iat]
     r2 = np.sum(dr * dr, axis=-1)
@@ -164,9 +218,12 @@ def _shell_disp(system, sh, x):
 def ao_value(system, x):
     """AO values (..., nbf) at positions x (..., 3) (``gto.py:1012-1056``)."""
     out = np.zeros(x.shape[:-1] + (system.nbf,))
-    for sh in system.shells:
+    for i, sh in enumerate(system.shells):
         dr, r2, r = _shell_disp(system, sh, x)
         R = np.sum(np.exp(-sh.alpha * r2[..., None]) * sh.norm, axis=-1)
+        sp = _shell_spline(system, i, sh)
+        if sp is not None:
+            R = spline_gdd(sp[0], sp[1], r2)[0]                    # _radial_val_spline
         if sh.am == 0 and sh.is_cusp:
             ia = sh.iat
             v = cusp_s(r, system.cusp_rc[ia], system.Z[ia], R,
@@ -185,12 +242,16 @@ def ao_vgl(system, x):
     val = np.zeros(shp + (system.nbf,))
     grad = np.zeros(shp + (system.nbf, 3))
     lap = np.zeros(shp + (system.nbf,))
-    for sh in system.shells:
+    for i, sh in enumerate(system.shells):
         dr, r2, r = _shell_disp(system, sh, x)
         e = np.exp(-sh.alpha * r2[..., None]) * sh.norm
         R = np.sum(e, axis=-1)
         Rp = np.sum(-2.0 * sh.alpha * e, axis=-1)
         Rl = np.sum((4.0 * sh.alpha ** 2 * r2[..., None] - 6.0 * sh.alpha) * e, axis=-1)
+        sp = _shell_spline(system, i, sh)
+        if sp is not None:                                          # _radial_vgl_spline
+            g, gp, gpp = spline_gdd(sp[0], sp[1], r2)
+            R, Rp, Rl = g, 2.0 * gp, 6.0 * gp + 4.0 * r2 * gpp
         sl = slice(sh.isgs, sh.isgs + sh.nsgs)
         if sh.am == 0:
             if sh.is_cusp:

@@ -194,6 +194,15 @@ jnp.concatenate = lambda xs, axis=0: torch.cat([_t(x) for x in xs], dim=axis)
 jnp.stack = lambda xs, axis=0: torch.stack([_t(x) for x in xs], dim=axis)
 jnp.ravel = lambda x: _t(x).reshape(-1)
 jnp.broadcast_to = lambda x, shape: _t(x).expand(*shape)
+
+
+def _searchsorted(a, v, side="left"):
+    a, v = _t(a), _t(v)
+    out = torch.searchsorted(a, v.reshape(-1), right=(side == "right"))
+    return out.reshape(v.shape)
+
+
+jnp.searchsorted = _searchsorted
 jnp.count_nonzero = lambda x: torch.count_nonzero(_t(x))
 jnp.finfo = lambda dt: torch.finfo(dt if isinstance(dt, torch.dtype) else torch.float64)
 jnp.einsum = lambda eq, *ops: torch.einsum(eq, *[_f(o) for o in ops])

@@ -89,6 +89,7 @@ class _RefMole:
         self.basis = mol.basis
         self.elements = mol.elements
         self.charge = mol.charge
+        self.ao_radial_transform = getattr(mol, "ao_radial_transform", None)
 
     def atom_charges(self):
         return torch.tensor(self._m.atom_charges(), dtype=torch.int64)
@@ -128,6 +129,11 @@ def _to_json(obj):
     if isinstance(obj, (np.floating, np.integer)):
         return obj.item()
     return obj
+
+
+def _with_splines(mol, transform):
+    mol.ao_radial_transform = transform
+    return mol
 
 
 def _j3_params(syms, npar, seed):
@@ -219,6 +225,19 @@ CASES = {
                                        _j3_params(("Li", "H"), 8, seed=17).items()
                                        if k != "unlike+H"}},
                1.0, 16),
+    # the quintic radial-spline AO transform (gto.py:141-240, 905-936):
+    # default grid without cusp correction (every shell splined), and a
+    # coarser grid with cusp-corrected s shells kept analytic
+    "h2o_spline": (lambda: _with_splines(M.named_system("H2O"), True), False,
+                   lambda mol: {"J1_pade": {"O": np.array(0.9), "H": np.array(0.4)},
+                                "J2_pade": {"like": np.array([0.25, 0.6]),
+                                            "unlike": np.array([0.5, 0.4])}},
+                   0.6, 24),
+    "lih_spline_cusp": (lambda: _with_splines(M.named_system("LiH"),
+                                              {"npts": 401, "tol": 1e-8}), True,
+                        lambda mol: {"J2_pade": {"like": np.array([0.25, 0.8]),
+                                                 "unlike": np.array([0.5, 0.8])}},
+                        1.0, 16),
     "h2o_md": (lambda: M.named_system("H2O"), False,
                lambda mol: {"J1_pade": {"O": np.array(0.9), "H": np.array(0.4)},
                             "J2_pade": {"like": np.array([0.25, 0.6]),
@@ -345,7 +364,8 @@ def run_case(gto, name, seed):
             warnings.simplefilter("ignore")
             ke_h.append(float(obj._local_energy_ke_hessian(x, nuc, tp)))
     spec = {"atoms": mol._atom, "basis": mol._basis, "cusp": pcusp,
-            "params_corr": params, "jastrow_config": jcfg}
+            "params_corr": params, "jastrow_config": jcfg,
+            "ao_splines": getattr(mol, "ao_radial_transform", None)}
     res = {k: np.array(v) for k, v in out.items()}
     res.update(X=X, mo_coeff=mf.mo_coeff, mo_occ=mf.mo_occ, e_nn=e_nn,
                e_ke_hessian=np.array(ke_h),

@@ -40,6 +40,7 @@ def load_golden(name):
     spec = json.loads(str(d["spec"]))
     atoms = [(a[0], tuple(a[1])) for a in spec["atoms"]]
     mol = Mole(atoms, spec["basis"], unit="Bohr")
+    mol.ao_radial_transform = spec.get("ao_splines")
     mf = MeanField(mol, d["mo_coeff"], d["mo_occ"])
     params = _params(spec["params_corr"])
     cusp = spec["cusp"]

@@ -31,12 +31,15 @@ def _rel(a, b, floor=1.0):
 def test_oracle_matches_reference_outputs(name):
     s, d = golden_system(name)
     r = O.evaluate(s, d["X"])
+    # spline radials: power-form quintics with large coefficients near the
+    # nucleus amplify last-bit differences of the evaluation order
+    tol2 = 5e-11 if s.spl is not None else 1e-11
     assert _rel(r["logpsi"], d["logpsi"]) < 1e-12
     assert _rel(r["e_ee"], d["e_ee"]) < 1e-13
     assert _rel(r["e_en"], d["e_en"]) < 1e-13
-    assert _rel(r["e_ke"], d["e_ke"]) < 1e-11
+    assert _rel(r["e_ke"], d["e_ke"]) < tol2
     assert _rel(r["grad"], d["grad"]) < 1e-12
-    assert _rel(r["lap"], d["lap"]) < 1e-11
+    assert _rel(r["lap"], d["lap"]) < tol2
     assert abs(s.e_nn - float(d["e_nn"])) < 1e-13
 
 
