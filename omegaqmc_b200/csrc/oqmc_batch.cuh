@@ -171,17 +171,13 @@ __device__ __forceinline__ void oq_batch_tile(const OqBatchArgs& a, const OqBatc
         if (d.proposal == 0) {
           nacc += oq_try_move<NOCC, T, Real, B>(J, S, SP, C, pos, Ai, WT, tid, e,
                                                 ox + d.step * n3[0], oy + d.step * n3[1],
-                                                oz + d.step * n3[2], 0.0, u, logdet);
+                                                oz + d.step * n3[2], 0.0, 1.0, u, logdet);
         } else {
-          const double so = oq_scaled_width(J, ox, oy, oz, d.step, d.scale_r0, d.scale_fmin);
-          const double nx = ox + so * n3[0], ny = oy + so * n3[1], nz = oz + so * n3[2];
-          const double sn = oq_scaled_width(J, nx, ny, nz, d.step, d.scale_r0, d.scale_fmin);
-          const double d2 =
-              (nx - ox) * (nx - ox) + (ny - oy) * (ny - oy) + (nz - oz) * (nz - oz);
-          const double log_extra =
-              3.0 * log(so / sn) + 0.5 * d2 * (1.0 / (so * so) - 1.0 / (sn * sn));
-          nacc += oq_try_move<NOCC, T, Real, B>(J, S, SP, C, pos, Ai, WT, tid, e, nx, ny, nz,
-                                                log_extra, u, logdet);
+          double nx, ny, nz, mul, lx;
+          oq_scaled_propose(J, ox, oy, oz, n3, d.step, d.scale_r0, d.scale_fmin, nx, ny, nz, mul,
+                            lx);
+          nacc += oq_try_move<NOCC, T, Real, B>(J, S, SP, C, pos, Ai, WT, tid, e, nx, ny, nz, lx,
+                                                mul, u, logdet);
         }
       }
     }

@@ -151,7 +151,7 @@ k_moves_mlp(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gspli
       const float lqr = oq_mix_logq_f(out, (float)(ox - nx), (float)(oy - ny), (float)(oz - nz));
       if (live)
         nacc += oq_try_move<NOCC, float, float, B>(J, S, SP, C, pos, Ai, W, w, e, nx, ny, nz,
-                                                   (double)(lqr - lqf), u, logdet);
+                                                   (double)(lqr - lqf), 1.0, u, logdet);
     }
   }
   if (live) a.logdet[w] = logdet;

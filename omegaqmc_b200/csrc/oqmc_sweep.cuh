@@ -317,8 +317,30 @@ __device__ __forceinline__ double oq_scaled_width(const SJ& S, double x, double 
     const double dx = x - S.nuc[I][0], dy = y - S.nuc[I][1], dz = z - S.nuc[I][2];
     r2 = fmin(r2, dx * dx + dy * dy + dz * dz);
   }
-  const double f = sqrt(r2) / r0;
+  // the width only has to be the same function of position on both sides
+  // of the ratio, so its square root runs in FP32
+  const double f = (double)(sqrtf((float)r2) / (float)r0);
   return step * fmin(1.0, fmax(fmn, f));
+}
+
+// Nucleus-scaled Gaussian proposal from (ox, oy, oz) with standard normals
+// n3: the new position and the proposal-density ratio q(old | new) /
+// q(new | old) = (so / sn)^3 exp(d^2 (1 / so^2 - 1 / sn^2) / 2), returned as
+// a factor mul and an exponent lx (no logarithm on the move path).
+template <class SJ>
+__device__ __forceinline__ void oq_scaled_propose(const SJ& S, double ox, double oy, double oz,
+                                                  const double n3[3], double step, double r0,
+                                                  double fmn, double& nx, double& ny,
+                                                  double& nz, double& mul, double& lx) {
+  const double so = oq_scaled_width(S, ox, oy, oz, step, r0, fmn);
+  nx = ox + so * n3[0];
+  ny = oy + so * n3[1];
+  nz = oz + so * n3[2];
+  const double sn = oq_scaled_width(S, nx, ny, nz, step, r0, fmn);
+  // with d = so n3: d^2 (1 / so^2 - 1 / sn^2) = |n3|^2 (1 - q^2), q = so / sn
+  const double q = so / sn;
+  mul = q * q * q;
+  lx = 0.5 * (n3[0] * n3[0] + n3[1] * n3[1] + n3[2] * n3[2]) * (1.0 - q * q);
 }
 
 // Change of the Jastrow factor (arithmetic in T) when electron e moves from
@@ -383,8 +405,11 @@ __device__ __forceinline__ T oq_jastrow_delta(const SJ& J, const OqSystem& S, co
 }
 
 // One single-electron Metropolis move of electron e to (nx, ny, nz) against
-// shared-memory state; log_extra is the log proposal-density ratio
-// log q(old)/q(new) (0 for symmetric proposals).  Returns acceptance.
+// shared-memory state; the proposal-density ratio q(old)/q(new) is
+// mul_extra * exp(log_extra) (1 for symmetric proposals).  The move is
+// accepted when u < |R|^2 exp(2 dJ) q(old)/q(new), the Metropolis-Hastings
+// test of metropolis_move_1w (OmegaQMC/vmc_gto.py:841-905) without
+// logarithms.  Returns acceptance.
 // J supplies the nuclei and Jastrow constants (natm, nuc, has_j1, j1a, j1b,
 // has_j2, j2): the system struct itself or a compact copy of those fields;
 // S is handed to the basis policy.
@@ -393,7 +418,8 @@ __device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, cons
                                             const Real* __restrict__ C, double* pos,
                                             Real* Ai, int WPB, int tid, int e,
                                             double nx, double ny, double nz,
-                                            double log_extra, double u, double& logdet) {
+                                            double log_extra, double mul_extra, double u,
+                                            double& logdet) {
   constexpr int NE = 2 * NOCC;
   constexpr int NN = NOCC * NOCC;
   const int s = e & 1, i = e >> 1;
@@ -418,8 +444,9 @@ __device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, cons
 #pragma unroll
   for (int j = 0; j < NOCC; ++j) R = (j == i) ? wv[j] : R;
   const double Rd = (double)R;
-  const double logp = 2.0 * log(fabs(Rd)) + 2.0 * (double)dJ + log_extra;
-  const bool acc = valid && (Rd != 0.0) && isfinite(logp) && (log(u) < logp);
+  const double ratio = Rd * Rd * mul_extra * exp(2.0 * (double)dJ + log_extra);
+  const bool acc = valid && (Rd != 0.0) && isfinite(Rd) && isfinite((double)dJ) &&
+                   isfinite(log_extra) && (u < ratio);
   if (acc) {
     // Sherman-Morrison: A[k][j] -= A[k][i] (w_j - delta_ij) / R
     const T rinv = (T)1 / R;
@@ -542,8 +569,8 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
         const double nx = pos[(3 * e) * WPB + tid] + a.step * n3[0];
         const double ny = pos[(3 * e + 1) * WPB + tid] + a.step * n3[1];
         const double nz = pos[(3 * e + 2) * WPB + tid] + a.step * n3[2];
-        nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz, 0.0, u,
-                                           logdet);
+        nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz, 0.0,
+                                           1.0, u, logdet);
       }
     } else if (PROP == 1) {
       // nucleus-scaled Gaussian: sigma(x) = step * clamp(r_near(x)/r0, fmin, 1);
@@ -553,21 +580,18 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
         oq_move_randoms(a.seed, (uint32_t)w, gstep, (uint32_t)e, n3, u);
         const double ox = pos[(3 * e) * WPB + tid], oy = pos[(3 * e + 1) * WPB + tid],
                      oz = pos[(3 * e + 2) * WPB + tid];
-        const double so = oq_scaled_width(S, ox, oy, oz, a.step, a.scale_r0, a.scale_fmin);
-        const double nx = ox + so * n3[0], ny = oy + so * n3[1], nz = oz + so * n3[2];
-        const double sn = oq_scaled_width(S, nx, ny, nz, a.step, a.scale_r0, a.scale_fmin);
-        const double d2 = (nx - ox) * (nx - ox) + (ny - oy) * (ny - oy) + (nz - oz) * (nz - oz);
-        const double log_extra =
-            3.0 * log(so / sn) + 0.5 * d2 * (1.0 / (so * so) - 1.0 / (sn * sn));
-        nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
-                                           log_extra, u, logdet);
+        double nx, ny, nz, mul, lx;
+        oq_scaled_propose(S, ox, oy, oz, n3, a.step, a.scale_r0, a.scale_fmin, nx, ny, nz, mul,
+                          lx);
+        nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz, lx,
+                                           mul, u, logdet);
       }
     } else {
       double u, nx, ny, nz, log_qratio;
       const int e = oq_basin_propose<NE>(S, pos + tid, WPB, a.seed, (uint32_t)w, gstep, a.step,
                                          nx, ny, nz, log_qratio, u);
       nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
-                                         log_qratio, u, logdet);
+                                         log_qratio, 1.0, u, logdet);
     }
   }
   if (live) {
