@@ -117,34 +117,39 @@ struct Gen {
   }
 
   // declare R<k> (and Rp<k>, Rl<k>) of type ty and accumulate group g's
-  // primitives (sel 0: all, 1: tight only, 2: all but the tight ones)
+  // primitives (sel 0: all, 1: tight only, 2: all but the tight ones).  With
+  // e_p = exp(-a_p r^2): R = sum n_p e_p, R'/r = sum (-2 a_p n_p) e_p and
+  // R'' + 2 R'/r = r^2 sum (4 a_p^2 n_p) e_p + 3 R'/r, the per-primitive
+  // constants folded on the host.
   void radial(int g, bool vgl, const std::string& ty, const char* r2, int sel = 0) {
     const int np = S.g_n[g], nc = S.g_ncol[g], off = S.g_off[g], sh0 = S.g_shell0[g];
     for (int k = 0; k < nc; ++k) {
       const std::string ks = std::to_string(k);
       add("      " + ty + " R" + ks + " = 0");
-      if (vgl) add(", Rp" + ks + " = 0, Rl" + ks + " = 0");
+      if (vgl) add(", Rp" + ks + " = 0, Rl" + ks + ", Ra" + ks + " = 0");
       add(";\n");
     }
     const std::string ex = (ty == "double") ? "exp" : "oq_exp<T>";
     for (int p = 0; p < np; ++p) {
       if ((sel == 1 && !tight(g, p)) || (sel == 2 && tight(g, p))) continue;
-      const std::string al = "((" + ty + ")" + num(S.alpha[off + p]) + ")";
-      add("      { const " + ty + " e = " + ex + "(-" + al + " * " + r2 + ");\n");
-      if (vgl) {
-        add("        const " + ty + " fp = (" + ty + ")-2 * " + al + " * e;\n");
-        add("        const " + ty + " fl = ((" + ty + ")4 * " + al + " * " + al + " * " + r2 +
-            " - (" + ty + ")6 * " + al + ") * e;\n");
-      }
+      const double a = S.alpha[off + p];
+      add("      { const " + ty + " e = " + ex + "(-((" + ty + ")" + num(a) + ") * " + r2 + ");\n");
       for (int k = 0; k < nc; ++k) {
-        const std::string nl = "((" + ty + ")" + num(S.norm[S.s_norm[sh0 + k] + p]) + ")";
+        const double n = S.norm[S.s_norm[sh0 + k] + p];
         const std::string ks = std::to_string(k);
-        add("        R" + ks + " += " + nl + " * e;");
-        if (vgl) add(" Rp" + ks + " += " + nl + " * fp; Rl" + ks + " += " + nl + " * fl;");
+        add("        R" + ks + " += ((" + ty + ")" + num(n) + ") * e;");
+        if (vgl)
+          add(" Rp" + ks + " += ((" + ty + ")" + num(-2.0 * a * n) + ") * e; Ra" + ks +
+              " += ((" + ty + ")" + num(4.0 * a * a * n) + ") * e;");
         add("\n");
       }
       add("      }\n");
     }
+    if (vgl)
+      for (int k = 0; k < nc; ++k) {
+        const std::string ks = std::to_string(k);
+        add("      Rl" + ks + " = " + r2 + " * Ra" + ks + " + (" + ty + ")3 * Rp" + ks + ";\n");
+      }
   }
 
   // accumulate one AO into the MOs (value expression v; grad g[3], lap l)
