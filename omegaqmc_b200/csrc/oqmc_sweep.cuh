@@ -623,17 +623,19 @@ __device__ __forceinline__ void oq_jastrow_vgl_coulomb(const SJ& J, const OqSyst
     const double dx = xe - pos[(size_t)(3 * j) * ps], dy = ye - pos[(size_t)(3 * j + 1) * ps],
                  dz = ze - pos[(size_t)(3 * j + 2) * ps];
     const double r2 = dx * dx + dy * dy + dz * dz;
-    if (j > e) ee += rsqrt(r2 + OQ_EPS);
+    const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
+    // Coulomb: FP64 with the reference's eps in FP64 kernels; the working-
+    // precision 1/r otherwise (eps is below FP32 resolution beyond the
+    // 1e-4 bohr minimum distance)
+    if (j > e) ee += (sizeof(T) == 8) ? rsqrt(r2 + OQ_EPS) : (double)rinv;
     if (J.has_j2) {
       const int o = ((e & 1) == (j & 1)) ? 0 : 2;
-      const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
       T upr, l;
       oq_pade_vgl_q((T)J.j2[o], (T)J.j2[o + 1], r2t * rinv, rinv, upr, l);
       jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
     }
     if (S.has_bs2) {
       const bool like = (e & 1) == (j & 1);
-      const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
       T upr, l;
       oq_bs_vgl<T>(like ? S.bs2_like : S.bs2_unlike, like ? S.bs2_n_like : S.bs2_n_unlike,
                    (T)(like ? S.bs2_dinv_like : S.bs2_dinv_unlike), (T)S.bs2_rcut, r2t * rinv,
@@ -644,16 +646,15 @@ __device__ __forceinline__ void oq_jastrow_vgl_coulomb(const SJ& J, const OqSyst
   for (int I = 0; I < J.natm; ++I) {
     const double dx = xe - J.nuc[I][0], dy = ye - J.nuc[I][1], dz = ze - J.nuc[I][2];
     const double r2 = dx * dx + dy * dy + dz * dz;
-    en -= J.Z[I] * rsqrt(r2 + OQ_EPS);
+    const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
+    en -= J.Z[I] * ((sizeof(T) == 8) ? rsqrt(r2 + OQ_EPS) : (double)rinv);
     if (J.has_j1) {
-      const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
       T upr, l;
       oq_pade_vgl_q((T)J.j1a[I], (T)J.j1b[I], r2t * rinv, rinv, upr, l);
       jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
     }
     if (S.has_bs1 && S.bs1_type[I] >= 0) {
       const int ty = S.bs1_type[I];
-      const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
       T upr, l;
       oq_bs_vgl<T>(S.bs1_c[ty], S.bs1_n[ty], (T)S.bs1_dinv[ty], (T)S.bs1_rcut[ty], r2t * rinv,
                    rinv, upr, l);
