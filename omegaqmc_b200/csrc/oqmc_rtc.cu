@@ -121,7 +121,8 @@ struct Gen {
   // e_p = exp(-a_p r^2): R = sum n_p e_p, R'/r = sum (-2 a_p n_p) e_p and
   // R'' + 2 R'/r = r^2 sum (4 a_p^2 n_p) e_p + 3 R'/r, the per-primitive
   // constants folded on the host.
-  void radial(int g, bool vgl, const std::string& ty, const char* r2, int sel = 0) {
+  void radial(int g, bool vgl, const std::string& ty, const char* r2, int sel = 0,
+              bool tight_arg = false) {
     const int np = S.g_n[g], nc = S.g_ncol[g], off = S.g_off[g], sh0 = S.g_shell0[g];
     for (int k = 0; k < nc; ++k) {
       const std::string ks = std::to_string(k);
@@ -133,7 +134,11 @@ struct Gen {
     for (int p = 0; p < np; ++p) {
       if ((sel == 1 && !tight(g, p)) || (sel == 2 && tight(g, p))) continue;
       const double a = S.alpha[off + p];
-      add("      { const " + ty + " e = " + ex + "(-((" + ty + ")" + num(a) + ") * " + r2 + ");\n");
+      if (tight_arg && tight(g, p))   // FP64 argument, see oq_exp_tight
+        add("      { const " + ty + " e = oq_exp_tight<" + ty + ">(" + num(a) + " * r2d);\n");
+      else
+        add("      { const " + ty + " e = " + ex + "(-((" + ty + ")" + num(a) + ") * " + r2 +
+            ");\n");
       for (int k = 0; k < nc; ++k) {
         const double n = S.norm[S.s_norm[sh0 + k] + p];
         const std::string ks = std::to_string(k);
@@ -243,10 +248,9 @@ struct Gen {
             angular(g, k, false, "R" + ks, "", "");
           }
         } else {
-          // Radial factors: cusp groups always in FP64; the tight exponents
-          // of a split group in FP64 within its split radius (the group's
-          // other exponents and every exponent outside the radius in the
-          // working precision); other groups in the working precision.
+          // Radial factors: cusp groups in FP64; the tight exponents of a
+          // split group with FP64 arguments; everything else in the working
+          // precision.
           bool cusp = false;
           for (int k = 0; k < nc; ++k) cusp = cusp || (s_shell && S.s_cusp[sh0 + k]);
           const bool split = SP.r2[g] > 0.0;
@@ -280,30 +284,16 @@ struct Gen {
           if (cusp) {
             fp64_inline();
           } else if (split) {
-            // the group's other primitives in the working precision for
-            // every lane; the tight ones in FP64 within the split radius
+            // the tight exponents with FP64 arguments (oq_exp_tight), every
+            // lane and every exponent of the group in the working precision
             add("      {\n");
-            radial(g, true, "T", "r2", 2);
+            radial(g, true, "T", "r2", 0, true);
             for (int k = 0; k < nc; ++k) {
               const std::string ks = std::to_string(k);
               add("      RT" + ks + " = R" + ks + "; RpT" + ks + " = Rp" + ks + "; RlT" + ks +
                   " = Rl" + ks + ";\n");
             }
-            add("      }\n    if (sizeof(T) == 8 || r2d < " + num(SP.r2[g]) + ") {\n      {\n");
-            radial(g, true, "double", "r2d", 1);
-            for (int k = 0; k < nc; ++k) {
-              const std::string ks = std::to_string(k);
-              add("      RT" + ks + " += (T)R" + ks + "; RpT" + ks + " += (T)Rp" + ks + "; RlT" +
-                  ks + " += (T)Rl" + ks + ";\n");
-            }
-            add("      }\n    } else {\n      {\n");
-            radial(g, true, "T", "r2", 1);
-            for (int k = 0; k < nc; ++k) {
-              const std::string ks = std::to_string(k);
-              add("      RT" + ks + " += R" + ks + "; RpT" + ks + " += Rp" + ks + "; RlT" + ks +
-                  " += Rl" + ks + ";\n");
-            }
-            add("      }\n    }\n");
+            add("      }\n");
           } else {
             working();
           }

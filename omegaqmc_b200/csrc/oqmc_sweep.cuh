@@ -30,6 +30,24 @@ template <typename T> __device__ __forceinline__ T oq_exp(T v);
 template <> __device__ __forceinline__ double oq_exp<double>(double v) { return exp(v); }
 template <> __device__ __forceinline__ float oq_exp<float>(float v) { return __expf(v); }
 
+// exp(-arg) for a tight exponent, arg = alpha r^2 formed in FP64.  In FP32
+// the rounding of a large argument would dominate the error, so the FP64
+// argument is split as arg log2(e) = k + f (k integer, f in [0, 1)) and only
+// 2^-f is evaluated in FP32, then scaled by 2^-k: FP32 relative accuracy for
+// every argument, without an FP64 exponential or a branch.
+template <typename T> __device__ __forceinline__ T oq_exp_tight(double arg);
+template <> __device__ __forceinline__ double oq_exp_tight<double>(double arg) {
+  return exp(-arg);
+}
+template <> __device__ __forceinline__ float oq_exp_tight<float>(double arg) {
+  const double t = arg * 1.4426950408889634;        // >= 0
+  const int k = (int)fmin(t, 126.0);                 // truncation = floor here
+  const float f = (float)(t - (double)k);            // in [0, 1) (or >= 1 past 2^-126)
+  float p;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(p) : "f"(-f));
+  return p * __int_as_float((127 - k) << 23);        // 2^-k, a normal float for k <= 126
+}
+
 // per-group "tight" split radius squared (FP64 evaluation inside it);
 // 0 disables.  Stored after the system struct in global memory.
 struct OqSplit {
