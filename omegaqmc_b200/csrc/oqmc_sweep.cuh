@@ -446,39 +446,30 @@ __device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, cons
   // Jastrow change (arithmetic in T) and the MIN_DIST_THRESHOLD test (FP64)
   bool valid;
   const T dJ = oq_jastrow_delta<NE, T>(J, S, pos + tid, WPB, e, ox, oy, oz, nx, ny, nz, valid);
-  // new MO row and the ratio vector w_j = sum_m v_m A[m][j]; R = w_i
+  // new MO row and the ratio R = sum_m v_m A[m][i] (column i of the inverse)
   T v[NOCC];
   B::template mo_val<T, Real>(S, SP, C, nx, ny, nz, v);
   Real* As = Ai + (size_t)s * NN * WPB;
-  T wv[NOCC];
-#pragma unroll
-  for (int j = 0; j < NOCC; ++j) {
-    T acc = (T)0;
-#pragma unroll
-    for (int m = 0; m < NOCC; ++m) acc += v[m] * (T)As[(m * NOCC + j) * WPB + tid];
-    wv[j] = acc;
-  }
   T R = (T)0;
 #pragma unroll
-  for (int j = 0; j < NOCC; ++j) R = (j == i) ? wv[j] : R;
+  for (int m = 0; m < NOCC; ++m) R += v[m] * (T)As[(m * NOCC + i) * WPB + tid];
   const double Rd = (double)R;
   const double ratio = Rd * Rd * mul_extra * exp(2.0 * (double)dJ + log_extra);
   const bool acc = valid && (Rd != 0.0) && isfinite(Rd) && isfinite((double)dJ) &&
                    isfinite(log_extra) && (u < ratio);
   if (acc) {
-    // Sherman-Morrison: A[k][j] -= A[k][i] (w_j - delta_ij) / R
+    // Sherman-Morrison with the ratio vector w_j = sum_m v_m A[m][j]:
+    // A[k][j] -= A[k][i] (w_j - delta_ij) / R, column i taken before the update
     const T rinv = (T)1 / R;
     T coli[NOCC];
 #pragma unroll
-    for (int k = 0; k < NOCC; ++k) {
-      T c = (T)0;
-#pragma unroll
-      for (int j = 0; j < NOCC; ++j) c = (j == i) ? (T)As[(k * NOCC + j) * WPB + tid] : c;
-      coli[k] = c;
-    }
+    for (int k = 0; k < NOCC; ++k) coli[k] = (T)As[(k * NOCC + i) * WPB + tid];
 #pragma unroll
     for (int j = 0; j < NOCC; ++j) {
-      const T f = (wv[j] - (j == i ? (T)1 : (T)0)) * rinv;
+      T w = (T)0;
+#pragma unroll
+      for (int m = 0; m < NOCC; ++m) w += v[m] * (T)As[(m * NOCC + j) * WPB + tid];
+      const T f = (w - (j == i ? (T)1 : (T)0)) * rinv;
 #pragma unroll
       for (int k = 0; k < NOCC; ++k) {
         Real& ref = As[(k * NOCC + j) * WPB + tid];
