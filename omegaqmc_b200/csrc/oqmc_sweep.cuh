@@ -454,7 +454,12 @@ __device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, cons
 #pragma unroll
   for (int m = 0; m < NOCC; ++m) R += v[m] * (T)As[(m * NOCC + i) * WPB + tid];
   const double Rd = (double)R;
-  const double ratio = Rd * Rd * mul_extra * exp(2.0 * (double)dJ + log_extra);
+  // the exponential in the working precision (accurate expf in FP32: its
+  // ~1e-7 relative error moves acceptance probabilities far below any
+  // statistical resolution)
+  const double ex = (sizeof(T) == 8) ? exp(2.0 * (double)dJ + log_extra)
+                                     : (double)expf((float)(2.0 * (double)dJ + log_extra));
+  const double ratio = Rd * Rd * mul_extra * ex;
   const bool acc = valid && (Rd != 0.0) && isfinite(Rd) && isfinite((double)dJ) &&
                    isfinite(log_extra) && (u < ratio);
   if (acc) {
