@@ -100,6 +100,7 @@ struct Gen {
   const double* C;     // nbf x nocc
   int nocc;
   std::string o;
+  bool contract = false;   // VGL contracted with an inverse column (mo_vgl_contract)
   void add(const std::string& s) { o += s; }
 
   static std::string num(double v) {
@@ -159,6 +160,21 @@ struct Gen {
 
   // accumulate one AO into the MOs (value expression v; grad g[3], lap l)
   void accum(int ao, const std::string& v, const std::string* g, const std::string* l) {
+    if (contract) {
+      // ca = sum_m C[ao][m] ac[m], then the AO's gradient and Laplacian
+      // weighted by ca: one contraction per AO instead of one per MO
+      std::string ca;
+      for (int m = 0; m < nocc; ++m) {
+        const double c = C[ao * nocc + m];
+        if (c == 0.0) continue;
+        ca += std::string(ca.empty() ? "" : " + ") + "(T)(" + num(c) + ") * ac[" +
+              std::to_string(m) + "]";
+      }
+      if (ca.empty()) return;
+      add("      { const T ca = " + ca + ";\n        gx += ca * " + g[0] + "; gy += ca * " + g[1] +
+          "; gz += ca * " + g[2] + "; lp += ca * " + *l + "; }\n");
+      return;
+    }
     for (int m = 0; m < nocc; ++m) {
       const double c = C[ao * nocc + m];
       if (c == 0.0) continue;
@@ -216,7 +232,8 @@ struct Gen {
   }
 
   void body(bool vgl) {
-    for (int m = 0; m < nocc; ++m) {
+    if (contract) add("  gx = (T)0; gy = (T)0; gz = (T)0; lp = (T)0;\n");
+    for (int m = 0; m < nocc && !contract; ++m) {
       const std::string ms = std::to_string(m);
       add("  mv[" + ms + "] = (T)0;");
       if (vgl)
@@ -331,6 +348,18 @@ std::string generate_basis(const OqSystem& S, const OqSplit& SP, const double* C
            "      const TC* __restrict__ C, double x, double y, double z, T* mv, T (*mg)[3],\n"
            "      T* ml) {\n  (void)SP; (void)C;\n";
     src += b + "  }\n";
+  }
+  {
+    Gen g{S, SP, C, nocc, ""};
+    g.contract = true;
+    g.body(true);
+    src += "\n  // gradient and Laplacian of sum_m ac[m] phi_m (the Slater part of the local\n"
+           "  // energy with ac a column of the inverse)\n"
+           "  template <typename T, typename TC>\n"
+           "  __device__ static __forceinline__ void mo_vgl_contract(const OqSystem& S,\n"
+           "      const OqSplit& SP, const TC* __restrict__ C, double x, double y, double z,\n"
+           "      const T* ac, T& gx, T& gy, T& gz, T& lp) {\n  (void)SP; (void)C;\n";
+    src += g.o + "  }\n";
   }
   src += "};\n";
   return src;

@@ -256,6 +256,21 @@ struct OqBasisTable {
                                                 double z, T* mv, T (*mg)[3], T* ml) {
     oq_mo_vgl_t<NOCC, T, TC>(S, SP, C, x, y, z, mv, mg, ml);
   }
+  // gradient and Laplacian of sum_m ac[m] phi_m
+  template <typename T, typename TC>
+  __device__ static __forceinline__ void mo_vgl_contract(const OqSystem& S, const OqSplit& SP,
+                                                         const TC* __restrict__ C, double x,
+                                                         double y, double z, const T* ac, T& gx,
+                                                         T& gy, T& gz, T& lp) {
+    T mv[NOCC], mg[NOCC][3], ml[NOCC];
+    oq_mo_vgl_t<NOCC, T, TC>(S, SP, C, x, y, z, mv, mg, ml);
+    gx = gy = gz = lp = (T)0;
+#pragma unroll
+    for (int m = 0; m < NOCC; ++m) {
+      gx += ac[m] * mg[m][0]; gy += ac[m] * mg[m][1]; gz += ac[m] * mg[m][2];
+      lp += ac[m] * ml[m];
+    }
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -695,15 +710,13 @@ __device__ __forceinline__ void oq_eloc_electron(const SJ& J, const OqSystem& S,
   const int s = e & 1, i = e >> 1;
   const double xe = pos[(size_t)(3 * e) * ps], ye = pos[(size_t)(3 * e + 1) * ps],
                ze = pos[(size_t)(3 * e + 2) * ps];
-  T mv[NOCC], mg[NOCC][3], ml[NOCC];
-  B::template mo_vgl<T, Real>(S, SP, C, xe, ye, ze, mv, mg, ml);
-  T gx = 0, gy = 0, gz = 0, lp = 0;
+  // Gamma = sum_m A[m][i] grad phi_m, sum_m A[m][i] lap phi_m: the MO
+  // coefficients contracted with column i of the inverse first
+  T ac[NOCC];
 #pragma unroll
-  for (int m = 0; m < NOCC; ++m) {
-    const T am = (T)A[(size_t)((s * NOCC + m) * NOCC + i) * as];
-    gx += am * mg[m][0]; gy += am * mg[m][1]; gz += am * mg[m][2];
-    lp += am * ml[m];
-  }
+  for (int m = 0; m < NOCC; ++m) ac[m] = (T)A[(size_t)((s * NOCC + m) * NOCC + i) * as];
+  T gx, gy, gz, lp;
+  B::template mo_vgl_contract<T, Real>(S, SP, C, xe, ye, ze, ac, gx, gy, gz, lp);
   T jx = (T)0, jy = (T)0, jz = (T)0, jl = (T)0;
   oq_jastrow_vgl_coulomb<NE, T>(J, S, pos, ps, e, xe, ye, ze, jx, jy, jz, jl, ee, en);
   const double sgx = (double)gx, sgy = (double)gy, sgz = (double)gz;
