@@ -580,29 +580,43 @@ def run_persistent(a):
                  "ms_per_step": pms / Kp, "steps": Kp, "path": "same persistent kernel, FP64",
                  "energy": {"mean": pm, "serr": pse},
                  "energy_diff_sigma": abs(pm - e_mean) / max(np.hypot(pse, e_serr), 1e-300)}
-        # precision: FP64 sampler with the same proposal, and the mixed vs FP64
-        # local energy on identical configurations
-        pb.set_proposal(0, proposal="scaled", scale_r0=HEAD_R0, scale_fmin=HEAD_FMIN)
-        pb.adapt_steps(HEAD_ACC, seed=seed ^ 5)
-        pb.reset(EQ2 + 10**6)
-        for _ in range(10):
-            pb.run(REFRESH_EVERY, REFRESH_EVERY + 1, seed ^ 6)
-        pb.reset(0)
+        # precision, paired: the mixed and the FP64 sampler start from the same
+        # walkers with the same proposal, step, seed and RNG counters, so they
+        # take the same decisions until a rounding difference flips one; the
+        # per-sweep difference of their walker-mean energies then measures
+        # the precision effect far below the runs' own statistical errors
         Kf = 4000
-        for _ in range(Kf // REFRESH_EVERY):
-            pb.run(REFRESH_EVERY, 1, seed ^ 6)
-        fn = pb.sums[0][:Kf].cpu().numpy()
-        fm, fse, _, fk = O.binning_analysis(fn[:, 3] / np.maximum(fn[:, 6], 1))
+        cfgm = b.config()
+        runs = {}
+        for prec_name in (a.precision, "fp64"):
+            sb = BatchedSampler([ctx], [b.walkers[0].clone()], [step], precision=prec_name,
+                                proposal=a.proposal, scale_r0=HEAD_R0, scale_fmin=HEAD_FMIN,
+                                cap=Kf)
+            sb.configure(cfgm["threads"], cfgm["walkers_per_tile"], cfgm["variant"])
+            sb.reset(EQ2 + 2 * 10**6)
+            for _ in range(Kf // REFRESH_EVERY):
+                sb.run(REFRESH_EVERY, 1, seed ^ 6)
+            sn = sb.sums[0][:Kf].cpu().numpy()
+            runs[prec_name] = (sn[:, 3] / np.maximum(sn[:, 6], 1), sb.walkers[0].clone())
+            del sb
+        mser, mX = runs[a.precision]
+        fser, fX = runs["fp64"]
+        mm, mse, _, _ = O.binning_analysis(mser)
+        fm, fse, _, fk = O.binning_analysis(fser)
+        dm, dse, _, _ = O.binning_analysis(mser - fser)
+        diverged = float(torch.any((mX != fX).reshape(W, -1), dim=1).float().mean())
         ctx.set_proposal(0)
         ens = WalkerEnsemble(ctx, b.walkers[0], a.precision, seed=seed ^ 7)
         ep = torch.empty(W, 4, dtype=torch.float64, device=dev)
         ens.run(1, 1e-9, eparts_last=ep)
         ref = ctx.evaluate(ens.X, want_grad=False, want_lap=False)["e_loc"]
         dE = (ep[:, 3] - ref).cpu().numpy()
-        prec = {"fp64_same_proposal": {"energy": {"mean": fm, "serr": fse}, "tau_int": fk,
-                                       "steps": Kf},
-                "sampled_diff_Ha": e_mean - fm,
-                "sampled_diff_sigma": abs(e_mean - fm) / max(np.hypot(fse, e_serr), 1e-300),
+        prec = {"paired": {"sweeps": Kf, "mixed_energy": {"mean": mm, "serr": mse},
+                           "fp64_energy": {"mean": fm, "serr": fse}, "fp64_tau_int": fk,
+                           "diff_Ha": dm, "diff_serr_Ha": dse,
+                           "walkers_diverged_frac": diverged},
+                "sampled_diff_Ha": mm - fm,
+                "sampled_diff_sigma": abs(mm - fm) / max(np.hypot(mse, fse), 1e-300),
                 "eloc_same_configs": {"walkers": W, "mean_diff_Ha": float(dE.mean()),
                                       "serr_Ha": float(dE.std() / np.sqrt(W)),
                                       "median_abs_Ha": float(np.median(np.abs(dE))),
