@@ -154,9 +154,9 @@ __device__ __forceinline__ void oq_move_randoms(uint64_t seed, uint32_t walker,
   const float k32 = 2.3283064365386963e-10f;
   const float a = sqrtf(-2.0f * __logf(((float)r0.x + 1.0f) * k32));
   const float b = sqrtf(-2.0f * __logf(((float)r0.z + 1.0f) * k32));
-  float s, c, s2, c2;
+  float s, c;
   __sincosf(6.283185307179586f * ((float)r0.y * k32), &s, &c);
-  __sincosf(6.283185307179586f * ((float)r0.w * k32), &s2, &c2);
+  const float c2 = __cosf(6.283185307179586f * ((float)r0.w * k32));   // third normal only
   n3[0] = (double)(a * c);
   n3[1] = (double)(a * s);
   n3[2] = (double)(b * c2);
@@ -174,6 +174,15 @@ __device__ __forceinline__ float oq_rsqrt(float x) { return rsqrtf(x); }
 template <typename T>
 __device__ __forceinline__ T oq_pade_q(T a, T b, T r) {
   return a * r * oq_rcp((T)1 + b * r);
+}
+// Change of a r / (1 + b r) from r_o to r_n.  FP32: the algebraically
+// equal a (r_n - r_o) / ((1 + b r_n)(1 + b r_o)), one reciprocal instead of
+// two (and no cancellation between two values); FP64: the difference of the
+// two values.
+template <typename T>
+__device__ __forceinline__ T oq_pade_diff(T a, T b, T rn, T ro) {
+  if (sizeof(T) == 8) return oq_pade_q(a, b, rn) - oq_pade_q(a, b, ro);
+  return a * (rn - ro) * oq_rcp(((T)1 + b * rn) * ((T)1 + b * ro));
 }
 template <typename T>
 __device__ __forceinline__ void oq_pade_vgl_q(T a, T b, T r, T rinv, T& up_r, T& lap) {

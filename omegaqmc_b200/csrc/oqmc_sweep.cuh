@@ -399,7 +399,7 @@ __device__ __forceinline__ T oq_jastrow_delta(const SJ& J, const OqSystem& S, co
       const T rn2t = (T)rn2, ro2t = (T)(bx * bx + by * by + bz * bz);
       const int o = ((e & 1) == (j & 1)) ? 0 : 2;
       const T pa = (T)J.j2[o], pb = (T)J.j2[o + 1];
-      dJ += oq_pade_q(pa, pb, rn2t * oq_rsqrt(rn2t)) - oq_pade_q(pa, pb, ro2t * oq_rsqrt(ro2t));
+      dJ += oq_pade_diff(pa, pb, rn2t * oq_rsqrt(rn2t), ro2t * oq_rsqrt(ro2t));
     }
     if (S.has_bs2) {
       const double bx = ox - xj, by = oy - yj, bz = oz - zj;
@@ -420,7 +420,7 @@ __device__ __forceinline__ T oq_jastrow_delta(const SJ& J, const OqSystem& S, co
       const double bx = ox - J.nuc[I][0], by = oy - J.nuc[I][1], bz = oz - J.nuc[I][2];
       const T rn2t = (T)rn2, ro2t = (T)(bx * bx + by * by + bz * bz);
       const T pa = (T)J.j1a[I], pb = (T)J.j1b[I];
-      dJ += oq_pade_q(pa, pb, rn2t * oq_rsqrt(rn2t)) - oq_pade_q(pa, pb, ro2t * oq_rsqrt(ro2t));
+      dJ += oq_pade_diff(pa, pb, rn2t * oq_rsqrt(rn2t), ro2t * oq_rsqrt(ro2t));
     }
     if (S.has_bs1 && S.bs1_type[I] >= 0) {
       const int ty = S.bs1_type[I];
