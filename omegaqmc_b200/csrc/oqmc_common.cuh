@@ -140,27 +140,29 @@ __device__ __forceinline__ double oq_u01(uint32_t v) {
   return ((double)v + 1.0) * 2.3283064365386963e-10;
 }
 
-// Three standard normals and one uniform for a single-electron proposal.
-// Counter = (walker, step, electron, stream); key = seed.
+// Three standard normals and one uniform for a single-electron proposal
+// from one Philox4x32-10 block, counter = (walker, step, electron, 0), key =
+// seed.  Box-Muller in FP32 on the top 24 bits of the four words (the
+// deviates only set proposal widths, 24-bit resolution is ample and the FP32
+// transcendental units are cheap); the acceptance uniform from the four low
+// bytes, bits disjoint from those, so all deviates are independent.
 __device__ __forceinline__ void oq_move_randoms(uint64_t seed, uint32_t walker,
                                                 uint32_t step, uint32_t elec,
                                                 double n3[3], double& u) {
-  OqU4 c0 = {walker, step, elec, 0u};
-  OqU4 r0 = oq_philox(c0, (uint32_t)seed, (uint32_t)(seed >> 32));
-  OqU4 c1 = {walker, step, elec, 1u};
-  OqU4 r1 = oq_philox(c1, (uint32_t)seed, (uint32_t)(seed >> 32));
-  // Box-Muller in FP32: the deviates only set proposal widths, 24-bit
-  // resolution is ample and the FP32 transcendental units are cheap
-  const float k32 = 2.3283064365386963e-10f;
-  const float a = sqrtf(-2.0f * __logf(((float)r0.x + 1.0f) * k32));
-  const float b = sqrtf(-2.0f * __logf(((float)r0.z + 1.0f) * k32));
+  const OqU4 c0 = {walker, step, elec, 0u};
+  const OqU4 r0 = oq_philox(c0, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const float k24 = 5.9604644775390625e-08f;                  // 2^-24
+  const float a = sqrtf(-2.0f * __logf(((float)(r0.x >> 8) + 1.0f) * k24));   // (0, 1]
+  const float b = sqrtf(-2.0f * __logf(((float)(r0.z >> 8) + 1.0f) * k24));
   float s, c;
-  __sincosf(6.283185307179586f * ((float)r0.y * k32), &s, &c);
-  const float c2 = __cosf(6.283185307179586f * ((float)r0.w * k32));   // third normal only
+  __sincosf(6.283185307179586f * ((float)(r0.y >> 8) * k24), &s, &c);
+  const float c2 = __cosf(6.283185307179586f * ((float)(r0.w >> 8) * k24));   // third normal only
   n3[0] = (double)(a * c);
   n3[1] = (double)(a * s);
   n3[2] = (double)(b * c2);
-  u = (double)r1.x * 2.3283064365386963e-10;   // in [0, 1)
+  const uint32_t lo = ((r0.x & 255u) << 24) | ((r0.y & 255u) << 16) | ((r0.z & 255u) << 8) |
+                      (r0.w & 255u);
+  u = (double)lo * 2.3283064365386963e-10;                     // in [0, 1)
 }
 
 // reciprocal / reciprocal square root in the working precision

@@ -18,7 +18,7 @@
 //   3. features at x' = x + d -> network -> log q(-d | x');
 //   4. oq_try_move accepts with |psi(x')/psi(x)|^2 q(x|x') / q(x'|x)
 //      (Sherman-Morrison update on acceptance).
-// Random numbers: Philox counters (walker, sweep, electron, stream 0/1) for
+// Random numbers: Philox counters (walker, sweep, electron, stream 0) for
 // the normals and the acceptance uniform, stream 2 for the component.
 #pragma once
 #include "oqmc_batch.cuh"
