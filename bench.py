@@ -974,7 +974,7 @@ def run_learned(a):
     feat, tgt = collect_training_set(ens, n_cfg, 8, step)
     t1.record(stream)
     mlp = MLPProposal(seed=11 + rank)
-    n_train, batch = (300 if a.quick else 2000), 8192
+    n_train, batch = (300 if a.quick else 10000), 8192
     torch.cuda.nvtx.range_push("mlp_train")
     hist = train_proposal(mlp, feat, tgt, steps=n_train, batch=batch, lr=2e-3, log_every=500)
     t2.record(stream)
