@@ -52,3 +52,20 @@ def test_spline_refused_by_analytic_radial_kernels():
     X = torch.as_tensor(seeded_walkers(s, 64, 0.9, 0), device="cuda")
     with pytest.raises(NotImplementedError):
         BatchedSampler([ctx], [X], [0.5], cap=1)
+
+
+def test_spline_optimiser_inputs_match_oracle():
+    """Jastrow-parameter derivatives on a splined basis: the orbitals enter
+    only through the gradient of ln|psi|."""
+    import json
+    from omegaqmc_b200.optim import raw_to_flat, walker_derivatives
+    s, d = golden_system("h2o_spline")
+    pc = {k: {kk: np.asarray(vv, dtype=np.float64) for kk, vv in v.items()}
+          for k, v in json.loads(str(d["spec"]))["params_corr"].items()}
+    ctx = GTOContext(s)
+    X = seeded_walkers(s, 130, 0.8, 22)
+    e, dl, de = walker_derivatives(ctx, X, pc)
+    rl, re_ = O.param_derivatives(s, X)
+    ref_dl, ref_de = raw_to_flat(rl, pc, s), raw_to_flat(re_, pc, s)
+    assert np.max(np.abs(dl - ref_dl) / (np.abs(ref_dl).max(axis=0) + 1.0)) < 1e-10
+    assert np.max(np.abs(de - ref_de) / (np.abs(ref_de).max(axis=0) + 1.0)) < 1e-9

@@ -113,3 +113,23 @@ def test_md_paths_without_support_refuse_it():
         BatchedSampler([ctx], [torch.as_tensor(X, device="cuda")], [0.5], cap=1)
     ctx.set_multidet(None)
     assert ctx.multidet_info() == (0, 0, 0, 0)
+
+
+def test_md_optimiser_inputs_match_oracle():
+    """Jastrow-parameter derivatives with a multi-determinant trial (the
+    linear-method inputs, vmcopt_gto_linear.py:686-703, which accepts
+    trials): the Slater part enters only through the gradient of ln|psi|."""
+    from omegaqmc_b200.optim import raw_to_flat, walker_derivatives
+    s, d = golden_system("h2o_md")
+    spec = __import__("json").loads(str(d["spec"]))
+    pc = {k: {kk: np.asarray(vv, dtype=np.float64) for kk, vv in v.items()}
+          for k, v in spec["params_corr"].items()}
+    ctx = GTOContext(s)
+    X = seeded_walkers(s, 130, 0.8, 21)
+    e, dl, de = walker_derivatives(ctx, X, pc)
+    rl, re_ = O.param_derivatives(s, X)
+    ref_dl, ref_de = raw_to_flat(rl, pc, s), raw_to_flat(re_, pc, s)
+    assert np.max(np.abs(dl - ref_dl) / (np.abs(ref_dl).max(axis=0) + 1.0)) < 1e-10
+    assert np.max(np.abs(de - ref_de) / (np.abs(ref_de).max(axis=0) + 1.0)) < 1e-9
+    ref_e = O.evaluate(s, X)["e_loc"]
+    assert np.max(np.abs(e - ref_e)) / (0.5 * np.abs(ref_e).max() + 1.0) < 1e-9
