@@ -229,7 +229,9 @@ int oqmc_set_proposal(oqmc_ctx* ctx, int kind, double r0, double fmin_frac);
  * in FP64 only (oqmc_sweeps_noalloc included); the batched, learned-proposal
  * and tensor-core paths refuse it.  ndet = 0 returns to the single determinant
  * of the descriptor.  Sampler state sizes (oqmc_state_bytes) change with the
- * expansion. */
+ * expansion.  With an expansion, oqmc_eval and oqmc_log_psi refresh a
+ * scratch state kept on the context: it grows with cudaMalloc when a call
+ * has more walkers than any before (synchronising that call's stream). */
 int oqmc_set_multidet(oqmc_ctx* ctx, int ndet, int ncol, const double* C, const double* coef,
                       const int* occ_up, const int* occ_dn);
 /* Terms, distinct up / down determinants and padded orbital columns of the
