@@ -78,6 +78,7 @@ _lib = None
 # (name, restype, argtypes)
 _SIGS = [
     ("oqmc_version", ctypes.c_char_p, []),
+    ("oqmc_set_move_kind", c_int, [c_void_p, c_int]),
     ("oqmc_set_multidet", c_int, [c_void_p, c_int, c_int, P_double, P_double, P_int, P_int]),
     ("oqmc_multidet_info", c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int),
                                    ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),

@@ -289,6 +289,11 @@ class GTOContext:
         self._check(self.lib.oqmc_multidet_info(self._h, *[ctypes.byref(x) for x in v]))
         return tuple(x.value for x in v)
 
+    def set_move_kind(self, kind):
+        """0: single-electron sweeps (default); 1: the reference's all-electron
+        steps (``metropolis_move_alle``), one proposal per sweep."""
+        self._check(self.lib.oqmc_set_move_kind(self._h, int(kind)))
+
     def set_proposal(self, kind, r0=1.0, fmin_frac=0.05):
         """0: fixed-width Gaussian (reference); 1: nucleus-scaled width."""
         self._check(self.lib.oqmc_set_proposal(self._h, int(kind), float(r0), float(fmin_frac)))

@@ -516,6 +516,13 @@ int oqmc_multidet_info(const oqmc_ctx* ctx, int* ndet, int* nu_up, int* nu_dn, i
   return OQ_OK;
 }
 
+int oqmc_set_move_kind(oqmc_ctx* ctx, int kind) {
+  if (!ctx) return OQ_ERR_ARG;
+  if (kind != 0 && kind != 1) return set_err(ctx, OQ_ERR_ARG, "move kind must be 0 or 1%s");
+  ctx->move_kind = kind;
+  return OQ_OK;
+}
+
 int oqmc_set_proposal(oqmc_ctx* ctx, int kind, double r0, double fmin_frac) {
   if (!ctx) return OQ_ERR_ARG;
   if (kind < 0 || kind > 1 || (kind == 1 && (!(r0 > 0.0) || !(fmin_frac > 0.0) || fmin_frac > 1.0)))
@@ -1183,8 +1190,18 @@ static int pick_wpb(oqmc_ctx* ctx, int wpb, int precision, size_t* sm) {
 
 static int launch_moves(oqmc_ctx* ctx, const OqMoveArgs& m, int wpb, size_t sm, int precision,
                         void* stream) {
-  const OqLaunch L = make_launch(ctx, stream, sm);
   const int mixed = precision == OQ_PREC_MIXED;
+  if (ctx->move_kind == 1 && m.mode == 0) {
+    // all-electron steps: table-driven FP64 evaluation of the proposals
+    const OqLaunch La = make_launch(ctx, stream, smem_sys_c64(ctx));
+    cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_moves_alle_##N(La, m, mixed)
+    OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+    OQ_CUDA(ctx, err);
+    return OQ_OK;
+  }
+  const OqLaunch L = make_launch(ctx, stream, sm);
   if (ctx->mlp && m.mode == 0) {
     OqMoveArgs mm = m;
     const void* C = (const void*)ctx->d_C32;
@@ -1289,6 +1306,12 @@ int oqmc_sweeps(oqmc_ctx* ctx, double* X, int W, void* state, int precision, int
     return set_err(ctx, OQ_ERR_ARG, "null buffer%s");
   if (ctx->mlp && precision != OQ_PREC_MIXED)
     return set_err(ctx, OQ_ERR_UNSUPPORTED, "the learned proposal runs in mixed precision only%s");
+  if (ctx->mlp && ctx->move_kind == 1)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED,
+                   "the learned proposal moves one electron at a time%s");
+  if (ctx->md && ctx->move_kind == 1)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED,
+                   "all-electron steps are built for single determinants%s");
   if (ctx->md)
     return md_sweeps(ctx, X, W, state, precision, n_sweeps, measure_every, step, seed, step_base,
                      sums, el_trace, eparts_last, stream);

@@ -32,6 +32,7 @@ struct oqmc_ctx {
   double* d_spl_coef;
   double tight_alpha;
   int proposal;           // 0 fixed-width Gaussian, 1 nucleus-scaled width
+  int move_kind;          // 0 single-electron sweeps, 1 all-electron steps
   OqSpecModule* spec;     // run-time specialised kernels, or null
   int use_tc;             // mixed local energy on the tensor cores
   unsigned char* d_Btc;   // split MO-coefficient operands of k_eloc_tc

@@ -169,3 +169,22 @@ cudaError_t OQ_FN(oq_md_local)(const OqLaunch& L, const OqMdTables& T, const OqM
   }
   return M == 16 ? md_local_m<16>(L, T, st, a, logpsi, grad, lap) : cudaErrorInvalidValue;
 }
+
+cudaError_t OQ_FN(oq_moves_alle)(const OqLaunch& L, const OqMoveArgs& a, int mixed) {
+  const int tpb = 128, nb = (a.W + tpb - 1) / tpb;
+  cudaError_t e;
+  if (mixed) {
+    e = oq_smem_attr(k_moves_alle<OQ_N, float>, L.smem);
+    if (e != cudaSuccess) return e;
+    k_moves_alle<OQ_N, float><<<nb, tpb, L.smem, L.stream>>>(
+        L.sys, L.C64, a.pos, (float*)a.ainv, a.logdet, a.W, a.n_steps, a.step, a.seed,
+        a.step_base, a.acc_sum, L.flags);
+  } else {
+    e = oq_smem_attr(k_moves_alle<OQ_N, double>, L.smem);
+    if (e != cudaSuccess) return e;
+    k_moves_alle<OQ_N, double><<<nb, tpb, L.smem, L.stream>>>(
+        L.sys, L.C64, a.pos, (double*)a.ainv, a.logdet, a.W, a.n_steps, a.step, a.seed,
+        a.step_base, a.acc_sum, L.flags);
+  }
+  return cudaGetLastError();
+}

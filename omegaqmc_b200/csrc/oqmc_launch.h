@@ -24,6 +24,7 @@ struct OqLaunch {
   cudaError_t oq_refresh_##N(const OqLaunch& L, const double* pos, int W, void* ainv, \
                              double* logdet, int mixed);                              \
   cudaError_t oq_moves_##N(const OqLaunch& L, const OqMoveArgs& a, int wpb, int mixed); \
+  cudaError_t oq_moves_alle_##N(const OqLaunch& L, const OqMoveArgs& a, int mixed);     \
   cudaError_t oq_eloc_##N(const OqLaunch& L, const OqElocArgs& a, int mixed);           \
   cudaError_t oq_eloc_tc_##N(const OqLaunch& L, const OqElocArgs& a, const void* Bpack, \
                              int nbf);                                                \

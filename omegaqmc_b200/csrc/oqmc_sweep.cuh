@@ -320,6 +320,98 @@ k_refresh(const OqSystem* __restrict__ gsys, const double* __restrict__ gC,
   if (!ok) atomicOr(flags, OQ_FLAG_SINGULAR);
 }
 
+// All-electron Metropolis steps, the reference's move (metropolis_move_alle
+// and metropolis_move_1w, OmegaQMC/vmc_gto.py:815-905): every electron is
+// displaced by step * N(0, 1); a proposal with an electron-electron or
+// electron-nucleus distance below 1e-4 bohr is rejected (ratio 0,
+// constants.py:23); otherwise it is accepted when u < exp(2 (ln|psi'| -
+// ln|psi|)), ln|psi| = log|det up| + log|det down| + J evaluated afresh in
+// FP64 (Gauss-Jordan inverses of the proposed Slater matrices, which become
+// the state's inverses on acceptance).  Random numbers: electron e's
+// normals from the Philox block (walker, step, e, 0), u from electron 0's
+// block.  One thread per walker, state in global memory (layout above).
+template <int NOCC, typename Real>
+__global__ void __launch_bounds__(128)
+k_moves_alle(const OqSystem* __restrict__ gsys, const double* __restrict__ gC, double* pos,
+             Real* __restrict__ ainv, double* __restrict__ logdet, int W, int n_steps,
+             double step, uint64_t seed, uint64_t step_base, double* acc_sum,
+             unsigned* __restrict__ flags) {
+  constexpr int NE = 2 * NOCC;
+  extern __shared__ __align__(16) unsigned char smem[];
+  OqSystem& S = *reinterpret_cast<OqSystem*>(smem);
+  double* C = reinterpret_cast<double*>(smem + sizeof(OqSystem));
+  oq_load_system(&S, gsys);
+  for (int i = threadIdx.x; i < S.nbf * NOCC; i += blockDim.x) C[i] = gC[i];
+  __syncthreads();
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = w < W;
+  int nacc = 0;
+  if (live) {
+    double x[3 * NE];
+    for (int k = 0; k < 3 * NE; ++k) x[k] = pos[(size_t)k * W + w];
+    double lpsi = logdet[w] + oq_jastrow_value(S, x, NE);
+    for (int t = 0; t < n_steps; ++t) {
+      const uint32_t gstep = (uint32_t)(step_base + t);
+      double xn[3 * NE], u = 0.0;
+      for (int e = 0; e < NE; ++e) {
+        double n3[3], ue;
+        oq_move_randoms(seed, (uint32_t)w, gstep, (uint32_t)e, n3, ue);
+        if (e == 0) u = ue;
+        for (int c = 0; c < 3; ++c) xn[3 * e + c] = x[3 * e + c] + step * n3[c];
+      }
+      bool valid = true;
+      for (int i = 0; i < NE; ++i) {
+        for (int j = i + 1; j < NE; ++j) {
+          const double dx = xn[3 * i] - xn[3 * j], dy = xn[3 * i + 1] - xn[3 * j + 1],
+                       dz = xn[3 * i + 2] - xn[3 * j + 2];
+          valid = valid && (dx * dx + dy * dy + dz * dz >= 1e-8);
+        }
+        for (int I = 0; I < S.natm; ++I) {
+          const double dx = xn[3 * i] - S.nuc[I][0], dy = xn[3 * i + 1] - S.nuc[I][1],
+                       dz = xn[3 * i + 2] - S.nuc[I][2];
+          valid = valid && (dx * dx + dy * dy + dz * dz >= 1e-8);
+        }
+      }
+      if (!valid) continue;
+      double An[2][NOCC][NOCC], ld = 0.0;
+      bool ok = true;
+      for (int s = 0; s < 2; ++s) {
+        double Sm[NOCC][NOCC];
+        for (int i = 0; i < NOCC; ++i) {
+          const int e = 2 * i + s;
+          double mv[NOCC];
+          oq_mo_val<NOCC>(S, C, xn[3 * e], xn[3 * e + 1], xn[3 * e + 2], mv);
+#pragma unroll
+          for (int m = 0; m < NOCC; ++m) Sm[i][m] = mv[m];
+        }
+        double lds;
+        ok = ok && oq_invert<NOCC>(Sm, An[s], lds);
+        ld += lds;
+      }
+      if (!ok) continue;
+      const double lpn = ld + oq_jastrow_value(S, xn, NE);
+      if (!isfinite(lpn)) { atomicOr(flags, OQ_FLAG_NAN); continue; }
+      // an old state with psi = 0 (log -inf) accepts any finite proposal
+      if (isfinite(lpsi) && !(log(u) < 2.0 * (lpn - lpsi))) continue;
+      ++nacc;
+      lpsi = lpn;
+      for (int k = 0; k < 3 * NE; ++k) x[k] = xn[k];
+      for (int s = 0; s < 2; ++s)
+        for (int m = 0; m < NOCC; ++m)
+          for (int j = 0; j < NOCC; ++j)
+            ainv[(size_t)((s * NOCC + m) * NOCC + j) * W + w] = (Real)An[s][m][j];
+      logdet[w] = ld;
+    }
+    for (int k = 0; k < 3 * NE; ++k) pos[(size_t)k * W + w] = x[k];
+  }
+  if (acc_sum) {
+    double v = (double)nacc * NE;   // accepted electron moves, as the sweeps count them
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(acc_sum, v);
+  }
+}
+
 // number of doubles reduced per measured sweep
 #define OQ_NSUM 8   // ee, en, ke, eloc, eloc^2, accepted moves, finite walkers, pad
 

@@ -98,15 +98,17 @@ def get_vmc_gto_func(mf, params_corr, cusp_scheme="Quady2025", gr_scheme="scheme
                      force_estimator="simple", force_warp="swct", prefix="vmc",
                      symmop_list=None, cluster_idx=None, mo_relax=True, trial=None,
                      jastrow_config=None, *, params_cusp=None, precision="fp64",
-                     proposal="plain", specialize=True):
+                     proposal="plain", specialize=True, move="single"):
     """Build a callable VMC driver (``vmc_gto.py:1620-1765``).
 
     Extra keywords (not in the reference): ``params_cusp`` supplies cusp
     constants instead of fitting them; ``precision`` is ``"fp64"`` or
     ``"mixed"``; ``proposal`` is ``"plain"`` (fixed-width Gaussian) or
     ``"scaled"`` (nucleus-scaled width); ``specialize`` compiles kernels for
-    this molecule (NVRTC) when available.  A multi-determinant ``trial``
-    samples in FP64 through the library's multi-determinant kernels."""
+    this molecule (NVRTC) when available; ``move`` is ``"single"``
+    (single-electron sweeps) or ``"all"`` (the reference's all-electron
+    step, one proposal moving every electron per sweep).  A multi-determinant
+    ``trial`` samples in FP64 through the library's multi-determinant kernels."""
     if trial is not None and precision != "fp64":
         raise ValueError("multi-determinant trials are sampled in precision='fp64'")
     if symmop_list not in (None, "E", ["E"]):
@@ -127,7 +129,7 @@ def get_vmc_gto_func(mf, params_corr, cusp_scheme="Quady2025", gr_scheme="scheme
     print("Begin time: {}".format(timestamp_init))
     return VMCDriverGTO(mf, params_corr, params_cusp, prefix, timestamp_init,
                         precision=precision, proposal=proposal, specialize=specialize,
-                        jastrow_config=jastrow_config, trial=trial)
+                        jastrow_config=jastrow_config, trial=trial, move=move)
 
 
 class VMCDriverGTO:
@@ -135,7 +137,7 @@ class VMCDriverGTO:
 
     def __init__(self, mf, params_corr, params_cusp, prefix, timestamp_init,
                  precision="fp64", proposal="plain", specialize=True, jastrow_config=None,
-                 trial=None):
+                 trial=None, move="single"):
         self.mf = mf
         self.params_corr = params_corr
         self.params_cusp = params_cusp
@@ -151,6 +153,14 @@ class VMCDriverGTO:
             self.ctx.set_proposal(1, 1.0, 0.05)
         elif proposal != "plain":
             raise ValueError("proposal must be 'plain' or 'scaled'")
+        # move="all": the reference's all-electron Gaussian step
+        # (metropolis_move_alle, vmc_gto.py:815-838), one proposal per sweep
+        if move == "all":
+            if proposal != "plain":
+                raise ValueError("all-electron steps use the plain Gaussian proposal")
+            self.ctx.set_move_kind(1)
+        elif move != "single":
+            raise ValueError("move must be 'single' or 'all'")
         self.precision = precision
         self.ofname_chkpt = prefix + ".chk"
         self.timestamp_init = timestamp_init
