@@ -217,7 +217,7 @@ int oqmc_sweeps_noalloc(oqmc_ctx* ctx, double* walkers, int W, int precision,
  * exact proposal-density ratio, so the stationary distribution is unchanged
  * while core electrons move with core-sized steps. */
 int oqmc_set_proposal(oqmc_ctx* ctx, int kind, double r0, double fmin_frac);
-/* Move kind of oqmc_sweeps / oqmc_sweeps_noalloc: 0 (default) single-electron
+/* Move kind of oqmc_sweeps: 0 (default) single-electron
  * sweeps (n_e proposals per sweep, Sherman-Morrison updates); 1 the
  * reference's all-electron step (metropolis_move_alle + metropolis_move_1w,
  * OmegaQMC/vmc_gto.py:815-905): per "sweep" one proposal moving every
@@ -225,7 +225,10 @@ int oqmc_set_proposal(oqmc_ctx* ctx, int kind, double r0, double fmin_frac);
  * afresh in FP64.  The proposal width setting (oqmc_set_proposal) applies
  * to single-electron sweeps only; the learned proposal and
  * multi-determinant trials refuse kind 1.  The accepted-move sum counts
- * electron moves in both kinds: an accepted all-electron step adds n_e. */
+ * electron moves in both kinds: an accepted all-electron step adds n_e.
+ * oqmc_sweeps_noalloc refuses kind 1 (OQ_ERR_UNSUPPORTED): the first launch
+ * of the all-electron kernel can grow the device's local-memory reservation
+ * (its per-thread stack exceeds the default), which is an allocation. */
 int oqmc_set_move_kind(oqmc_ctx* ctx, int kind);
 /* Multi-determinant trial (the `trial` dict of get_psi_fun /
  * get_vmc_gto_func, OmegaQMC/psi/gto.py:846-863, 1312-1488):

@@ -125,6 +125,8 @@ static void compute_split(oqmc_ctx* ctx) {
 }
 
 // Record an error on a context (used by entry points in other files).
+int oq_ctx_move_kind(const oqmc_ctx* ctx) { return ctx->move_kind; }
+
 int oq_ctx_set_error(oqmc_ctx* ctx, int code, const char* msg) {
   return set_err(ctx, code, "%s", msg);
 }

@@ -50,6 +50,7 @@ static cudaError_t scratch_address(void** out) {
 }
 
 int oq_ctx_set_error(oqmc_ctx* ctx, int code, const char* msg);
+int oq_ctx_move_kind(const oqmc_ctx* ctx);
 
 extern "C" int oqmc_sweeps_noalloc(oqmc_ctx* ctx, double* walkers, int W, int precision,
                                    int n_sweeps, int measure_every, double step,
@@ -59,6 +60,12 @@ extern "C" int oqmc_sweeps_noalloc(oqmc_ctx* ctx, double* walkers, int W, int pr
   if (W < 0 || n_sweeps < 0 || (precision != OQ_PREC_FP64 && precision != OQ_PREC_MIXED))
     return oq_ctx_set_error(ctx, OQ_ERR_ARG, "bad arguments");
   if (W == 0 || n_sweeps == 0) return OQ_OK;
+  // the all-electron kernel needs more per-thread stack than the driver's
+  // default local-memory reservation; growing that reservation on its first
+  // launch is a device allocation
+  if (oq_ctx_move_kind(ctx) != 0)
+    return oq_ctx_set_error(ctx, OQ_ERR_UNSUPPORTED,
+                            "all-electron steps are not allocation-free; use oqmc_sweeps");
   const size_t need = oqmc_state_bytes(ctx, W, precision);
   if (need > (size_t)OQ_NOALLOC_SCRATCH_BYTES)
     return oq_ctx_set_error(ctx, OQ_ERR_ARG,

@@ -99,3 +99,20 @@ def test_move_kind_arguments_and_refusals():
     ens = WalkerEnsemble(md, seeded_walkers(s, 64, 0.5, 0), "fp64", seed=1)
     with pytest.raises(NotImplementedError):
         ens.run(2, 0.5)
+
+
+def test_noalloc_entry_refuses_all_electron_steps():
+    import ctypes
+    from omegaqmc_b200 import _lib as L
+    lib = L.load()
+    s = _sys("H2")
+    ctx = GTOContext(s)
+    ctx.set_move_kind(1)
+    X = ctx.walkers_tensor(seeded_walkers(s, 64, 0.5, 0))
+    sums = torch.zeros(1, 8, dtype=torch.float64, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = lib.oqmc_sweeps_noalloc(ctx._h, ctypes.c_void_p(X.data_ptr()), 64, L.PREC_FP64, 1, 1,
+                                 0.5, ctypes.c_uint64(1), ctypes.c_uint64(0),
+                                 ctypes.c_void_p(sums.data_ptr()), None, None, st)
+    assert rc == L.OQ_ERR_UNSUPPORTED
+    assert b"allocation-free" in lib.oqmc_last_error(ctx._h)
