@@ -38,6 +38,28 @@ def test_driver_runs_logs_and_restarts(tmp_path, capsys):
         drv(1, num_walkers=8, compute_gradients=True)
 
 
+def test_driver_all_electron_moves(tmp_path, capsys):
+    """move="all": the reference's all-electron step through the driver."""
+    mf = generate_molecular_orbitals("H 0 0 -0.7; H 0 0 0.7", basis="sto-3g")
+    J2 = {"J2_pade": {"like": np.array([0.25, 1.0]), "unlike": np.array([0.5, 1.0])}}
+    with pytest.raises(ValueError):
+        get_vmc_gto_func(mf, J2, cusp_scheme=None, prefix=str(tmp_path / "x"), move="some")
+    with pytest.raises(ValueError):
+        get_vmc_gto_func(mf, J2, cusp_scheme=None, prefix=str(tmp_path / "x"), move="all",
+                         proposal="scaled")
+    drv = get_vmc_gto_func(mf, J2, cusp_scheme=None, prefix=str(tmp_path / "h2a"), move="all")
+    log = str(tmp_path / "h2a.log")
+    drv(5, num_walkers=512, num_steps_per_block=20, num_blocks=4, num_blocks_equil=2,
+        num_steps_basin=20, fname_log=log)
+    rows = [l.split() for l in open(log).read().splitlines()[1:]]
+    assert len(rows) == 4
+    E = np.array([float(r[1]) for r in rows])
+    acc = np.array([float(r[-1]) for r in rows])
+    assert np.all(E < -0.9) and np.all(E > -1.3)
+    # step adaptation drives the all-electron acceptance towards 0.4
+    assert np.all((acc > 0.2) & (acc < 0.7)), acc
+
+
 def test_get_psi_fun_matches_golden_per_walker():
     mf, params, cusp, d = load_golden("h2o_cusp")
     log_psi, (e_ee, e_nn, e_en, e_ke), (get_mo, _), _ = get_psi_fun(mf, params_cusp=cusp)
