@@ -223,8 +223,8 @@ int oqmc_set_proposal(oqmc_ctx* ctx, int kind, double r0, double fmin_frac);
  * OmegaQMC/vmc_gto.py:815-905): per "sweep" one proposal moving every
  * electron by step * N(0, 1), accepted on the ratio of |psi|^2 evaluated
  * afresh in FP64.  The proposal width setting (oqmc_set_proposal) applies
- * to single-electron sweeps only; the learned proposal and
- * multi-determinant trials refuse kind 1.  The accepted-move sum counts
+ * to single-electron sweeps only; the learned proposal, multi-determinant
+ * trials and oqmc_batch_bind refuse kind 1.  The accepted-move sum counts
  * electron moves in both kinds: an accepted all-electron step adds n_e.
  * oqmc_sweeps_noalloc refuses kind 1 (OQ_ERR_UNSUPPORTED): the first launch
  * of the all-electron kernel can grow the device's local-memory reservation

@@ -311,6 +311,10 @@ int oqmc_batch_bind(oqmc_batch* b, const oqmc_batch_system* sys) {
       return berr(b, OQ_ERR_UNSUPPORTED,
                   "system " + std::to_string(k) + " has a multi-determinant trial; the "
                   "batched kernel samples single determinants");
+    if (c->move_kind != 0)
+      return berr(b, OQ_ERR_UNSUPPORTED,
+                  "system " + std::to_string(k) + " is set to all-electron steps; the "
+                  "batched kernel runs single-electron sweeps");
     OqBatchSys& d = b->hsys[k];
     memset(&d, 0, sizeof(d));
     d.sys = c->d_sys;

@@ -26,6 +26,7 @@ from datetime import datetime
 import numpy as np
 import torch
 
+from .batch import BatchedSampler
 from .context import GTOContext
 from .cusp import cusp_params_for_mol
 from . import replicas as RP
@@ -98,7 +99,7 @@ def get_vmc_gto_func(mf, params_corr, cusp_scheme="Quady2025", gr_scheme="scheme
                      force_estimator="simple", force_warp="swct", prefix="vmc",
                      symmop_list=None, cluster_idx=None, mo_relax=True, trial=None,
                      jastrow_config=None, *, params_cusp=None, precision="fp64",
-                     proposal="plain", specialize=True, move="single"):
+                     proposal="plain", specialize=True, move="single", persistent=True):
     """Build a callable VMC driver (``vmc_gto.py:1620-1765``).
 
     Extra keywords (not in the reference): ``params_cusp`` supplies cusp
@@ -107,8 +108,11 @@ def get_vmc_gto_func(mf, params_corr, cusp_scheme="Quady2025", gr_scheme="scheme
     ``"scaled"`` (nucleus-scaled width); ``specialize`` compiles kernels for
     this molecule (NVRTC) when available; ``move`` is ``"single"``
     (single-electron sweeps) or ``"all"`` (the reference's all-electron
-    step, one proposal moving every electron per sweep).  A multi-determinant
-    ``trial`` samples in FP64 through the library's multi-determinant kernels."""
+    step, one proposal moving every electron per sweep); ``persistent`` runs
+    the production blocks as fused persistent launches (refresh, sweeps and
+    local energies in one kernel, the same Markov chain) wherever the batched
+    kernel accepts the configuration.  A multi-determinant ``trial`` samples in
+    FP64 through the library's multi-determinant kernels."""
     if trial is not None and precision != "fp64":
         raise ValueError("multi-determinant trials are sampled in precision='fp64'")
     if symmop_list not in (None, "E", ["E"]):
@@ -129,7 +133,8 @@ def get_vmc_gto_func(mf, params_corr, cusp_scheme="Quady2025", gr_scheme="scheme
     print("Begin time: {}".format(timestamp_init))
     return VMCDriverGTO(mf, params_corr, params_cusp, prefix, timestamp_init,
                         precision=precision, proposal=proposal, specialize=specialize,
-                        jastrow_config=jastrow_config, trial=trial, move=move)
+                        jastrow_config=jastrow_config, trial=trial, move=move,
+                        persistent=persistent)
 
 
 class VMCDriverGTO:
@@ -137,7 +142,7 @@ class VMCDriverGTO:
 
     def __init__(self, mf, params_corr, params_cusp, prefix, timestamp_init,
                  precision="fp64", proposal="plain", specialize=True, jastrow_config=None,
-                 trial=None, move="single"):
+                 trial=None, move="single", persistent=True):
         self.mf = mf
         self.params_corr = params_corr
         self.params_cusp = params_cusp
@@ -161,6 +166,8 @@ class VMCDriverGTO:
             self.ctx.set_move_kind(1)
         elif move != "single":
             raise ValueError("move must be 'single' or 'all'")
+        self.proposal = proposal
+        self.persistent = bool(persistent)
         self.precision = precision
         self.ofname_chkpt = prefix + ".chk"
         self.timestamp_init = timestamp_init
@@ -168,6 +175,44 @@ class VMCDriverGTO:
         self.results = None
 
     # ------------------------------------------------------------------
+    def _fused_sampler(self, ens, step, n_meas):
+        """The fused persistent launch (FP64 refresh, sweeps and local energies
+        in one kernel per <= 50 sweeps) for the production blocks.  Same
+        proposals, acceptance and random numbers as the separate move and
+        local-energy kernels (Philox counters (walker, sweep, electron)), so
+        the chain is the same.  Its tile shape is autotuned on a copy of the
+        walkers, whose positions are then restored, so tuning leaves the
+        chain untouched.  None where the batched kernel refuses the
+        configuration (radial splines, multi-determinant trials, all-electron
+        steps) or NVRTC is absent; the production blocks then run on the
+        separate kernels."""
+        if not self.persistent:
+            return None
+        try:
+            fused = BatchedSampler([self.ctx], [ens.X.clone()], [step], precision=self.precision,
+                                   proposal=self.proposal, scale_r0=1.0, scale_fmin=0.05,
+                                   cap=max(1, n_meas))
+        except NotImplementedError:
+            return None
+        fused.tune(4, seed=(ens.seed ^ 0x7E57) & 0x7FFFFFFF)
+        fused.walkers[0].copy_(ens.X)
+        return fused
+
+    def _fused_block(self, fused, ens, n_sw, every, n_meas):
+        """One production block on the fused launch: launches of at most 50
+        sweeps (the refresh cadence of the separate kernels), each a multiple
+        of the measurement interval, continuing the ensemble's sweep counter
+        and measurement slots.  Returns the block's (n_meas, 8) sums."""
+        fused.reset(ens.step_count)
+        done = 0
+        while done < n_sw:
+            chunk = min(n_sw - done, max(every, (ens.refresh_every // every) * every))
+            fused.run(chunk, every, ens.seed)
+            done += chunk
+        ens.step_count += n_sw
+        ens.X.copy_(fused.walkers[0])
+        return fused.sums[0][:n_meas]
+
     def _save(self, path, data):
         try:
             import h5py
@@ -253,10 +298,14 @@ class VMCDriverGTO:
               " acc_ratio", file=fout)
         t_prev = datetime.now()
         block_cnt = block_cnt_start - 1
+        fused = self._fused_sampler(ens, mc_stepsize, num_steps_per_block)
         for block_cnt in range(block_cnt_start, block_cnt_start + num_blocks):
             n_sw = num_steps_per_block * num_steps_decorr
-            sums = RP.combine_sums(ens.run(n_sw, mc_stepsize,
-                                           measure_every=num_steps_decorr)).cpu().numpy()
+            if fused is not None:
+                blk = self._fused_block(fused, ens, n_sw, num_steps_decorr, num_steps_per_block)
+            else:
+                blk = ens.run(n_sw, mc_stepsize, measure_every=num_steps_decorr)
+            sums = RP.combine_sums(blk).cpu().numpy()
             nv = np.maximum(sums[:, 6], 1.0)
             ee_s, en_s, ke_s = sums[:, 0] / nv, sums[:, 1] / nv, sums[:, 2] / nv
             E_loc_s = ee_s + en_s + ke_s + self.enr_nn
@@ -273,6 +322,9 @@ class VMCDriverGTO:
             t_prev = t_cur
         if fout is not sys.stdout:
             fout.close()
+        if fused is not None:
+            fused.close()
+            ens.refresh()
         t_fin = datetime.now()
         print("End time: {}\t({:.6f} seconds total)".format(
             t_fin, (t_fin - self.timestamp_init).total_seconds()))

@@ -60,6 +60,24 @@ def test_driver_all_electron_moves(tmp_path, capsys):
     assert np.all((acc > 0.2) & (acc < 0.7)), acc
 
 
+def test_driver_fused_blocks_follow_the_split_chain(tmp_path):
+    """Production blocks on the fused persistent launch continue the same
+    Markov chain as the separate move and local-energy kernels."""
+    mf = generate_molecular_orbitals("H 0 0 -0.7; H 0 0 0.7", basis="sto-3g")
+    J2 = {"J2_pade": {"like": np.array([0.25, 1.0]), "unlike": np.array([0.5, 1.0])}}
+    out = {}
+    for fused in (True, False):
+        drv = get_vmc_gto_func(mf, J2, cusp_scheme=None, prefix=str(tmp_path / f"h2{fused}"),
+                               persistent=fused)
+        drv(31, num_walkers=512, num_steps_per_block=30, num_blocks=3, num_blocks_equil=1,
+            num_steps_basin=10, fname_log=str(tmp_path / f"h2{fused}.log"))
+        d = np.load(drv.results["chk"])
+        out[fused] = (d["walkers"], drv.results["E_blocks"])
+    same = np.all(out[True][0] == out[False][0], axis=(1, 2)).mean()
+    assert same > 0.95, same
+    np.testing.assert_allclose(out[True][1], out[False][1], atol=5e-3)
+
+
 def test_get_psi_fun_matches_golden_per_walker():
     mf, params, cusp, d = load_golden("h2o_cusp")
     log_psi, (e_ee, e_nn, e_en, e_ke), (get_mo, _), _ = get_psi_fun(mf, params_cusp=cusp)
