@@ -31,7 +31,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import subprocess
 import sys
@@ -203,6 +202,29 @@ def cpu_reference(system, seconds, nthreads, step, seed=7, n_equil=300):
             f"steps, step {step:.3f}", ser[:, 3])
 
 
+def sweep_launches(ens, n_sweeps, measure_every=1):
+    """Kernels that ``ens.run(n_sweeps)`` launches from the ensemble's current
+    refresh phase (the chunking of WalkerEnsemble.run): per oqmc_sweeps call a
+    layout conversion in and one out, per measurement a move kernel and a
+    local-energy kernel (one more move kernel for sweeps after the last
+    measurement of a call), per FP64 refresh a conversion and the refresh
+    kernel."""
+    since, n, done = ens.since_refresh, 0, 0
+    while done < n_sweeps:
+        chunk = min(n_sweeps - done, ens.refresh_every - since)
+        if measure_every > 1:
+            chunk = max(measure_every, chunk - chunk % measure_every)
+            chunk = min(chunk, n_sweeps - done)
+        m = chunk // measure_every
+        n += 2 + 2 * m + (1 if chunk > m * measure_every else 0)
+        done += chunk
+        since += chunk
+        if since >= ens.refresh_every:
+            n += 2
+            since = 0
+    return n
+
+
 def adapt_step(ens, step, n_chunks=40, chunk=5, target=0.4):
     """Equilibrate with the reference's rule log s += 0.05 (acc - target)
     applied once per chunk of sweeps (OmegaQMC/vmc_gto.py:121-126)."""
@@ -301,6 +323,7 @@ def run_ours(a):
     sums = torch.zeros(K, NSUM, dtype=torch.float64, device=dev)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    n_launch = sweep_launches(ens, K)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -431,7 +454,7 @@ def run_ours(a):
                          "inputs 41 MB are re-read once per 50-sweep launch"},
         "walker_sweeps_per_s": wss, "tau_int": kappa, "tau_source": tau_src,
         "energy": {"mean": e_mean, "serr": e_serr}, "acceptance": acc, "kernel_flags": flags,
-        "gpu_launches": int(math.ceil(K / REFRESH_EVERY)) * 2,
+        "gpu_launches": n_launch,
         "roofline": {"bound": "fp64" if peak_kind == 0 else "fp32",
                      "achieved": achieved / 1e12, "peak": rate / 1e12, "unit": "TFLOP/s",
                      "frac": achieved / rate if rate else None, "traffic": traffic,
@@ -1003,6 +1026,7 @@ def run_learned(a):
         lens.run(max(a.warmup // 10, 3), step)
         probe_ms = timed(lens, 20)[0] / 20
         K_l = max(50, int(ms_p / probe_ms))
+        n_launch_l = sweep_launches(lens, K_l)
         torch.cuda.nvtx.range_push("learned_timed")
         ms_l, e_l, se_l, tau_l, acc_l = timed(lens, K_l)
         torch.cuda.nvtx.range_pop()
@@ -1051,7 +1075,7 @@ def run_learned(a):
         "training": {"collect_ms": collect_ms, "train_ms": train_ms, "loss": hist,
                      "train_tflops": train_tflops},
         "kernel_flags": list(flags),
-        "gpu_launches": int(math.ceil(K_l / REFRESH_EVERY)) * 2,
+        "gpu_launches": n_launch_l,
         "roofline": {"bound": "tensor", "achieved": ach, "peak": bf16_peak, "unit": "TFLOP/s",
                      "frac": ach / bf16_peak if bf16_peak else None, "traffic": None,
                      "kernel": "k_moves_mlp (network flops only, two passes per move)",

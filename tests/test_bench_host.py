@@ -33,3 +33,21 @@ def test_clock_summary_flags_slowdowns_and_empty_records():
     assert c.summary()["samples"] == 2
     empty = bench.ClockSampler(0)
     assert empty.summary()["reasons"] == ["unsampled"]
+
+
+class _Ens:
+    def __init__(self, since=0, every=50):
+        self.since_refresh = since
+        self.refresh_every = every
+
+
+def test_sweep_launch_count_follows_the_ensemble_chunking():
+    # 100 sweeps from a fresh refresh phase: two 50-sweep calls, each with two
+    # layout conversions and 50 move + 50 local-energy kernels, then a refresh
+    # (conversion + refresh kernel) after each
+    assert bench.sweep_launches(_Ens(0), 100) == 2 * (2 + 100 + 2)
+    # 30 sweeps left in the phase: a 30-sweep call, refresh, then 20 more
+    assert bench.sweep_launches(_Ens(20), 50) == (2 + 60 + 2) + (2 + 40)
+    # measurements every 4 sweeps: a 48-sweep call (12 measurements), then 2
+    # sweeps with no measurement still take a move kernel, then the refresh
+    assert bench.sweep_launches(_Ens(0), 50, measure_every=4) == (2 + 24) + (2 + 0 + 1) + 2
