@@ -11,7 +11,7 @@ local-energy kernels through oqmc_sweeps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--precision mixed|fp64] [--system H2O] [--walkers 65536]
-                    [--path persistent|split] [--workload h2o|batched|learned]
+                    [--path persistent|split] [--workload h2o|batched|learned|alle]
 
 value     = walkers x sweeps/s / tau_int(E_L)  (decorrelated samples/s, all ranks)
 tau_int   = kappa of the reference's do_binning_analysis (OmegaQMC/utils.py:86-150)
@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--proposal", default="scaled", choices=["scaled", "plain"])
     ap.add_argument("--eloc", default="cc", choices=["cc", "tc"],
                     help="local energy on CUDA cores (specialised) or tensor cores (tcgen05)")
-    ap.add_argument("--workload", default="h2o", choices=["h2o", "batched", "learned"],
+    ap.add_argument("--workload", default="h2o", choices=["h2o", "batched", "learned", "alle"],
                     help="h2o: the headline H2O metric; batched: H2, LiH, H2O, N2 and "
                          "(H2O)2 in one persistent launch under a CUDA graph; learned: N2 "
                          "with the trained MLP proposal against the plain random walk")
@@ -1108,10 +1108,84 @@ def ncu_traffic(system, precision):
     return d.get(f"{system}/{precision}")
 
 
+def run_alle(a):
+    """The reference's own move on the GPU: all-electron Gaussian steps with
+    |psi|^2 recomputed in FP64 (oqmc_set_move_kind(ctx, 1)), the reference's
+    step adaptation to acceptance 0.4, E_L every step.  One step = one
+    all-electron proposal per walker.  For comparison with the single-electron
+    sweeps of the headline; no roofline (a parity form, not a tuned kernel)."""
+    import torch
+    import torch.distributed as dist
+    from omegaqmc_b200 import replicas as RP
+    from omegaqmc_b200.context import GTOContext
+    from omegaqmc_b200.sampler import WalkerEnsemble, init_walkers_gaussian, NSUM
+    from oracle import gto_oracle as O  # noqa: F401  (tau estimator is the oracle's restatement)
+
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    system = build_system(a.system)
+    ctx = GTOContext(system)
+    ctx.set_move_kind(1)
+    W = a.walkers
+    X0 = init_walkers_gaussian(system, W, 1.0, seed=1000 + rank)
+    ens = WalkerEnsemble(ctx, X0, "fp64", seed=2024 + 7919 * rank, refresh_every=REFRESH_EVERY)
+    stream = torch.cuda.current_stream()
+    step = a.step_size or (3 * 0.1) ** 0.5          # the reference's initial step
+    if not a.quick:
+        if not a.step_size:
+            step = adapt_step(ens, step, n_chunks=200)
+        ens.run(EQUIL_SWEEPS, step)
+    ens.run(max(a.warmup, 3), step)
+    K = a.steps
+    sums = torch.zeros(K, NSUM, dtype=torch.float64, device=dev)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    n_launch = sweep_launches(ens, K)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        ens.run(K, step, sums=sums)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t = torch.tensor([ev0.elapsed_time(ev1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sums = RP.combine_sums(sums)
+    ms_max = float(t[0])
+    s_np = sums.cpu().numpy()
+    series = s_np[:, 3] / np.maximum(s_np[:, 6], 1)
+    e_mean, e_serr, _, kappa = O.binning_analysis(series)
+    acc = float(s_np[:, 5].sum() / (K * W * world * system.n_e))
+    rate = W * world * K / (ms_max * 1e-3)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "decorrelated samples/s, all-electron steps (the reference's move) on the GPU",
+            "value": rate / kappa, "unit": "decorrelated samples/s", "n_gpus": world,
+            "steps": K, "warmup": a.warmup, "ms_per_step": ms_max / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{a.system} cc-pVDZ-shaped, {W} walkers/GPU, all-electron "
+                                   "Gaussian steps, E_L every step, FP64",
+                       "step": step, "parallelism": f"replicas x{world}"},
+            "walker_steps_per_s": rate, "tau_int": kappa, "acceptance": acc,
+            "energy": {"mean": e_mean, "serr": e_serr}, "kernel_flags": ctx.flags(),
+            "gpu_launches": n_launch, "roofline": None, "clocks": clk.summary()}), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "alle":
+        run_alle(a)
     elif a.workload == "batched":
         run_batched(a)
     elif a.workload == "learned":
