@@ -118,7 +118,10 @@ k_eval(const OqSystem* __restrict__ gsys, const double* __restrict__ gC,
   OqSystem& S = *reinterpret_cast<OqSystem*>(smem);
   double* C = reinterpret_cast<double*>(smem + sizeof(OqSystem));
   oq_load_system(&S, gsys);
-  for (int i = threadIdx.x; i < S.nbf * NOCC; i += blockDim.x) C[i] = gC[i];
+  // the count comes from global memory: the shared copy S is complete only
+  // after the barrier below
+  const int nbf_g = gsys->nbf;
+  for (int i = threadIdx.x; i < nbf_g * NOCC; i += blockDim.x) C[i] = gC[i];
   __syncthreads();
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= W) return;
@@ -253,7 +256,10 @@ k_logpsi(const OqSystem* __restrict__ gsys, const double* __restrict__ gC,
   OqSystem& S = *reinterpret_cast<OqSystem*>(smem);
   double* C = reinterpret_cast<double*>(smem + sizeof(OqSystem));
   oq_load_system(&S, gsys);
-  for (int i = threadIdx.x; i < S.nbf * NOCC; i += blockDim.x) C[i] = gC[i];
+  // the count comes from global memory: the shared copy S is complete only
+  // after the barrier below
+  const int nbf_g = gsys->nbf;
+  for (int i = threadIdx.x; i < nbf_g * NOCC; i += blockDim.x) C[i] = gC[i];
   __syncthreads();
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= W) return;
@@ -290,7 +296,10 @@ k_mo_values(const OqSystem* __restrict__ gsys, const double* __restrict__ gC,
   OqSystem& S = *reinterpret_cast<OqSystem*>(smem);
   double* C = reinterpret_cast<double*>(smem + sizeof(OqSystem));
   oq_load_system(&S, gsys);
-  for (int i = threadIdx.x; i < S.nbf * NOCC; i += blockDim.x) C[i] = gC[i];
+  // the count comes from global memory: the shared copy S is complete only
+  // after the barrier below
+  const int nbf_g = gsys->nbf;
+  for (int i = threadIdx.x; i < nbf_g * NOCC; i += blockDim.x) C[i] = gC[i];
   __syncthreads();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)W * 2 * NOCC) return;
