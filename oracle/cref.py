@@ -39,20 +39,38 @@ def _desc(system):
     return pack_system(system)
 
 
+def supports(system):
+    """True when the C restatement covers the system's trial (Padé J1/J2,
+    cusp-corrected s shells, one determinant)."""
+    return (system.md is None and system.bs1 is None and system.bs2 is None
+            and system.j3 is None and system.spl is None)
+
+
+def _check(system):
+    if not supports(system):
+        raise ValueError("the C restatement covers Padé Jastrows, cusp-corrected s shells "
+                         "and single determinants only")
+
+
 def evaluate(system, X, nthreads=0):
-    """(logpsi (W,), eparts (W, 4)) from the C restatement."""
+    """(logpsi (W,), eparts (W, 4): e_ee, e_en, e_ke, E_L) from the C
+    restatement."""
+    _check(system)
     d, keep = _desc(system)
     X = np.ascontiguousarray(X, dtype=np.float64)
     W = X.shape[0]
     lp = np.empty(W)
     ep = np.empty((W, 4))
-    load().vmc_ref_eval(ctypes.byref(d), X.ctypes.data, W, lp.ctypes.data, ep.ctypes.data,
-                        int(nthreads))
+    rc = load().vmc_ref_eval(ctypes.byref(d), X.ctypes.data, W, lp.ctypes.data,
+                             ep.ctypes.data, int(nthreads))
+    if rc != 0:
+        raise ValueError("descriptor outside the C restatement")
     return lp, ep
 
 
 def run(system, X, n_steps, step, seed=0, nthreads=0):
     """Reference-algorithm steps in place on X; returns (series (n,4), acc)."""
+    _check(system)
     d, keep = _desc(system)
     assert X.dtype == np.float64 and X.flags.c_contiguous
     series = np.empty((n_steps, 4))

@@ -393,9 +393,19 @@ static int valid_move(const oqmc_system_desc* d, const double* X) {
   return 1;
 }
 
-/* Full evaluation of W walkers: logpsi (W) and eparts (W x 4). */
+/* The restatement covers Pade J1/J2, cusp-corrected s shells and a single
+ * determinant; descriptors with B-spline, J3 or spline-AO terms are refused
+ * rather than evaluated without them. */
+static int supported(const oqmc_system_desc* d) {
+  return !d->has_bs1 && !d->has_bs2 && !d->has_j3 && !d->has_spl && d->n_e <= MAXE &&
+         d->nocc <= MAXO && d->nbf <= MAXBF;
+}
+
+/* Full evaluation of W walkers: logpsi (W) and eparts (W x 4).  Returns 0,
+ * or -1 for a descriptor outside the restatement. */
 int vmc_ref_eval(const oqmc_system_desc* d, const double* X, int W, double* logpsi,
                  double* eparts, int nthreads) {
+  if (!supported(d)) return -1;
   sys_t S;
   sys_init(&S, d);
   if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -410,9 +420,10 @@ int vmc_ref_eval(const oqmc_system_desc* d, const double* X, int W, double* logp
 
 /* n_steps reference steps (all-electron move + E_L) on W walkers in place.
  * series: (n_steps, 4) walker means of ee, en, ke, E_L; acc: mean acceptance.
- * Returns 0. */
+ * Returns 0, or -1 for a descriptor outside the restatement. */
 int vmc_ref_run(const oqmc_system_desc* d, double* X, int W, int n_steps, double step,
                 uint64_t seed, double* series, double* acc, int nthreads) {
+  if (!supported(d)) return -1;
   sys_t S;
   sys_init(&S, d);
   if (nthreads > 0) omp_set_num_threads(nthreads);

@@ -1,9 +1,19 @@
 """Generate golden vectors by running the reference's own wavefunction code.
 
-Run in a container that has the reference checkout (read-only) at
-``/root/reference`` (override with ``OMEGAQMC_REF``)::
+Run where the reference checkout is available, naming it with ``--ref`` or
+the ``OMEGAQMC_REF`` environment variable::
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --ref <checkout> [--cases ...] [--verify]
+
+A case whose fixture already exists is recomputed from the inputs stored in
+that fixture (atoms, basis, cusp and Jastrow parameters, orbitals, trial,
+walkers), so re-running the script reproduces every committed fixture
+whatever the package's molecule builders do today; ``--fresh`` rebuilds the
+inputs from the builders instead.  ``--verify`` recomputes and compares with
+the stored outputs without writing.  The ``bench_*`` cases are the exact
+trials the benchmark runs: the synthetic cc-pVDZ-shaped basis, RHF orbitals
+from this package's SCF and the benchmark Jastrow (``h2o``, ``n2``), the
+configuration-1 H2 trial and the configuration-2 LiH trial.
 
 JAX and PySCF are not installed, so the reference modules
 ``OmegaQMC/psi/shell.py``, ``OmegaQMC/psi/gto.py`` and ``OmegaQMC/utils.py``
@@ -44,7 +54,7 @@ import torch  # noqa: E402
 from omegaqmc_b200.system import Mole, MeanField, ELEMENT_Z  # noqa: E402
 from omegaqmc_b200 import molecules as M  # noqa: E402
 
-REF = os.environ.get("OMEGAQMC_REF", "/root/reference")
+REF = os.environ.get("OMEGAQMC_REF")
 
 
 def _stub(name, **attrs):
@@ -57,6 +67,8 @@ def _stub(name, **attrs):
 
 def load_reference():
     """Import the reference's shell/gto/utils modules from the checkout."""
+    if not REF or not os.path.isdir(os.path.join(REF, "OmegaQMC")):
+        raise SystemExit("name the reference checkout with --ref or OMEGAQMC_REF")
     _stub("h5py")
     _stub("pyscf", __config__=types.SimpleNamespace(),
           gto=types.SimpleNamespace(Mole=type("Mole", (), {})))
@@ -247,7 +259,20 @@ CASES = {
                    lambda mol: {"J2_pade": {"like": np.array([0.25, 0.8]),
                                             "unlike": np.array([0.5, 0.8])}},
                    1.0, 16),
+    # the benchmark's own trials (RHF orbitals, see RHF_CASES): H2O and N2
+    # with the benchmark Jastrow (Padé J2, b = 3, no J1); configuration 1
+    # (H2/STO-3G, J2 b = 1); configuration 2 (LiH, Padé J1 with a = -Z and
+    # J2, b = 1)
+    "bench_h2o": (lambda: M.named_system("H2O"), False, M.benchmark_params_corr, 1.0, 24),
+    "bench_n2": (lambda: M.named_system("N2"), False, M.benchmark_params_corr, 1.0, 16),
+    "bench_h2": (lambda: M.named_system("H2"), False,
+                 lambda mol: M.default_params_corr(mol, j1=False), 0.5, 24),
+    "bench_lih": (lambda: M.named_system("LiH"), False, M.default_params_corr, 1.0, 24),
 }
+
+# cases whose orbitals come from this package's RHF (the others use seeded
+# orbitals)
+RHF_CASES = {"bench_h2o": "H2O", "bench_n2": "N2", "bench_h2": "H2", "bench_lih": "LiH"}
 
 # B-spline cutoffs and J3 orders per case (jastrow_config of _PsiGTO,
 # gto.py:948-984)
@@ -292,16 +317,63 @@ TRIALS = {"h2o_md": _trial_h2o, "lih_md_uhf": _trial_lih_uhf}
 EEI_MAPS = [(3, 3, 5.0), (2, 2, 4.0), (2, 3, 6.0), (4, 3, 5.0), (1, 2, 3.0)]
 
 
-def run_case(gto, name, seed):
+def _json_params(d):
+    if d is None:
+        return None
+    out = {}
+    for k, v in d.items():
+        if isinstance(v, dict):
+            out[k] = {kk: np.asarray(vv, dtype=np.float64) for kk, vv in v.items()}
+        else:
+            out[k] = np.asarray(v, dtype=np.float64)
+    return out
+
+
+def stored_inputs(name):
+    """The inputs stored in an existing fixture, or None."""
+    path = os.path.join(HERE, f"golden_{name}.npz")
+    if not os.path.exists(path):
+        return None
+    d = dict(np.load(path))
+    spec = json.loads(str(d["spec"]))
+    mol = Mole([(a[0], tuple(a[1])) for a in spec["atoms"]], spec["basis"], unit="Bohr")
+    if spec.get("ao_splines") is not None:
+        mol.ao_radial_transform = spec["ao_splines"]
+    mf = M.MeanField(mol, d["mo_coeff"], d["mo_occ"])
+    pcusp = spec["cusp"]
+    if pcusp is not None:
+        pcusp = {k: {"q0": v["q0"], "coeff": np.asarray(v["coeff"])} for k, v in pcusp.items()}
+    trial = None
+    if "trial_ci" in d:
+        trial = {"mo_coeff": d["trial_mo_coeff"], "ci_coeffs": d["trial_ci"],
+                 "occ_up": d["trial_occ_up"], "occ_dn": d["trial_occ_dn"],
+                 "ndet": len(d["trial_ci"])}
+    return (mol, mf, _json_params(spec["params_corr"]), pcusp, d["X"],
+            spec.get("jastrow_config"), trial), d
+
+
+def built_inputs(name, seed):
+    """Inputs of a case from the package's builders."""
     mk, cusp, mkp, sigma, nw = CASES[name]
     mol = mk()
-    mf = M.MeanField(mol, M.seeded_mo_coeff(mol, seed=seed))
+    if name in RHF_CASES:
+        ref = M.make_mf(RHF_CASES[name])
+        mf = M.MeanField(mol, ref.mo_coeff, ref.mo_occ)
+    else:
+        mf = M.MeanField(mol, M.seeded_mo_coeff(mol, seed=seed))
     params = mkp(mol)
     pcusp = M.synthetic_cusp_params(mol, seed=seed + 11) if cusp else None
     X = _walkers(mol, nw, sigma, seed + 101)
-    rmf = _RefMF(mf)
     jcfg = JASTROW_CONFIG.get(name)
     trial = TRIALS[name](mf, seed + 31) if name in TRIALS else None
+    return mol, mf, params, pcusp, X, jcfg, trial
+
+
+def run_case(gto, inputs):
+    mol, mf, params, pcusp, X, jcfg, trial = inputs
+    cusp = pcusp is not None
+    nw = len(X)
+    rmf = _RefMF(mf)
     ref_trial = None
     if trial is not None:
         ref_trial = {"mo_coeff": trial["mo_coeff"],
@@ -381,15 +453,38 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cases", nargs="*", default=None,
                     help="generate only these cases (default: all, plus binning and cusp)")
+    ap.add_argument("--ref", default=None, help="the reference checkout (or OMEGAQMC_REF)")
+    ap.add_argument("--fresh", action="store_true",
+                    help="build inputs from the package's builders even where a fixture exists")
+    ap.add_argument("--verify", action="store_true",
+                    help="recompute from the stored inputs and compare; write nothing")
     args = ap.parse_args()
+    global REF
+    REF = args.ref or REF
     gto, shell, utils = load_reference()
     os.makedirs(HERE, exist_ok=True)
+    worst = 0.0
     for k, name in enumerate(CASES):
         if args.cases is not None and name not in args.cases:
             continue
-        res = run_case(gto, name, seed=k)
+        stored = None if args.fresh else stored_inputs(name)
+        if args.verify and stored is None:
+            print(f"{name}: no fixture to verify")
+            continue
+        inputs = stored[0] if stored is not None else built_inputs(name, seed=k)
+        res = run_case(gto, inputs)
+        if args.verify:
+            d = stored[1]
+            diff = max(float(np.max(np.abs(res[q] - d[q]) / (np.abs(d[q]) + 1.0)))
+                       for q in ("logpsi", "e_ee", "e_en", "e_ke", "grad", "lap"))
+            worst = max(worst, diff)
+            print(f"{name}: max relative difference to the fixture {diff:.3e}")
+            continue
         np.savez_compressed(os.path.join(HERE, f"golden_{name}.npz"), **res)
         print(f"{name}: {len(res['logpsi'])} walkers, logpsi[0]={res['logpsi'][0]:.12f}")
+    if args.verify:
+        print(f"worst {worst:.3e}")
+        return
     if args.cases is None or "eeI_map" in args.cases:
         maps = {}
         for n_ei, n_ee, rc in EEI_MAPS:

@@ -6,10 +6,10 @@ from __future__ import annotations
 import ctypes
 import os
 
-from . import _lib as L
-from .context import pack_system
+from omegaqmc_b200 import _lib as L
+from omegaqmc_b200.context import pack_system
 
-CSRC = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc")
+CSRC = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "omegaqmc_b200", "csrc")
 HEADERS = ("oqmc_common.cuh", "oqmc_ao.cuh", "oqmc_eval.cuh", "oqmc_sweep.cuh", "oqmc_batch.cuh",
            "oqmc_tc.cuh", "oqmc_mlp.cuh", "oqmc_mlp_sweep.cuh")
 

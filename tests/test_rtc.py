@@ -3,7 +3,7 @@ host, no GPU) and carries the system's data."""
 import pytest
 
 from omegaqmc_b200 import molecules as M
-from omegaqmc_b200 import rtc_check as R
+import rtc_check as R
 from omegaqmc_b200.system import build_system
 
 
