@@ -200,10 +200,18 @@ int oqmc_basin(oqmc_ctx* ctx, double* walkers, int W, void* state, int precision
  * call refreshes the state from `walkers`, then runs the sweeps; the other
  * arguments mean what they mean for oqmc_sweeps.  W is limited to
  * oqmc_state_bytes(ctx, W, precision) <= OQ_NOALLOC_SCRATCH_BYTES (about
- * 25,000 FP64 H2O walkers); larger W returns OQ_ERR_ARG.  Allocates
- * nothing.  The first call on a device looks up the array's device address;
- * make it before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race, so serialise them. */
+ * 25,000 FP64 H2O walkers); larger W returns OQ_ERR_ARG.  Calls no
+ * allocating routine.  The first call on a device looks up the array's
+ * device address; make it before any stream capture.  Under CUDA's default
+ * lazy module loading that first call can also load the library's kernels
+ * into device memory: make one call outside the memory-constrained region
+ * (or set CUDA_MODULE_LOADING=EAGER).  A call whose kernels need more
+ * per-thread local memory than the device's current stack limit
+ * (cudaLimitStackSize) returns OQ_ERR_UNSUPPORTED instead of letting the
+ * driver grow its local-memory reservation: at the default 1 KiB this
+ * refuses all-electron steps and multi-determinant trials until an
+ * allocating call has raised the limit.  All calls share the array: calls
+ * that overlap on the GPU race, so serialise them. */
 int oqmc_sweeps_noalloc(oqmc_ctx* ctx, double* walkers, int W, int precision,
                         int n_sweeps, int measure_every, double step,
                         uint64_t seed, uint64_t step_base, double* sums,
@@ -226,9 +234,9 @@ int oqmc_set_proposal(oqmc_ctx* ctx, int kind, double r0, double fmin_frac);
  * to single-electron sweeps only; the learned proposal, multi-determinant
  * trials and oqmc_batch_bind refuse kind 1.  The accepted-move sum counts
  * electron moves in both kinds: an accepted all-electron step adds n_e.
- * oqmc_sweeps_noalloc refuses kind 1 (OQ_ERR_UNSUPPORTED): the first launch
- * of the all-electron kernel can grow the device's local-memory reservation
- * (its per-thread stack exceeds the default), which is an allocation. */
+ * The all-electron kernel's per-thread stack exceeds the default local-memory
+ * reservation, so oqmc_sweeps_noalloc refuses kind 1 on a device whose stack
+ * limit has not been raised (see there). */
 int oqmc_set_move_kind(oqmc_ctx* ctx, int kind);
 /* Multi-determinant trial (the `trial` dict of get_psi_fun /
  * get_vmc_gto_func, OmegaQMC/psi/gto.py:846-863, 1312-1488):
@@ -239,7 +247,8 @@ int oqmc_set_move_kind(oqmc_ctx* ctx, int kind);
  * determinant order.  At most 16 distinct columns and 64 distinct
  * determinants per spin.  Evaluation (oqmc_eval, oqmc_log_psi) and
  * sampling (oqmc_refresh, oqmc_sweeps, oqmc_basin) then use the expansion,
- * in FP64 only (oqmc_sweeps_noalloc included); the batched, learned-proposal
+ * in FP64 only (oqmc_sweeps_noalloc included, under its local-memory rule);
+ * the batched, learned-proposal
  * and tensor-core paths refuse it.  ndet = 0 returns to the single determinant
  * of the descriptor.  Sampler state sizes (oqmc_state_bytes) change with the
  * expansion.  With an expansion, oqmc_eval and oqmc_log_psi refresh a

@@ -125,7 +125,52 @@ static void compute_split(oqmc_ctx* ctx) {
 }
 
 // Record an error on a context (used by entry points in other files).
-int oq_ctx_move_kind(const oqmc_ctx* ctx) { return ctx->move_kind; }
+
+// Largest per-thread local memory (bytes) among the kernels that
+// oqmc_refresh followed by oqmc_sweeps launch for this context and precision
+// (the same dispatch as those two entry points).  Returns OQ_OK or an error.
+int oq_ctx_sweep_local_bytes(oqmc_ctx* ctx, int precision, size_t* out) {
+  const int mixed = precision == OQ_PREC_MIXED;
+  size_t best = 0, v = 0;
+  cudaError_t err = cudaSuccess;
+  auto take = [&](int kind, int prop, int M) -> bool {
+#define OQ_X(N) err = oq_local_bytes_##N(kind, mixed, prop, M, &v)
+    OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+    if (err != cudaSuccess) return false;
+    best = v > best ? v : best;
+    return true;
+  };
+  auto take_rtc = [&](void* fn) -> bool {
+    const int b = fn ? oq_rtc_local_bytes(fn) : -1;
+    if (b < 0) return false;
+    best = (size_t)b > best ? (size_t)b : best;
+    return true;
+  };
+  bool ok = true;
+  if (ctx->md) {
+    ok = take(4, 0, ctx->md->M) && take(5, 0, ctx->md->M) && take(6, 0, ctx->md->M);
+  } else {
+    ok = take(0, 0, 0);
+    if (ok) {
+      if (ctx->move_kind == 1) ok = take(7, 0, 0);
+      else if (ctx->mlp) ok = take_rtc(ctx->mlp_fn[ctx->mlp_groups == 4 ? 1 : 0]);
+      else if (ctx->spec)
+        ok = take_rtc(oq_spec_function(ctx->spec, (ctx->proposal == 1 ? 4 : 0) + mixed));
+      else ok = take(1, ctx->proposal == 1 ? 1 : 0, 0);
+    }
+    if (ok) {
+      if (mixed && ctx->use_tc) ok = take(3, 0, 0);
+      else if (ctx->spec) ok = take_rtc(oq_spec_function(ctx->spec, 2 + mixed));
+      else ok = take(2, 0, 0);
+    }
+  }
+  if (!ok)
+    return set_err(ctx, OQ_ERR_CUDA, "kernel attribute query failed: %s",
+                   cudaGetErrorString(err != cudaSuccess ? err : cudaErrorInvalidValue));
+  *out = best;
+  return OQ_OK;
+}
 
 int oq_ctx_set_error(oqmc_ctx* ctx, int code, const char* msg) {
   return set_err(ctx, code, "%s", msg);

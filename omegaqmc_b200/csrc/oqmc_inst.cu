@@ -188,3 +188,53 @@ cudaError_t OQ_FN(oq_moves_alle)(const OqLaunch& L, const OqMoveArgs& a, int mix
   }
   return cudaGetLastError();
 }
+
+// Per-thread local memory (bytes) of one kernel this size launches: kind 0
+// k_refresh, 1 k_moves (prop 0/1/2), 2 k_eloc, 3 k_eloc_tc, 4 k_md_refresh,
+// 5 k_md_moves, 6 k_md_local (M = 8 or 16 columns), 7 k_moves_alle.
+template <typename K>
+static cudaError_t oq_lmem(K kernel, size_t* out) {
+  cudaFuncAttributes a;
+  const cudaError_t e = cudaFuncGetAttributes(&a, kernel);
+  if (e == cudaSuccess) *out = a.localSizeBytes;
+  return e;
+}
+
+template <int M>
+static cudaError_t md_lmem(int kind, size_t* out) {
+  if (kind == 4) return oq_lmem(k_md_refresh<OQ_N, M>, out);
+  if (kind == 5) return oq_lmem(k_md_moves<OQ_N, M>, out);
+  return oq_lmem(k_md_local<OQ_N, M>, out);
+}
+
+cudaError_t OQ_FN(oq_local_bytes)(int kind, int mixed, int prop, int M, size_t* out) {
+  switch (kind) {
+    case 0:
+      return mixed ? oq_lmem(k_refresh<OQ_N, float>, out) : oq_lmem(k_refresh<OQ_N, double>, out);
+    case 1:
+      if (prop == 2)
+        return mixed ? oq_lmem(k_moves<OQ_N, float, float, 2>, out)
+                     : oq_lmem(k_moves<OQ_N, double, double, 2>, out);
+      if (prop == 1)
+        return mixed ? oq_lmem(k_moves<OQ_N, float, float, 1>, out)
+                     : oq_lmem(k_moves<OQ_N, double, double, 1>, out);
+      return mixed ? oq_lmem(k_moves<OQ_N, float, float, 0>, out)
+                   : oq_lmem(k_moves<OQ_N, double, double, 0>, out);
+    case 2:
+      return mixed ? oq_lmem(k_eloc<OQ_N, float, float>, out)
+                   : oq_lmem(k_eloc<OQ_N, double, double>, out);
+    case 3:
+      return oq_lmem(k_eloc_tc<OQ_N>, out);
+    case 4:
+    case 5:
+    case 6:
+      if constexpr (OQ_N <= 8) {
+        if (M == 8) return md_lmem<8>(kind, out);
+      }
+      return M == 16 ? md_lmem<16>(kind, out) : cudaErrorInvalidValue;
+    case 7:
+      return mixed ? oq_lmem(k_moves_alle<OQ_N, float>, out)
+                   : oq_lmem(k_moves_alle<OQ_N, double>, out);
+  }
+  return cudaErrorInvalidValue;
+}

@@ -34,7 +34,8 @@ struct OqLaunch {
                               const OqMoveArgs& a, double* sgn, int M);                \
   cudaError_t oq_md_local_##N(const OqLaunch& L, const OqMdTables& T,                  \
                               const OqMdState& st, const OqElocArgs& a, double* logpsi, \
-                              double* grad, double* lap, int M);
+                              double* grad, double* lap, int M);                \
+  cudaError_t oq_local_bytes_##N(int kind, int mixed, int prop, int M, size_t* out);
 
 #define OQ_NOCC_LIST(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(10) X(12) X(14) X(16)
 

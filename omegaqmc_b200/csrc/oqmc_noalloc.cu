@@ -18,6 +18,21 @@
 // contexts on one device) race with each other: serialise them.  Every call
 // rewrites the whole state it uses from the caller's walkers before the first
 // sweep, so nothing in it needs to start at zero.
+//
+// Two things outside this file can still allocate device memory on a call,
+// and the entry point guards against or documents both:
+//  * Local memory.  The driver reserves per-thread stack for every resident
+//    thread at the size of the device's current stack limit and grows the
+//    reservation when a launched kernel needs more.  Before launching, the
+//    call compares the local memory of every kernel it would run with
+//    cudaDeviceGetLimit(cudaLimitStackSize) and refuses (OQ_ERR_UNSUPPORTED)
+//    rather than grow it.
+//  * Module loading.  Under CUDA's default lazy loading a kernel's module is
+//    loaded into device memory on its first use, so the first call on a
+//    device may allocate for that.  Make one call (or one oqmc_sweeps call on
+//    the same context) outside the memory-constrained region, or run with
+//    CUDA_MODULE_LOADING=EAGER.
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <cuda_runtime.h>
@@ -50,7 +65,7 @@ static cudaError_t scratch_address(void** out) {
 }
 
 int oq_ctx_set_error(oqmc_ctx* ctx, int code, const char* msg);
-int oq_ctx_move_kind(const oqmc_ctx* ctx);
+int oq_ctx_sweep_local_bytes(oqmc_ctx* ctx, int precision, size_t* out);
 
 extern "C" int oqmc_sweeps_noalloc(oqmc_ctx* ctx, double* walkers, int W, int precision,
                                    int n_sweeps, int measure_every, double step,
@@ -60,12 +75,23 @@ extern "C" int oqmc_sweeps_noalloc(oqmc_ctx* ctx, double* walkers, int W, int pr
   if (W < 0 || n_sweeps < 0 || (precision != OQ_PREC_FP64 && precision != OQ_PREC_MIXED))
     return oq_ctx_set_error(ctx, OQ_ERR_ARG, "bad arguments");
   if (W == 0 || n_sweeps == 0) return OQ_OK;
-  // the all-electron kernel needs more per-thread stack than the driver's
-  // default local-memory reservation; growing that reservation on its first
-  // launch is a device allocation
-  if (oq_ctx_move_kind(ctx) != 0)
-    return oq_ctx_set_error(ctx, OQ_ERR_UNSUPPORTED,
-                            "all-electron steps are not allocation-free; use oqmc_sweeps");
+  // a kernel whose per-thread local memory exceeds the device's current
+  // stack limit makes the driver grow its local-memory reservation at launch,
+  // which is a device allocation (the all-electron step and the
+  // multi-determinant kernels need more than the default 1 KiB)
+  size_t lmem = 0, limit = 0;
+  const int lrc = oq_ctx_sweep_local_bytes(ctx, precision, &lmem);
+  if (lrc != OQ_OK) return lrc;
+  const cudaError_t le = cudaDeviceGetLimit(&limit, cudaLimitStackSize);
+  if (le != cudaSuccess) return oq_ctx_set_error(ctx, OQ_ERR_CUDA, cudaGetErrorString(le));
+  if (lmem > limit) {
+    char msg[256];
+    snprintf(msg, sizeof(msg),
+             "a kernel of this call needs %zu B of local memory per thread, above the "
+             "device's current stack reservation of %zu B; growing it is an allocation: "
+             "use oqmc_sweeps", lmem, limit);
+    return oq_ctx_set_error(ctx, OQ_ERR_UNSUPPORTED, msg);
+  }
   const size_t need = oqmc_state_bytes(ctx, W, precision);
   if (need > (size_t)OQ_NOALLOC_SCRATCH_BYTES)
     return oq_ctx_set_error(ctx, OQ_ERR_ARG,

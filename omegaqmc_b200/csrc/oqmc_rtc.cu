@@ -538,6 +538,10 @@ void oq_spec_destroy(OqSpecModule* m) {
   delete m;
 }
 
+void* oq_spec_function(OqSpecModule* m, int which) {
+  return (m && which >= 0 && which < 6) ? (void*)m->fn[which] : nullptr;
+}
+
 int oq_spec_launch(OqSpecModule* m, int which, dim3 grid, dim3 block, size_t smem,
                    cudaStream_t stream, void** args) {
   const Api& A = g_api;

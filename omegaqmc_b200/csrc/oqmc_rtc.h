@@ -16,6 +16,8 @@ void oq_spec_destroy(OqSpecModule* m);
 // 4/5 = nucleus-scaled moves FP64/mixed
 int oq_spec_launch(OqSpecModule* m, int which, dim3 grid, dim3 block, size_t smem,
                    cudaStream_t stream, void** args);
+// The CUfunction behind `which` (numbering as for oq_spec_launch).
+void* oq_spec_function(OqSpecModule* m, int which);
 std::string oq_spec_source(const OqSystem& S, const OqSplit& SP, const double* C, int nocc);
 
 // The basis policy of one system as C++ source for a struct named `name`.

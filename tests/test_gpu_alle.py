@@ -101,18 +101,32 @@ def test_move_kind_arguments_and_refusals():
         ens.run(2, 0.5)
 
 
-def test_noalloc_entry_refuses_all_electron_steps():
+def test_noalloc_entry_runs_all_electron_steps_once_the_stack_allows():
+    """The allocation-free entry point refuses a kernel only while its local
+    memory exceeds the device's stack limit; after the allocating path has
+    run the all-electron kernel (raising the limit where it needed more), the
+    allocation-free call runs the same chain."""
     import ctypes
     from omegaqmc_b200 import _lib as L
     lib = L.load()
-    s = _sys("H2")
+    s = _sys("H2O")
     ctx = GTOContext(s)
     ctx.set_move_kind(1)
-    X = ctx.walkers_tensor(seeded_walkers(s, 64, 0.5, 0))
-    sums = torch.zeros(1, 8, dtype=torch.float64, device="cuda")
+    W = 64
+    X0 = ctx.walkers_tensor(seeded_walkers(s, W, 0.9, 0))
     st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-    rc = lib.oqmc_sweeps_noalloc(ctx._h, ctypes.c_void_p(X.data_ptr()), 64, L.PREC_FP64, 1, 1,
-                                 0.5, ctypes.c_uint64(1), ctypes.c_uint64(0),
-                                 ctypes.c_void_p(sums.data_ptr()), None, None, st)
-    assert rc == L.OQ_ERR_UNSUPPORTED
-    assert b"allocation-free" in lib.oqmc_last_error(ctx._h)
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    Xa, Xb = X0.clone(), X0.clone()
+    sa = torch.zeros(3, 8, dtype=torch.float64, device="cuda")
+    sb = torch.zeros(3, 8, dtype=torch.float64, device="cuda")
+    state = torch.empty(lib.oqmc_state_bytes(ctx._h, W, L.PREC_FP64), dtype=torch.uint8,
+                        device="cuda")
+    assert lib.oqmc_refresh(ctx._h, p(Xa), W, p(state), L.PREC_FP64, st) == 0
+    assert lib.oqmc_sweeps(ctx._h, p(Xa), W, p(state), L.PREC_FP64, 3, 1, 0.2,
+                           ctypes.c_uint64(1), ctypes.c_uint64(0), p(sa), None, None, 0, st) == 0
+    rc = lib.oqmc_sweeps_noalloc(ctx._h, p(Xb), W, L.PREC_FP64, 3, 1, 0.2, ctypes.c_uint64(1),
+                                 ctypes.c_uint64(0), p(sb), None, None, st)
+    assert rc == 0, lib.oqmc_last_error(ctx._h)
+    torch.cuda.synchronize()
+    assert torch.equal(Xa, Xb) and torch.allclose(sa, sb, rtol=1e-12, atol=1e-12)
+    assert not torch.equal(Xa, X0)
