@@ -162,6 +162,41 @@ size_t oqmc_state_bytes(const oqmc_ctx* ctx, int W, int precision);
 int oqmc_refresh(oqmc_ctx* ctx, const double* walkers, int W, void* state,
                  int precision, void* stream);
 
+/* Equilibration with the step adapted on the device: n_steps sweeps, each
+ * followed by the reference's rule log s <- log s + rate (acc - target)
+ * applied to the width at `step` (one device double, read by the next sweep
+ * and left holding the final width); the equilibration_step scan of
+ * OmegaQMC/vmc_gto.py:1338-1357 with _adapt_step_size (121-126), without
+ * the host reading the acceptance between steps.  acc_trace (device,
+ * n_steps) receives each sweep's acceptance ratio, step_trace (device,
+ * n_steps, optional) the width after each adaptation.  The state is
+ * refreshed (FP64 LU) whenever refresh_every sweeps have passed since the
+ * last refresh, counting from since_refresh at entry.  Random numbers as
+ * oqmc_sweeps (counter step_base + t).  Single-determinant, single-electron
+ * Gaussian or nucleus-scaled sweeps; other contexts return
+ * OQ_ERR_UNSUPPORTED. */
+int oqmc_equilibrate(oqmc_ctx* ctx, double* walkers, int W, void* state, int precision,
+                     int n_steps, double* step, double target, double rate, uint64_t seed,
+                     uint64_t step_base, int refresh_every, int since_refresh,
+                     double* acc_trace, double* step_trace, void* stream);
+
+/* Per-walker outputs of the sampler state in its own precision: what the
+ * sampler itself sees, for stating the error of each output of the mixed
+ * path against the FP64 evaluation.  Counterparts: log_trial_wavefunction
+ * (OmegaQMC/psi/gto.py:2220-2254) and the grad_flat / per-electron
+ * Laplacian / local-energy parts of local_energy_ke (gto.py:2506-2579) and
+ * local_energy_ee/en (gto.py:2406-2451).  logpsi (W) = the state's
+ * Sherman-Morrison-tracked log|det| (FP64 sum of the accepted moves' ratio
+ * logarithms since the last refresh) + the Jastrow in working precision;
+ * grad (W x n_e x 3) and lap (W x n_e) from the state's inverse (FP32 in
+ * the mixed state) and the working-precision orbitals and Jastrow; eparts
+ * (W x 4) ee, en, ke, E_L.  Any output may be null.  Uses the specialised
+ * local-energy kernel when the context is specialised; positions and state
+ * are not changed. */
+int oqmc_state_eval(oqmc_ctx* ctx, const void* state, int W, int precision,
+                    double* logpsi, double* grad, double* lap, double* eparts,
+                    void* stream);
+
 /* n_sweeps single-electron Metropolis sweeps over all walkers (positions
  * updated in place), measuring the local energy after every
  * measure_every-th sweep.  sums: (n_sweeps/measure_every, 8) doubles that

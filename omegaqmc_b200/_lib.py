@@ -91,6 +91,11 @@ _SIGS = [
     ("oqmc_mo_values", c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     ("oqmc_state_bytes", c_size_t, [c_void_p, c_int, c_int]),
     ("oqmc_refresh", c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p]),
+    ("oqmc_state_eval", c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p,
+                                c_void_p, c_void_p, c_void_p]),
+    ("oqmc_equilibrate", c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_int, c_void_p,
+                                 c_double, c_double, c_uint64, c_uint64, c_int, c_int,
+                                 c_void_p, c_void_p, c_void_p]),
     ("oqmc_sweeps", c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_int, c_int,
                             c_double, c_uint64, c_uint64, c_void_p, c_void_p, c_void_p,
                             c_int, c_void_p]),

@@ -228,6 +228,23 @@ class GTOContext:
         return out
 
     # -- sampler ------------------------------------------------------------
+    def state_evaluate(self, state, W, precision, stream=None):
+        """Outputs of a sampler state in its own precision (``oqmc_state_eval``):
+        the tracked log|det| plus the Jastrow, the gradient and per-electron
+        Laplacian of log|psi| from the state's inverse, and the local-energy
+        parts; a dict of CUDA tensors keyed like :meth:`evaluate`."""
+        opt = dict(dtype=torch.float64, device=self.device)
+        W = int(W)
+        logpsi = torch.empty(W, **opt)
+        grad = torch.empty(W, self.n_e, 3, **opt)
+        lap = torch.empty(W, self.n_e, **opt)
+        ep = torch.empty(W, 4, **opt)
+        self._check(self.lib.oqmc_state_eval(self._h, _dptr(state), W, int(precision),
+                                             _dptr(logpsi), _dptr(grad), _dptr(lap),
+                                             _dptr(ep), _stream_ptr(stream)))
+        return {"logpsi": logpsi, "grad": grad, "lap": lap, "e_ee": ep[:, 0],
+                "e_en": ep[:, 1], "e_ke": ep[:, 2], "e_loc": ep[:, 3]}
+
     def state_bytes(self, W, precision):
         return int(self.lib.oqmc_state_bytes(self._h, int(W), int(precision)))
 
@@ -247,6 +264,16 @@ class GTOContext:
             int(measure_every), float(step), ctypes.c_uint64(seed & (2**64 - 1)),
             ctypes.c_uint64(step_base), _dptr(sums), _dptr(el_trace), _dptr(eparts_last),
             int(walkers_per_block), _stream_ptr(stream)))
+
+    def equilibrate(self, X, state, precision, n_steps, step, target, rate, seed, step_base,
+                    refresh_every, since_refresh, acc_trace, step_trace=None, stream=None):
+        """``oqmc_equilibrate``: n_steps sweeps with the step width (the
+        one-element CUDA tensor ``step``) adapted on the device after each."""
+        self._check(self.lib.oqmc_equilibrate(
+            self._h, _dptr(X), X.shape[0], _dptr(state), int(precision), int(n_steps),
+            _dptr(step), float(target), float(rate), ctypes.c_uint64(seed & (2**64 - 1)),
+            ctypes.c_uint64(step_base), int(refresh_every), int(since_refresh),
+            _dptr(acc_trace), _dptr(step_trace), _stream_ptr(stream)))
 
     def basin(self, X, state, precision, n_steps, sigma, seed, step_base, acc_sum=None,
               stream=None):

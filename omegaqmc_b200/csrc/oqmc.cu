@@ -1426,6 +1426,125 @@ int oqmc_sweeps(oqmc_ctx* ctx, double* X, int W, void* state, int precision, int
   return OQ_OK;
 }
 
+// One step of the reference's step-size rule (_adapt_step_size,
+// OmegaQMC/vmc_gto.py:121-126): with the acceptance ratio
+// acc = (*accepted) * inv_moves of the sweep just made,
+// log s <- log s + rate (acc - target).  Records the ratio in place of the
+// count and the new width in step_trace (if set).  One thread.
+__global__ void k_adapt_step(double* __restrict__ step, double* __restrict__ accepted,
+                             double inv_moves, double rate, double target,
+                             double* __restrict__ step_trace) {
+  const double acc = *accepted * inv_moves;
+  const double s = exp(log(*step) + rate * (acc - target));
+  *step = s;
+  *accepted = acc;
+  if (step_trace) *step_trace = s;
+}
+
+int oqmc_equilibrate(oqmc_ctx* ctx, double* X, int W, void* state, int precision,
+                     int n_steps, double* step, double target, double rate, uint64_t seed,
+                     uint64_t step_base, int refresh_every, int since_refresh,
+                     double* acc_trace, double* step_trace, void* stream) {
+  if (!ctx) return OQ_ERR_ARG;
+  if (W < 0 || n_steps < 0 || refresh_every < 1 || since_refresh < 0 || !valid_prec(precision))
+    return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
+  if (W == 0 || n_steps == 0) return OQ_OK;
+  if (!X || !state || !step || !acc_trace) return set_err(ctx, OQ_ERR_ARG, "null buffer%s");
+  if (ctx->md || ctx->mlp || ctx->move_kind != 0)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED,
+                   "device-side equilibration runs single-determinant, single-electron "
+                   "Gaussian sweeps only%s");
+  size_t sm;
+  const int wpb = pick_wpb(ctx, 0, precision, &sm);
+  if (wpb < 0)
+    return set_err(ctx, OQ_ERR_UNSUPPORTED, "system too large for the shared-memory move kernel%s");
+  cudaStream_t s = (cudaStream_t)stream;
+  const OqStatePtrs st = state_ptrs(ctx, state, W, precision);
+  OQ_CUDA(ctx, to_soa(ctx, X, st.pos, W, s));
+  OQ_CUDA(ctx, cudaMemsetAsync(acc_trace, 0, sizeof(double) * (size_t)n_steps, s));
+  OqMoveArgs m;
+  memset(&m, 0, sizeof(m));
+  m.pos = st.pos; m.ainv = st.ainv; m.logdet = st.logdet; m.W = W; m.mode = 0;
+  m.n_steps = 1; m.step = 0.0; m.step_dev = step; m.seed = seed; m.flags = ctx->d_flags;
+  m.proposal = ctx->proposal; m.scale_r0 = ctx->scale_r0; m.scale_fmin = ctx->scale_fmin;
+  const OqLaunch Lr = make_launch(ctx, stream, smem_sys_c64(ctx));
+  const int mixed = precision == OQ_PREC_MIXED;
+  const double inv_moves = 1.0 / ((double)W * ctx->n_e);
+  int since = since_refresh;
+  for (int t = 0; t < n_steps; ++t) {
+    m.step_base = step_base + t;
+    m.acc_sum = acc_trace + t;
+    int rc = launch_moves(ctx, m, wpb, sm, precision, stream);
+    if (rc != OQ_OK) return rc;
+    k_adapt_step<<<1, 1, 0, s>>>(step, acc_trace + t, inv_moves, rate, target,
+                                 step_trace ? step_trace + t : nullptr);
+    OQ_CUDA(ctx, cudaGetLastError());
+    if (++since >= refresh_every) {
+      cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_refresh_##N(Lr, st.pos, W, st.ainv, st.logdet, mixed)
+      OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+      OQ_CUDA(ctx, err);
+      since = 0;
+    }
+  }
+  OQ_CUDA(ctx, to_aos(ctx, st.pos, X, W, s));
+  return OQ_OK;
+}
+
+int oqmc_state_eval(oqmc_ctx* ctx, const void* state, int W, int precision, double* logpsi,
+                    double* grad, double* lap, double* eparts, void* stream) {
+  if (!ctx) return OQ_ERR_ARG;
+  if (W < 0 || !valid_prec(precision)) return set_err(ctx, OQ_ERR_ARG, "bad arguments%s");
+  if (W == 0) return OQ_OK;
+  if (!state) return set_err(ctx, OQ_ERR_ARG, "null buffer%s");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (ctx->md) {
+    if (precision != OQ_PREC_FP64)
+      return set_err(ctx, OQ_ERR_UNSUPPORTED,
+                     "multi-determinant trials are sampled in FP64 only%s");
+    // the expansion's local-energy kernel on the state's inverses
+    const OqMdState st = md_state(ctx, const_cast<void*>(state), W);
+    const OqMdTables T = md_tables(ctx);
+    const OqLaunch L = make_launch(ctx, stream, sizeof(OqSystem));
+    OqElocArgs a;
+    memset(&a, 0, sizeof(a));
+    a.pos = st.pos; a.W = W; a.eparts = eparts; a.flags = ctx->d_flags;
+    cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_md_local_##N(L, T, st, a, logpsi, grad, lap, ctx->md->M)
+    OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+    OQ_CUDA(ctx, err);
+    return OQ_OK;
+  }
+  const OqStatePtrs st = state_ptrs(ctx, const_cast<void*>(state), W, precision);
+  const int mixed = precision == OQ_PREC_MIXED;
+  if (logpsi)
+    OQ_CUDA(ctx, cudaMemcpyAsync(logpsi, st.logdet, sizeof(double) * (size_t)W,
+                                 cudaMemcpyDeviceToDevice, s));
+  OqElocArgs el;
+  memset(&el, 0, sizeof(el));
+  el.pos = st.pos; el.ainv = st.ainv; el.W = W; el.flags = ctx->d_flags;
+  el.eparts = eparts; el.logpsi = logpsi; el.grad = grad; el.lap = lap;
+  const OqLaunch Le = make_launch(ctx, stream, eloc_smem(ctx, precision));
+  if (ctx->spec) {
+    // the specialised kernel the sweeps use (the tensor-core form has no
+    // per-electron outputs)
+    const void* C = mixed ? (const void*)ctx->d_C32 : (const void*)ctx->d_C64;
+    void* args[4] = {(void*)&Le.sys, (void*)&Le.split, (void*)&C, (void*)&el};
+    if (oq_spec_launch(ctx->spec, mixed ? 3 : 2, dim3((W + 31) / 32), dim3(32, ctx->n_e),
+                       Le.smem, Le.stream, args) != 0)
+      return set_err(ctx, OQ_ERR_CUDA, "specialised local-energy kernel launch failed%s");
+    return OQ_OK;
+  }
+  cudaError_t err = cudaSuccess;
+#define OQ_X(N) err = oq_eloc_##N(Le, el, mixed)
+  OQ_SWITCH(ctx->nocc, OQ_X)
+#undef OQ_X
+  OQ_CUDA(ctx, err);
+  return OQ_OK;
+}
+
 int oqmc_basin(oqmc_ctx* ctx, double* X, int W, void* state, int precision, int n_steps,
                double sigma, uint64_t seed, uint64_t step_base, double* acc_sum,
                void* stream) {

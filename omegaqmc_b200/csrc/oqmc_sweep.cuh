@@ -436,6 +436,8 @@ struct OqMoveArgs {
   uint64_t step_base;     // RNG counter of the first step
   double* acc_sum;        // += accepted moves (may be null)
   unsigned* flags;
+  const double* step_dev; // when set, the Gaussian width is read here (device-side step
+                          // adaptation, oqmc_equilibrate); else `step`
 };
 
 // Proposal width at x for the nucleus-scaled Gaussian move.
@@ -685,6 +687,7 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
     for (int k = 0; k < 2 * NN; ++k) Ai[k * WPB + tid] = gA[(size_t)k * W + w];
   }
   __syncthreads();
+  const double step = a.step_dev ? *a.step_dev : a.step;
   double logdet = live ? a.logdet[w] : 0.0;
   int nacc = 0;
   for (int t = 0; t < (live ? a.n_steps : 0); ++t) {
@@ -693,9 +696,9 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
       for (int e = 0; e < NE; ++e) {
         double n3[3], u;
         oq_move_randoms(a.seed, (uint32_t)w, gstep, (uint32_t)e, n3, u);
-        const double nx = pos[(3 * e) * WPB + tid] + a.step * n3[0];
-        const double ny = pos[(3 * e + 1) * WPB + tid] + a.step * n3[1];
-        const double nz = pos[(3 * e + 2) * WPB + tid] + a.step * n3[2];
+        const double nx = pos[(3 * e) * WPB + tid] + step * n3[0];
+        const double ny = pos[(3 * e + 1) * WPB + tid] + step * n3[1];
+        const double nz = pos[(3 * e + 2) * WPB + tid] + step * n3[2];
         nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz, 0.0,
                                            1.0, u, logdet);
       }
@@ -708,14 +711,14 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
         const double ox = pos[(3 * e) * WPB + tid], oy = pos[(3 * e + 1) * WPB + tid],
                      oz = pos[(3 * e + 2) * WPB + tid];
         double nx, ny, nz, mul, lx;
-        oq_scaled_propose(S, ox, oy, oz, n3, a.step, a.scale_r0, a.scale_fmin, nx, ny, nz, mul,
+        oq_scaled_propose(S, ox, oy, oz, n3, step, a.scale_r0, a.scale_fmin, nx, ny, nz, mul,
                           lx);
         nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz, lx,
                                            mul, u, logdet);
       }
     } else {
       double u, nx, ny, nz, log_qratio;
-      const int e = oq_basin_propose<NE>(S, pos + tid, WPB, a.seed, (uint32_t)w, gstep, a.step,
+      const int e = oq_basin_propose<NE>(S, pos + tid, WPB, a.seed, (uint32_t)w, gstep, step,
                                          nx, ny, nz, log_qratio, u);
       nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
                                          log_qratio, 1.0, u, logdet);
@@ -798,12 +801,17 @@ __device__ __forceinline__ void oq_jastrow_vgl_coulomb(const SJ& J, const OqSyst
 // Padé VGL, gto.py:1575-1649).  pos points at the walker's x of electron 0
 // with stride ps between coordinates; A at its inverse entry (0,0,0) with
 // stride as between entries.  The four outputs are accumulated (+=).
+// The _out form also returns electron e's gradient of log|psi| (Gx, Gy, Gz)
+// and its Laplacian of log|psi| (lap_e).
 template <int NOCC, typename T, typename Real, class B, class SJ>
-__device__ __forceinline__ void oq_eloc_electron(const SJ& J, const OqSystem& S,
-                                                 const OqSplit& SP, const Real* __restrict__ C,
-                                                 const double* pos, size_t ps, const Real* A,
-                                                 size_t as, int e, double& ee, double& en,
-                                                 double& lp_tot, double& g2) {
+__device__ __forceinline__ void oq_eloc_electron_out(const SJ& J, const OqSystem& S,
+                                                     const OqSplit& SP,
+                                                     const Real* __restrict__ C,
+                                                     const double* pos, size_t ps,
+                                                     const Real* A, size_t as, int e,
+                                                     double& ee, double& en, double& lp_tot,
+                                                     double& g2, double& gxo, double& gyo,
+                                                     double& gzo, double& lape) {
   constexpr int NE = 2 * NOCC;
   const int s = e & 1, i = e >> 1;
   const double xe = pos[(size_t)(3 * e) * ps], ye = pos[(size_t)(3 * e + 1) * ps],
@@ -819,8 +827,59 @@ __device__ __forceinline__ void oq_eloc_electron(const SJ& J, const OqSystem& S,
   oq_jastrow_vgl_coulomb<NE, T>(J, S, pos, ps, e, xe, ye, ze, jx, jy, jz, jl, ee, en);
   const double sgx = (double)gx, sgy = (double)gy, sgz = (double)gz;
   const double Gx = sgx + (double)jx, Gy = sgy + (double)jy, Gz = sgz + (double)jz;
-  lp_tot += (double)lp - (sgx * sgx + sgy * sgy + sgz * sgz) + (double)jl;
+  lape = (double)lp - (sgx * sgx + sgy * sgy + sgz * sgz) + (double)jl;
+  lp_tot += lape;
   g2 += Gx * Gx + Gy * Gy + Gz * Gz;
+  gxo = Gx; gyo = Gy; gzo = Gz;
+}
+
+template <int NOCC, typename T, typename Real, class B, class SJ>
+__device__ __forceinline__ void oq_eloc_electron(const SJ& J, const OqSystem& S,
+                                                 const OqSplit& SP, const Real* __restrict__ C,
+                                                 const double* pos, size_t ps, const Real* A,
+                                                 size_t as, int e, double& ee, double& en,
+                                                 double& lp_tot, double& g2) {
+  double gx, gy, gz, le;
+  oq_eloc_electron_out<NOCC, T, Real, B>(J, S, SP, C, pos, ps, A, as, e, ee, en, lp_tot, g2,
+                                         gx, gy, gz, le);
+}
+
+// Electron e's share of the Jastrow value J (log_trial_wavefunction,
+// gto.py:2220-2254): its pairs with the electrons j > e and its
+// electron-nucleus terms, each term in working precision T, summed in FP64.
+// Summed over all electrons this is J1 + J2 (+ B-spline, J3).
+template <int NE, typename T>
+__device__ __forceinline__ double oq_jastrow_value_electron(const OqSystem& S, const double* pos,
+                                                           size_t ps, int e, double xe,
+                                                           double ye, double ze) {
+  double J = 0.0;
+  for (int j = e + 1; j < NE; ++j) {
+    const double dx = xe - pos[(size_t)(3 * j) * ps], dy = ye - pos[(size_t)(3 * j + 1) * ps],
+                 dz = ze - pos[(size_t)(3 * j + 2) * ps];
+    const T r = sqrt((T)(dx * dx + dy * dy + dz * dz));
+    const bool like = (e & 1) == (j & 1);
+    if (S.has_j2) {
+      const int o = like ? 0 : 2;
+      J += (double)oq_pade<T>((T)S.j2[o], (T)S.j2[o + 1], r);
+    }
+    if (S.has_bs2)
+      J += (double)oq_bs_val<T>(like ? S.bs2_like : S.bs2_unlike,
+                                like ? S.bs2_n_like : S.bs2_n_unlike,
+                                (T)(like ? S.bs2_dinv_like : S.bs2_dinv_unlike),
+                                (T)S.bs2_rcut, r);
+  }
+  for (int I = 0; I < S.natm; ++I) {
+    const double dx = xe - S.nuc[I][0], dy = ye - S.nuc[I][1], dz = ze - S.nuc[I][2];
+    const T r = sqrt((T)(dx * dx + dy * dy + dz * dz));
+    if (S.has_j1) J += (double)oq_pade<T>((T)S.j1a[I], (T)S.j1b[I], r);
+    if (S.has_bs1 && S.bs1_type[I] >= 0) {
+      const int ty = S.bs1_type[I];
+      J += (double)oq_bs_val<T>(S.bs1_c[ty], S.bs1_n[ty], (T)S.bs1_dinv[ty],
+                                (T)S.bs1_rcut[ty], r);
+    }
+  }
+  if (S.has_j3) J -= (double)oq_j3_electron<T>(S, pos, ps, NE, e, e + 1, xe, ye, ze);
+  return J;
 }
 
 struct OqElocArgs {
@@ -832,6 +891,10 @@ struct OqElocArgs {
   double* el_trace;       // (W) local energies of this measurement, or null
   double* eparts;         // (W, 4) ee, en, ke, E_L, or null
   unsigned* flags;
+  // per-walker outputs of oqmc_state_eval (null in the sampling kernels)
+  double* logpsi;         // (W): holds log|det| on entry; each electron adds its J share
+  double* grad;           // (W, NE, 3) gradient of log|psi|
+  double* lap;            // (W, NE) Laplacian of log|psi|
 };
 
 // Local energy, one thread per (walker, electron): blockDim = (32, NE), lane
@@ -871,10 +934,24 @@ k_eloc(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
   const int w = blockIdx.x * 32 + lane;
   const bool live = w < W;
   double ee = 0.0, en = 0.0, lp_tot = 0.0, g2 = 0.0;
-  if (live)
-    oq_eloc_electron<NOCC, T, Real, B>(S, S, SP, C, a.pos + w, (size_t)W,
-                                       reinterpret_cast<const Real*>(a.ainv) + w, (size_t)W, e,
-                                       ee, en, lp_tot, g2);
+  if (live) {
+    double gx, gy, gz, le;
+    oq_eloc_electron_out<NOCC, T, Real, B>(S, S, SP, C, a.pos + w, (size_t)W,
+                                           reinterpret_cast<const Real*>(a.ainv) + w,
+                                           (size_t)W, e, ee, en, lp_tot, g2, gx, gy, gz, le);
+    if (a.grad) {
+      double* g = a.grad + ((size_t)w * NE + e) * 3;
+      g[0] = gx; g[1] = gy; g[2] = gz;
+    }
+    if (a.lap) a.lap[(size_t)w * NE + e] = le;
+    if (a.logpsi) {
+      const double* pw = a.pos + w;
+      atomicAdd(a.logpsi + w,
+                oq_jastrow_value_electron<NE, T>(S, pw, (size_t)W, e, pw[(size_t)(3 * e) * W],
+                                                 pw[(size_t)(3 * e + 1) * W],
+                                                 pw[(size_t)(3 * e + 2) * W]));
+    }
+  }
   red[(e * 4 + 0) * 32 + lane] = ee;
   red[(e * 4 + 1) * 32 + lane] = en;
   red[(e * 4 + 2) * 32 + lane] = lp_tot;
@@ -908,7 +985,7 @@ k_eloc(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     vals[k] = v;
   }
-  if (lane == 0) {
+  if (lane == 0 && a.sums) {
 #pragma unroll
     for (int k = 0; k < 5; ++k) atomicAdd(a.sums + k, vals[k]);
     atomicAdd(a.sums + 6, vals[5]);

@@ -115,6 +115,23 @@ class WalkerEnsemble:
                 self.refresh(stream=stream)
         return sums
 
+    def equilibrate(self, n_steps, step, target=0.4, rate=0.05, stream=None):
+        """Equilibration with the reference's per-step width adaptation
+        (``vmc_gto.py:121-126, 1338-1357``) done on the device: n_steps
+        sweeps, no host round trip between them.  Returns (final width,
+        per-sweep acceptance ratios, per-sweep widths) as a float and two
+        CUDA tensors."""
+        dev = self.X.device
+        s = torch.tensor([float(step)], dtype=torch.float64, device=dev)
+        acc = torch.empty(max(int(n_steps), 1), dtype=torch.float64, device=dev)
+        trace = torch.empty_like(acc)
+        self.ctx.equilibrate(self.X, self.state, self.prec, n_steps, s, target, rate, self.seed,
+                             self.step_count, self.refresh_every, self.since_refresh, acc,
+                             trace, stream=stream)
+        self.step_count += int(n_steps)
+        self.since_refresh = (self.since_refresh + int(n_steps)) % self.refresh_every
+        return float(s.item()), acc[:n_steps], trace[:n_steps]
+
     def basin(self, n_steps, sigma=1.5, stream=None):
         """Basin relocation moves (``vmc_gto.py:925-957``); returns the mean
         acceptance."""
@@ -124,6 +141,11 @@ class WalkerEnsemble:
         self.step_count += n_steps
         self.refresh(stream=stream)
         return float(acc.item()) / max(1, n_steps * self.W)
+
+    def state_evaluate(self, stream=None):
+        """Per-walker log|psi|, gradient, Laplacian and local-energy parts as
+        the sampler sees them (tracked inverses, this ensemble's precision)."""
+        return self.ctx.state_evaluate(self.state, self.W, self.prec, stream=stream)
 
     def logdet(self):
         off = self.state.numel() - ((self.W * 8 + 255) // 256) * 256
