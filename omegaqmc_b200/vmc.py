@@ -63,6 +63,27 @@ def binning_analysis(a):
     return float(xbar), float(sdev * math.sqrt(kappa / n)), float(sdev), float(kappa)
 
 
+def key_data_from_seed(seed):
+    """The checkpoint's ``rng_key``: two uint32 words, the key data of
+    ``jax.random.PRNGKey(seed)`` for the threefry generator (high word,
+    low word), which the reference restores with ``jax.random.wrap_key_data``
+    (``OmegaQMC/vmc_gto.py:1403-1410, 1606-1610``)."""
+    seed = int(seed) & (2**64 - 1)
+    return np.array([seed >> 32, seed & 0xFFFFFFFF], dtype=np.uint32)
+
+
+def seed_from_key_data(key):
+    """Inverse of :func:`key_data_from_seed`: the 64-bit seed of a
+    checkpoint's ``rng_key`` (two uint32 words, as the reference writes
+    them); a single integer is taken as the seed itself."""
+    k = np.asarray(key).ravel()
+    if k.size == 2:
+        return (int(k[0]) & 0xFFFFFFFF) << 32 | (int(k[1]) & 0xFFFFFFFF)
+    if k.size == 1:
+        return int(k[0])
+    raise ValueError(f"rng_key must hold one seed or two uint32 words, got {k.size} values")
+
+
 def _validate_params_corr(params_corr):
     """Empty entries are dropped; J2 cusp coefficients are checked
     (``vmc_gto.py:542-626``)."""
@@ -167,6 +188,8 @@ class VMCDriverGTO:
         elif move != "single":
             raise ValueError("move must be 'single' or 'all'")
         self.proposal = proposal
+        self.move = move
+        self.equilibration_seconds = None
         self.persistent = bool(persistent)
         self.precision = precision
         self.ofname_chkpt = prefix + ".chk"
@@ -175,6 +198,11 @@ class VMCDriverGTO:
         self.results = None
 
     # ------------------------------------------------------------------
+    def _device_equilibration(self, world):
+        """Whether equilibration runs on the device (``oqmc_equilibrate``):
+        one process, single-determinant trial, single-electron moves."""
+        return world == 1 and self.system.md is None and self.move == "single"
+
     def _fused_sampler(self, ens, step, n_meas):
         """The fused persistent launch (FP64 refresh, sweeps and local energies
         in one kernel per <= 50 sweeps) for the production blocks.  Same
@@ -249,7 +277,7 @@ class VMCDriverGTO:
                              f"or 'off', got {gpu_memory_check!r}")
         if compute_gradients:
             raise NotImplementedError("force estimators are not on this path")
-        seed = int(np.asarray(rng_key).ravel()[0]) if not isinstance(rng_key, int) else rng_key
+        seed = rng_key if isinstance(rng_key, int) else seed_from_key_data(rng_key)
         s = self.system
         # replicas: with an initialised torch.distributed process group every
         # rank samples num_walkers walkers of its own and the block statistics
@@ -264,7 +292,7 @@ class VMCDriverGTO:
             d = self._load()
             block_cnt_start = int(d["block_count"]) + 1
             mc_stepsize = float(d["mc_stepsize"])
-            seed = int(np.asarray(d["rng_key"]).ravel()[0])
+            seed = seed_from_key_data(d["rng_key"])
             X = np.asarray(d["walkers"])
             E_b = list(np.asarray(d["E_blocks"]))
             print("Restarting ...")
@@ -275,16 +303,30 @@ class VMCDriverGTO:
             print(f"ℹ️\tBasin thermalization: {num_steps_basin} "
                   f"relocation steps, acceptance {acc:.2f}")
         ratio = TARGET_ACCEPTANCE_RATE
-        if not mode_restart:
-            one = torch.zeros(1, NSUM, dtype=torch.float64, device=ens.X.device)
-            for _ in range(num_blocks_equil * num_steps_per_block):
-                one.zero_()
-                ens.run(1, mc_stepsize, sums=one)
-                RP.combine_sums(one)
-                ratio = float(one[0, 5]) / (ens.W * world * s.n_e)
-                mc_stepsize = float(np.exp(np.log(mc_stepsize) + STEP_SIZE_ADAPTATION_RATE
-                                           * (ratio - TARGET_ACCEPTANCE_RATE)))
+        n_equil = num_blocks_equil * num_steps_per_block
+        if not mode_restart and n_equil > 0:
+            t_eq = datetime.now()
+            if self._device_equilibration(world):
+                # the whole scan on the device: sweep, adapt, sweep, ...
+                mc_stepsize, accs, _ = ens.equilibrate(n_equil, mc_stepsize,
+                                                       TARGET_ACCEPTANCE_RATE,
+                                                       STEP_SIZE_ADAPTATION_RATE)
+                ratio = float(accs[-1])
+            else:
+                # replicas adapt one width from the acceptance of all ranks;
+                # other move kinds adapt on the host
+                one = torch.zeros(1, NSUM, dtype=torch.float64, device=ens.X.device)
+                for _ in range(n_equil):
+                    one.zero_()
+                    ens.run(1, mc_stepsize, sums=one)
+                    RP.combine_sums(one)
+                    ratio = float(one[0, 5]) / (ens.W * world * s.n_e)
+                    mc_stepsize = float(np.exp(np.log(mc_stepsize) + STEP_SIZE_ADAPTATION_RATE
+                                               * (ratio - TARGET_ACCEPTANCE_RATE)))
+            self.equilibration_seconds = (datetime.now() - t_eq).total_seconds()
             print(f"ℹ️\tEquilibration acceptance rate: {ratio:.2f}")
+            print(f"ℹ️\tEquilibration: {n_equil} steps in "
+                  f"{self.equilibration_seconds:.2f} s")
         mc_timestep = mc_stepsize * mc_stepsize / 3
         print(f"ℹ️\tAdjusted step size: {mc_stepsize:.4f} bohr "
               f"~ {mc_timestep:.4f} Ha⁻¹ in Brownian time")
@@ -344,7 +386,7 @@ class VMCDriverGTO:
             "system/ao_basis": " ".join([str(mol.basis)] * mol.natm),
             "system/units": "BOHR",
             "E_blocks": np.array(E_b),
-            "rng_key": np.array([seed], dtype=np.int64),
+            "rng_key": key_data_from_seed(seed),
             "block_count": np.int32(block_cnt),
             "mc_stepsize": float(mc_stepsize),
             "walkers": ens.X.cpu().numpy(),

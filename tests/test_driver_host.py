@@ -44,3 +44,55 @@ def test_fused_block_launches(per_block, every):
     assert ens.step_count == 120 + n_sw
     assert torch.all(ens.X == n_sw)          # walkers copied back from the launch
     assert out.shape == (per_block, 8)
+
+
+def test_rng_key_is_threefry_key_data():
+    """rng_key in the checkpoint is what jax.random.key_data(PRNGKey(seed))
+    holds for the threefry generator, two uint32 words (high, low), which
+    the reference's restart wraps back into a key
+    (OmegaQMC/vmc_gto.py:1403-1410, 1606-1610)."""
+    import numpy as np
+    from omegaqmc_b200.vmc import key_data_from_seed, seed_from_key_data
+    for seed in (0, 1, 888, 2**32 - 1, 2**32 + 5, 2**64 - 1):
+        k = key_data_from_seed(seed)
+        assert k.dtype == np.uint32 and k.shape == (2,)
+        assert seed_from_key_data(k) == seed
+    assert list(key_data_from_seed(42)) == [0, 42]          # PRNGKey(42) key data
+    assert seed_from_key_data(np.array([7], dtype=np.int64)) == 7
+    with pytest.raises(ValueError):
+        seed_from_key_data(np.zeros(3, dtype=np.uint32))
+
+
+def _ckpt(W=3, n_e=2):
+    import numpy as np
+    from omegaqmc_b200.vmc import key_data_from_seed
+    return {"version": "0.1.0", "timestamps/start": "t0", "timestamps/end": "t1",
+            "system/atom_symbols": "H H", "system/atom_coords": np.zeros((2, 3)),
+            "system/ao_basis": "sto-3g sto-3g", "system/units": "BOHR",
+            "E_blocks": np.array([-1.1, -1.2]), "rng_key": key_data_from_seed(2**33 + 9),
+            "block_count": np.int32(2), "mc_stepsize": 0.45,
+            "walkers": np.arange(W * n_e * 3, dtype=np.float64).reshape(W, n_e, 3)}
+
+
+@pytest.mark.parametrize("use_h5", [False, True])
+def test_checkpoint_round_trip(tmp_path, use_h5, monkeypatch):
+    """The checkpoint keeps the reference's dataset names and types; HDF5
+    where h5py imports (the reference's format), else .npz with the same
+    keys."""
+    import sys
+    import types
+    import numpy as np
+    from omegaqmc_b200.vmc import seed_from_key_data
+    if use_h5:
+        pytest.importorskip("h5py")
+    else:
+        monkeypatch.setitem(sys.modules, "h5py", None)
+    base = str(tmp_path / "run.chk")
+    data = _ckpt()
+    path = VMCDriverGTO._save(None, base, data)
+    assert path.endswith(".h5" if use_h5 else ".npz")
+    d = VMCDriverGTO._load(types.SimpleNamespace(ofname_chkpt=base))
+    assert int(d["block_count"]) == 2 and float(d["mc_stepsize"]) == 0.45
+    assert seed_from_key_data(d["rng_key"]) == 2**33 + 9
+    assert np.array_equal(d["walkers"], data["walkers"])
+    assert np.array_equal(d["E_blocks"], data["E_blocks"])
