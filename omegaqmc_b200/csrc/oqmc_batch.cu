@@ -24,9 +24,31 @@
 #include "oqmc_rtc.h"
 #include "../../include/oqmc_b200.h"
 
-static_assert(sizeof(OqJas) + sizeof(int) <= OQ_BATCH_HDR, "batch header too small");
-
 namespace {
+
+std::string lit(double v) {
+  char b[40];
+  snprintf(b, sizeof(b), "%.17g", v);
+  return b;
+}
+
+// The nuclei and Jastrow constants of one system as a constant-memory
+// OqJas with the values written in.
+std::string jas_source(const OqSystem& S, const std::string& name) {
+  std::string nuc, Z, a, b;
+  for (int I = 0; I < S.natm; ++I) {
+    const char* sep = I ? ", " : "";
+    nuc += std::string(sep) + "{" + lit(S.nuc[I][0]) + ", " + lit(S.nuc[I][1]) + ", " +
+           lit(S.nuc[I][2]) + "}";
+    Z += sep + lit(S.Z[I]);
+    a += sep + lit(S.j1a[I]);
+    b += sep + lit(S.j1b[I]);
+  }
+  return "__constant__ OqJas " + name + " = {" + std::to_string(S.natm) + ", " +
+         std::to_string(S.has_j1) + ", " + std::to_string(S.has_j2) + ", 0, " + lit(S.e_nn) +
+         ", {" + nuc + "}, {" + Z + "}, {" + a + "}, {" + b + "}, {" + lit(S.j2[0]) + ", " +
+         lit(S.j2[1]) + ", " + lit(S.j2[2]) + ", " + lit(S.j2[3]) + "}};\n";
+}
 
 struct Variant {
   int maxt, minb;
@@ -42,7 +64,7 @@ std::string batch_source(const std::vector<const OqSystem*>& S,
   std::string src = "#include \"oqmc_batch.cuh\"\n\n";
   for (size_t k = 0; k < S.size(); ++k)
     src += oq_spec_basis_source(*S[k], *SP[k], C[k], nocc[k], "OqSpecBasis_" + std::to_string(k)) +
-           "\n";
+           "\n" + jas_source(*S[k], "oq_jas_" + std::to_string(k)) + "\n";
   src +=
       "template <typename T, typename Real, int MAXT, int MINB>\n"
       "__global__ void __launch_bounds__(MAXT, MINB) k_batch(OqBatchArgs a) {\n"
@@ -58,7 +80,8 @@ std::string batch_source(const std::vector<const OqSystem*>& S,
   for (size_t k = 0; k < S.size(); ++k) {
     const std::string ks = std::to_string(k);
     src += "      case " + ks + ": oq_batch_tile<" + std::to_string(nocc[k]) +
-           ", T, Real, OqSpecBasis_" + ks + ">(a, d, tl.w0, step0, slot0, smem); break;\n";
+           ", T, Real, OqSpecBasis_" + ks + ">(a, d, oq_jas_" + ks +
+           ", tl.w0, step0, slot0, smem); break;\n";
   }
   src +=
       "      default: break;\n"
@@ -75,10 +98,12 @@ std::string kernel_name(int precision, int v) {
          std::to_string(kVariants[v].minb) + ">";
 }
 
-// Shared memory of one tile (matches the carve-up in oq_batch_tile).
+// Shared memory of one tile (matches the carve-up in oq_batch_tile): the
+// reduction buffer only when several threads share a walker, then positions
+// and inverses.
 size_t tile_smem(int nocc, int wt, int nt, int precision) {
   const size_t real = precision == OQ_PREC_MIXED ? 4 : 8;
-  return OQ_BATCH_HDR + (size_t)4 * nt * 8 + (size_t)6 * nocc * wt * 8 +
+  return (nt > wt ? (size_t)4 * nt * 8 : 0) + (size_t)6 * nocc * wt * 8 +
          (size_t)2 * nocc * nocc * wt * real;
 }
 

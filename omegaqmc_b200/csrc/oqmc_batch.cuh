@@ -100,16 +100,21 @@ __device__ __forceinline__ void oq_jas_load(OqJas& J, const OqSystem& S) {
   }
 }
 
-// Process one tile: refresh, n_sweeps sweeps with measurements, write back.
-template <int NOCC, typename T, typename Real, class B>
-__device__ __forceinline__ void oq_batch_tile(const OqBatchArgs& a, const OqBatchSys& d, int w0,
-                                              uint64_t step0, uint64_t slot0,
-                                              unsigned char* smem) {
+// Shared memory of one tile: [reduction [NT/WT][4][WT] doubles, only when
+// several threads share a walker's local energy][positions [3 NE][WT]
+// doubles][inverses [2 NOCC^2][WT] Real].  The nuclei and Jastrow constants
+// (J) are the system's OqJas in constant memory, written into the generated
+// module, so every lane of a warp reads the same word (a broadcast) and the
+// tile's shared memory holds walker state only.
+template <int NOCC, typename T, typename Real, class B, class SJ>
+__device__ __forceinline__ void oq_batch_tile(const OqBatchArgs& a, const OqBatchSys& d,
+                                              const SJ& J, int w0, uint64_t step0,
+                                              uint64_t slot0, unsigned char* smem) {
   constexpr int NE = 2 * NOCC;
   const int NT = blockDim.x, tid = threadIdx.x, WT = d.wt;
-  OqJas& J = *reinterpret_cast<OqJas*>(smem);
-  double* red = reinterpret_cast<double*>(smem + OQ_BATCH_HDR);   // [NT/WT][4][WT]
-  double* pos = red + 4 * NT;                                      // [3 NE][WT]
+  const int parts = NT / WT, part = tid / WT, wl = tid - part * WT;
+  double* red = reinterpret_cast<double*>(smem);                    // [parts][4][WT]
+  double* pos = red + (parts > 1 ? 4 * NT : 0);                     // [3 NE][WT]
   Real* Ai = reinterpret_cast<Real*>(pos + 3 * NE * WT);           // [2 NOCC^2][WT]
   const OqSystem& S = *d.sys;
   const OqSplit& SP = *d.split;
@@ -117,7 +122,6 @@ __device__ __forceinline__ void oq_batch_tile(const OqBatchArgs& a, const OqBatc
                                     : reinterpret_cast<const Real*>(d.C64);
   unsigned long long t_start = 0;
   if (tid == 0) t_start = oq_globaltimer();
-  oq_jas_load(J, S);
   const int cnt = min(WT, d.W - w0);
   {
     const double* src = d.walkers + (size_t)w0 * 3 * NE;
@@ -158,7 +162,6 @@ __device__ __forceinline__ void oq_batch_tile(const OqBatchArgs& a, const OqBatc
     }
   }
   __syncthreads();
-  const int parts = NT / WT, part = tid / WT, wl = tid - part * WT;
   int nacc = 0, meas = 0;
   for (int t = 0; t < a.n_sweeps; ++t) {
     if (live) {
@@ -183,26 +186,31 @@ __device__ __forceinline__ void oq_batch_tile(const OqBatchArgs& a, const OqBatc
     }
     if ((t + 1) % a.measure_every != 0) continue;
     __syncthreads();
+    double see = 0.0, sen = 0.0, slp = 0.0, sg2 = 0.0;
     {
       double ee = 0.0, en = 0.0, lp = 0.0, g2 = 0.0;
       if (wl < cnt)
         for (int e = part; e < NE; e += parts)
           oq_eloc_electron<NOCC, T, Real, B>(J, S, SP, C, pos + wl, (size_t)WT, Ai + wl,
                                              (size_t)WT, e, ee, en, lp, g2);
-      red[(part * 4 + 0) * WT + wl] = ee;
-      red[(part * 4 + 1) * WT + wl] = en;
-      red[(part * 4 + 2) * WT + wl] = lp;
-      red[(part * 4 + 3) * WT + wl] = g2;
-    }
-    __syncthreads();
-    if (mover) {
-      double see = 0.0, sen = 0.0, slp = 0.0, sg2 = 0.0;
-      for (int k = 0; k < parts; ++k) {
-        see += red[(k * 4 + 0) * WT + tid];
-        sen += red[(k * 4 + 1) * WT + tid];
-        slp += red[(k * 4 + 2) * WT + tid];
-        sg2 += red[(k * 4 + 3) * WT + tid];
+      if (parts > 1) {
+        red[(part * 4 + 0) * WT + wl] = ee;
+        red[(part * 4 + 1) * WT + wl] = en;
+        red[(part * 4 + 2) * WT + wl] = lp;
+        red[(part * 4 + 3) * WT + wl] = g2;
+      } else {
+        see = ee; sen = en; slp = lp; sg2 = g2;
       }
+    }
+    if (parts > 1) __syncthreads();
+    if (mover) {
+      if (parts > 1)
+        for (int k = 0; k < parts; ++k) {
+          see += red[(k * 4 + 0) * WT + tid];
+          sen += red[(k * 4 + 1) * WT + tid];
+          slp += red[(k * 4 + 2) * WT + tid];
+          sg2 += red[(k * 4 + 3) * WT + tid];
+        }
       const double ke = -0.5 * (slp + sg2);
       const double el = see + sen + ke + J.e_nn;
       const bool ok = live && isfinite(el);
@@ -238,9 +246,12 @@ __device__ __forceinline__ void oq_batch_tile(const OqBatchArgs& a, const OqBatc
   __syncthreads();
 }
 
-// Claim the next tile for the whole CTA; -1 when none is left.
+// Claim the next tile for the whole CTA; -1 when none is left.  The claimed
+// index passes through the first word of shared memory, which belongs to the
+// tile state only between this call's second barrier and the end of the
+// tile (oq_batch_tile ends with a barrier).
 __device__ __forceinline__ int oq_batch_next(const OqBatchArgs& a, unsigned char* smem) {
-  int* slot = reinterpret_cast<int*>(smem + sizeof(OqJas));
+  int* slot = reinterpret_cast<int*>(smem);
   if (threadIdx.x == 0) {
     const unsigned k = atomicAdd(&a.ctl->next, 1u);
     *slot = k < (unsigned)a.n_tiles ? (int)k : -1;
