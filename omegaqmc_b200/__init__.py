@@ -7,6 +7,8 @@ The arithmetic runs in ``liboqmc_b200.so`` (sm_100a CUDA, C ABI in
 ``include/oqmc_b200.h``)."""
 from __future__ import annotations
 
+import os
+
 from .system import Mole, MeanField, build_system, read_shell  # noqa: F401
 
 __version__ = "0.1.0"
@@ -36,8 +38,10 @@ def generate_molecular_orbitals(astr, units="Bohr", basis="cc-pvdz-shaped", spin
                                 charge=0, ao_splines=None, **kw):
     """RHF mean-field object for ``astr`` (``OmegaQMC/vmc_gto.py:217-452`` runs
     PySCF; here the package's own RHF).  ``basis`` is a PySCF-format dict
-    ``{element: [[am, [alpha, c...], ...], ...]}`` or one of the generated
-    sets ``"cc-pvdz-shaped"`` / ``"sto-3g"`` (H only).  ``ao_splines``
+    ``{element: [[am, [alpha, c...], ...], ...]}``, basis-set text in NWChem
+    or Gaussian94 format (or the path of such a file, or a dict of texts per
+    element; :mod:`omegaqmc_b200.basis`), or one of the generated sets
+    ``"cc-pvdz-shaped"`` / ``"sto-3g"`` (H only).  ``ao_splines``
     (True or a dict of grid options) switches on the quintic radial-spline
     AO transform, stored on ``mf.mol.ao_radial_transform`` as in the
     reference (``vmc_gto.py:278-290, 415``)."""
@@ -45,16 +49,22 @@ def generate_molecular_orbitals(astr, units="Bohr", basis="cc-pvdz-shaped", spin
     from .rhf import run_rhf
     if spin != 0:
         raise NotImplementedError("only closed-shell RHF is supported")
+    from .basis import load_basis
+    atoms = Mole(astr, {s: [] for s in M.ELEMENT_Z}, unit=units)._atom
+    syms = sorted({s for s, _ in atoms})
     if isinstance(basis, str):
         name = basis.lower()
-        atoms = Mole(astr, {s: [] for s in M.ELEMENT_Z}, unit=units)._atom
-        syms = sorted({s for s, _ in atoms})
         if name == "cc-pvdz-shaped":
             basis = {s: M.ccpvdz_shaped(s) for s in syms}
         elif name == "sto-3g" and syms == ["H"]:
             basis = {"H": M.sto3g_h()}
+        elif "\n" in basis or os.path.exists(basis):
+            basis = load_basis(basis, syms)
         else:
-            raise ValueError(f"unknown basis {basis!r}; pass a PySCF-format dict")
+            raise ValueError(f"unknown basis {basis!r}; pass a PySCF-format dict or the "
+                             "NWChem / Gaussian94 text of the basis set")
+    elif isinstance(basis, dict) and any(isinstance(v, str) for v in basis.values()):
+        basis = load_basis(basis, syms)
     mol = Mole(astr, basis, unit=units, charge=charge, basis_name="gen")
     mol.ao_radial_transform = ao_splines
     return run_rhf(mol, **kw)
