@@ -11,7 +11,8 @@ local-energy kernels through oqmc_sweeps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--precision mixed|fp64] [--system H2O] [--walkers 65536]
-                    [--path persistent|split] [--workload h2o|batched|learned|alle]
+                    [--path persistent|split]
+                    [--workload h2o|batched|learned|alle|h2|lih]
 
 value     = walkers x sweeps/s / tau_int(E_L)  (decorrelated samples/s, all ranks)
 tau_int   = kappa of the reference's do_binning_analysis (OmegaQMC/utils.py:86-150)
@@ -43,12 +44,27 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 REFRESH_EVERY = 50
+
+
+def binning_analysis(series):
+    """(mean, serr, sdev, kappa) of the reference's do_binning_analysis
+    (OmegaQMC/utils.py:86-150), the package's copy the VMC driver uses."""
+    from omegaqmc_b200.vmc import binning_analysis as ba
+    return ba(series)
+
 EQUIL_SWEEPS = 3000
 SCALED_R0, SCALED_FMIN = 1.0, 0.05
 # nucleus-scaled proposal of the persistent headline path (chosen by measured
 # tau_int on H2O: fmin 0.02 and acceptance 0.5 gave tau 1.5 sweeps, against
 # 2.4 for fmin 0.05 and 4.1 at the reference's 0.4 target)
 HEAD_R0, HEAD_FMIN, HEAD_ACC = 1.0, 0.02, 0.5
+# the headline's timed region lasts at least this long (s); its sweep count
+# is capped by the measurement buffer
+MIN_TIMED_S = 2.0
+MAX_TIMED_SWEEPS = 60000
+# the plain FP64 sampler's tau_int (several hundred sweeps) comes from this
+# many consecutive segments of PLAIN_SEG sweeps: their kappas give the spread
+PLAIN_SEGS, PLAIN_SEG = 4, 12500
 
 
 def parse():
@@ -67,10 +83,14 @@ def parse():
     ap.add_argument("--proposal", default="scaled", choices=["scaled", "plain"])
     ap.add_argument("--eloc", default="cc", choices=["cc", "tc"],
                     help="local energy on CUDA cores (specialised) or tensor cores (tcgen05)")
-    ap.add_argument("--workload", default="h2o", choices=["h2o", "batched", "learned", "alle"],
+    ap.add_argument("--workload", default="h2o",
+                    choices=["h2o", "batched", "learned", "alle", "h2", "lih"],
                     help="h2o: the headline H2O metric; batched: H2, LiH, H2O, N2 and "
                          "(H2O)2 in one persistent launch under a CUDA graph; learned: N2 "
-                         "with the trained MLP proposal against the plain random walk")
+                         "with the trained MLP proposal against the plain random walk; "
+                         "alle: the reference's all-electron move; h2, lih: "
+                         "configurations 1 and 2 (H2 FP64; LiH FP64 against mixed, with "
+                         "per-output errors)")
     ap.add_argument("--path", default="persistent", choices=["persistent", "split"],
                     help="persistent: one fused launch per 50 sweeps (refresh, moves, E_L) "
                          "under a CUDA graph; split: separate move / local-energy kernels")
@@ -181,7 +201,6 @@ def cpu_reference(system, seconds, nthreads, step, seed=7, n_equil=300):
     adaptation during equilibration, then fixed-step production); returns
     (walker-steps/s, tau_int, acceptance, sample description, E_L series)."""
     from oracle import cref
-    from oracle import gto_oracle as O
     from omegaqmc_b200.sampler import init_walkers_gaussian
     W = 256
     X = np.ascontiguousarray(init_walkers_gaussian(system, W, 1.0, seed))
@@ -196,10 +215,50 @@ def cpu_reference(system, seconds, nthreads, step, seed=7, n_equil=300):
     ser, acc = cref.run(system, X, n, step, seed=seed + 2, nthreads=nthreads)
     dt = time.perf_counter() - t0
     rate = W * n / dt
-    _, _, _, kappa = O.binning_analysis(ser[:, 3])
+    _, _, _, kappa = binning_analysis(ser[:, 3])
     return (rate, kappa, acc,
             f"{W} walkers x {n} steps ({dt:.1f} s) after {n_equil} adaptive equilibration "
             f"steps, step {step:.3f}", ser[:, 3])
+
+
+def output_errors(ctx, X, precision, step, seed):
+    """Error of every per-walker output the sampler works with
+    (oqmc_state_eval: tracked log|psi|, grad log|psi|, per-electron
+    Laplacian, E_L) against the FP64 evaluation at the same positions
+    (oqmc_eval, itself matched to the oracle at 1e-10), on the given
+    configurations: right after the FP64 LU refresh, and after 49 sweeps of
+    Sherman-Morrison updates (the longest stretch between refreshes).
+    Errors: |d| for log|psi| and E_L (Ha); |d| / (|x| + 1) for each
+    gradient component and Laplacian.  Returns max / p99 / median each."""
+    from omegaqmc_b200.sampler import WalkerEnsemble
+    out = {"walkers": int(X.shape[0])}
+    for sweeps in (0, 49):
+        ens = WalkerEnsemble(ctx, X, precision, seed=seed, refresh_every=10**9)
+        if sweeps:
+            ens.run(sweeps, step)
+        got = ens.state_evaluate()
+        ref = ctx.evaluate(ens.X)
+        errs = {"logpsi": (got["logpsi"] - ref["logpsi"]).abs(),
+                "grad": (got["grad"] - ref["grad"]).abs() / (ref["grad"].abs() + 1),
+                "lap": (got["lap"] - ref["lap"]).abs() / (ref["lap"].abs() + 1),
+                "e_loc": (got["e_loc"] - ref["e_loc"]).abs()}
+        st = {}
+        for k, v in errs.items():
+            v = v.reshape(-1).cpu().numpy()
+            st[k] = {"max": float(v.max()), "p99": float(np.quantile(v, 0.99)),
+                     "median": float(np.median(v))}
+        out[f"after_{sweeps}_sweeps"] = st
+        del ens
+    return out
+
+
+def kappa_spread(series, parts):
+    """kappa of each of `parts` consecutive segments of a series: their mean
+    and standard error (the uncertainty of a tau_int estimate)."""
+    n = len(series) // parts
+    ks = [binning_analysis(series[i * n:(i + 1) * n])[3] for i in range(parts)]
+    return {"segments": parts, "segment_sweeps": n, "kappas": ks,
+            "mean": float(np.mean(ks)), "serr": float(np.std(ks, ddof=1) / np.sqrt(parts))}
 
 
 def sweep_launches(ens, n_sweeps, measure_every=1):
@@ -259,9 +318,10 @@ def run_reference(a):
         "value": value, "unit": unit, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": 256 / rate * 1e3, "higher_is_better": True, "scaling": "weak",
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{a.system} cc-pVDZ-shaped, {a.walkers} walkers/GPU, "
-                               "single-electron sweeps + E_L every sweep, FP64 LU refresh "
-                               f"every {REFRESH_EVERY}",
+        "config": {"workload": f"{a.system} cc-pVDZ-shaped, 256 walkers per timed sample on "
+                               f"{cores} host threads, all-electron Gaussian steps (the "
+                               "reference's move) + E_L every step, FP64, no refresh (every "
+                               "step recomputes log|psi| afresh)",
                    "reference_path": "the reference algorithm (all-electron Gaussian moves, "
                                      "log|psi| recomputed twice per step, E_L every step) in "
                                      f"C/OpenMP on {cores} host threads",
@@ -284,7 +344,6 @@ def run_ours(a):
     from omegaqmc_b200 import _lib as L
     from omegaqmc_b200.context import GTOContext
     from omegaqmc_b200.sampler import WalkerEnsemble, init_walkers_gaussian, NSUM
-    from oracle import gto_oracle as O  # noqa: F401  (tau estimator is the oracle's restatement)
 
     rank, world, local = dist_env()
     if world > 1:
@@ -345,7 +404,7 @@ def run_ours(a):
         aux = ens.run(2000, step).cpu().numpy()
         tau_series = aux[:, 3] / np.maximum(aux[:, 6], 1)
         tau_src = "untimed 2000-sweep series"
-    e_mean, e_serr, e_sdev, kappa = O.binning_analysis(tau_series)
+    e_mean, e_serr, e_sdev, kappa = binning_analysis(tau_series)
     acc = float(s_np[:, 5].sum() / (K * W * system.n_e))
 
     # the comparison target: the plain FP64 sampler on the same walkers
@@ -368,7 +427,7 @@ def run_ours(a):
         pms = p0.elapsed_time(p1)
         pn = ps.cpu().numpy()
         pser = pn[:, 3] / np.maximum(pn[:, 6], 1)
-        pm, pse, _, pk = O.binning_analysis(pser)
+        pm, pse, _, pk = binning_analysis(pser)
         pw = W * Kp / (pms * 1e-3)
         plain = {"value": pw * world / pk, "walker_sweeps_per_s": pw * world, "tau_int": pk,
                  "proposal": "fixed-width Gaussian", "step": pstep,
@@ -435,6 +494,9 @@ def run_ours(a):
     line = {
         "metric": "decorrelated samples/s (walker-steps/s / tau_int) vs plain FP64, H2O 64k walkers",
         "value": value, "unit": "decorrelated samples/s", "n_gpus": world, "steps": K,
+        "steps_requested": a.steps,
+        "steps_note": f"the timed region replays whole 50-sweep launches for at least "
+                      f"{MIN_TIMED_S:g} s: {K} sweeps",
         "warmup": a.warmup, "ms_per_step": ms_max / K, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64" if a.precision == "mixed" else "f64",
@@ -501,7 +563,6 @@ def run_persistent(a):
     from omegaqmc_b200.batch import BatchedSampler
     from omegaqmc_b200.context import GTOContext
     from omegaqmc_b200.sampler import WalkerEnsemble, init_walkers_gaussian, NSUM
-    from oracle import gto_oracle as O  # noqa: F401  (tau estimator is the oracle's restatement)
 
     rank, world, local = dist_env()
     if world > 1:
@@ -513,14 +574,14 @@ def run_persistent(a):
     t_spec = time.perf_counter()
     ctx.specialize()
     W = a.walkers
-    K = max(REFRESH_EVERY, (a.steps // REFRESH_EVERY) * REFRESH_EVERY)
-    n_launch = K // REFRESH_EVERY
+    K_req = max(REFRESH_EVERY, (a.steps // REFRESH_EVERY) * REFRESH_EVERY)
+    cap = max(K_req, MAX_TIMED_SWEEPS, 2000)
     seed = 2024 + 7919 * rank
     scaled = a.proposal == "scaled"
     X0 = init_walkers_gaussian(system, W, 1.0, seed=1000 + rank)
     b = BatchedSampler([ctx], [X0], [a.step_size or 0.8], precision=a.precision,
                        proposal=a.proposal, scale_r0=HEAD_R0, scale_fmin=HEAD_FMIN,
-                       cap=max(K, 2000))
+                       cap=cap)
     t_spec = time.perf_counter() - t_spec
     stream = torch.cuda.current_stream()
     EQ1, EQ2, WARM, KERN, E2E = 10**7, 2 * 10**7, 3 * 10**7, 4 * 10**7, 5 * 10**7
@@ -538,6 +599,26 @@ def run_persistent(a):
     cfg, _ = b.tune(4, seed=seed ^ 0x55)
     step = b.steps()[0]
     sweeps_no_meas(max(a.warmup, 3), WARM)
+    # the timed region replays at least MIN_TIMED_S of launches, whatever
+    # --steps asks for: two launches timed alone set the count (the same on
+    # every rank: the max over ranks)
+    b.reset(KERN)
+    q0 = torch.cuda.Event(enable_timing=True)
+    q1 = torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    for _ in range(2):
+        b.run(REFRESH_EVERY, 1, seed)
+    q1.record(stream)
+    torch.cuda.synchronize()
+    tq = torch.tensor([q0.elapsed_time(q1) / 2], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tq, op=dist.ReduceOp.MAX)
+    n_launch = max(K_req // REFRESH_EVERY,
+                   int(np.ceil(MIN_TIMED_S * 1e3 / max(float(tq[0]), 1e-3))))
+    n_launch = min(n_launch, cap // REFRESH_EVERY)
+    if a.quick:                      # profiling: exactly the launches asked for
+        n_launch = K_req // REFRESH_EVERY
+    K = n_launch * REFRESH_EVERY
     b.capture(n_launch, REFRESH_EVERY, 1, seed)
     b.reset(0)
     torch.cuda.synchronize()
@@ -570,7 +651,8 @@ def run_persistent(a):
         aux = RP.combine_sums(b.sums[0][:2000].clone()).cpu().numpy()
         tau_series = RP.walker_mean_series(aux)
         tau_src = "untimed 2000-sweep series"
-    e_mean, e_serr, e_sdev, kappa = O.binning_analysis(tau_series)
+    e_mean, e_serr, e_sdev, kappa = binning_analysis(tau_series)
+    kq = kappa_spread(tau_series, 4)
 
     # one launch (refresh + 50 sweeps) timed on its own: the roofline denominator
     b.reset(KERN)
@@ -582,35 +664,75 @@ def run_persistent(a):
     torch.cuda.synchronize()
     launch_ms = k0.elapsed_time(k1)
 
-    plain = prec = None
+    plain = prec = fp64s = None
     if not a.quick and (a.precision != "fp64" or a.proposal != "plain"):
-        # the comparison: plain FP64 sampler through the same path
+        # the comparison: plain FP64 sampler through the same path; its
+        # tau_int (several hundred sweeps) from PLAIN_SEGS consecutive
+        # segments of one chain, PLAIN_SEG sweeps each, all timed
         pb = BatchedSampler([ctx], [b.walkers[0].clone()], [STEP_DEFAULT.get(a.system, 0.3)],
-                            precision="fp64", proposal="plain", cap=4000)
+                            precision="fp64", proposal="plain", cap=PLAIN_SEG)
         pstep = pb.adapt_steps(0.4, seed=seed ^ 2)[0]
         pb.reset(EQ1 + 10**6)
-        for _ in range(10):
+        for _ in range(20):
             pb.run(REFRESH_EVERY, REFRESH_EVERY + 1, seed ^ 3)
         pb.tune(4, seed=seed ^ 4)
-        Kp = 4000
-        pb.reset(0)
-        p0 = torch.cuda.Event(enable_timing=True)
-        p1 = torch.cuda.Event(enable_timing=True)
-        p0.record(stream)
-        for _ in range(Kp // REFRESH_EVERY):
-            pb.run(REFRESH_EVERY, 1, seed ^ 3)
-        p1.record(stream)
-        torch.cuda.synchronize()
-        pms = p0.elapsed_time(p1)
-        pn = pb.sums[0][:Kp].cpu().numpy()
-        pser = pn[:, 3] / np.maximum(pn[:, 6], 1)
-        pm, pse, _, pk = O.binning_analysis(pser)
+        pms, pser = 0.0, []
+        for seg in range(PLAIN_SEGS):
+            pb.reset(seg * PLAIN_SEG)
+            p0 = torch.cuda.Event(enable_timing=True)
+            p1 = torch.cuda.Event(enable_timing=True)
+            p0.record(stream)
+            for _ in range(PLAIN_SEG // REFRESH_EVERY):
+                pb.run(REFRESH_EVERY, 1, seed ^ 3)
+            p1.record(stream)
+            torch.cuda.synchronize()
+            pms += p0.elapsed_time(p1)
+            pn = pb.sums[0][:PLAIN_SEG].cpu().numpy()
+            pser.append(pn[:, 3] / np.maximum(pn[:, 6], 1))
+        pser = np.concatenate(pser)
+        Kp = PLAIN_SEGS * PLAIN_SEG
+        pm, pse, _, pk = binning_analysis(pser)
+        pks = kappa_spread(pser, PLAIN_SEGS)
         pw = W * Kp / (pms * 1e-3)
         plain = {"value": pw * world / pk, "walker_sweeps_per_s": pw * world, "tau_int": pk,
+                 "tau_int_segments": pks,
                  "proposal": "fixed-width Gaussian", "step": pstep, "precision": "fp64",
                  "ms_per_step": pms / Kp, "steps": Kp, "path": "same persistent kernel, FP64",
                  "energy": {"mean": pm, "serr": pse},
                  "energy_diff_sigma": abs(pm - e_mean) / max(np.hypot(pse, e_serr), 1e-300)}
+        del pb
+        # FP64 with the headline's proposal: separates the precision factor
+        # (mixed vs FP64, same proposal) from the proposal factor (scaled vs
+        # fixed-width, both FP64)
+        if a.precision != "fp64" and scaled:
+            fb = BatchedSampler([ctx], [b.walkers[0].clone()], [step], precision="fp64",
+                                proposal="scaled", scale_r0=HEAD_R0, scale_fmin=HEAD_FMIN,
+                                cap=10000)
+            fb.adapt_steps(HEAD_ACC, seed=seed ^ 8)
+            fb.reset(EQ1 + 3 * 10**6)
+            for _ in range(10):
+                fb.run(REFRESH_EVERY, REFRESH_EVERY + 1, seed ^ 9)
+            fb.tune(4, seed=seed ^ 10)
+            Kf = 10000
+            fb.reset(0)
+            f0 = torch.cuda.Event(enable_timing=True)
+            f1 = torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            for _ in range(Kf // REFRESH_EVERY):
+                fb.run(REFRESH_EVERY, 1, seed ^ 9)
+            f1.record(stream)
+            torch.cuda.synchronize()
+            fms = f0.elapsed_time(f1)
+            fn = fb.sums[0][:Kf].cpu().numpy()
+            fser = fn[:, 3] / np.maximum(fn[:, 6], 1)
+            fmu, fse, _, fk = binning_analysis(fser)
+            fw = W * Kf / (fms * 1e-3)
+            fp64s = {"value": fw * world / fk, "walker_sweeps_per_s": fw * world,
+                     "tau_int": fk, "tau_int_segments": kappa_spread(fser, 4),
+                     "ms_per_step": fms / Kf, "steps": Kf, "step": fb.steps()[0],
+                     "proposal": "nucleus-scaled Gaussian (the headline's)", "precision": "fp64",
+                     "energy": {"mean": fmu, "serr": fse}}
+            del fb
         # precision, paired: the mixed and the FP64 sampler start from the same
         # walkers with the same proposal, step, seed and RNG counters, so they
         # take the same decisions until a rounding difference flips one; the
@@ -632,9 +754,9 @@ def run_persistent(a):
             del sb
         mser, mX = runs[a.precision]
         fser, fX = runs["fp64"]
-        mm, mse, _, _ = O.binning_analysis(mser)
-        fm, fse, _, fk = O.binning_analysis(fser)
-        dm, dse, _, _ = O.binning_analysis(mser - fser)
+        mm, mse, _, _ = binning_analysis(mser)
+        fm, fse, _, fk = binning_analysis(fser)
+        dm, dse, _, _ = binning_analysis(mser - fser)
         diverged = float(torch.any((mX != fX).reshape(W, -1), dim=1).float().mean())
         ctx.set_proposal(0)
         ens = WalkerEnsemble(ctx, b.walkers[0], a.precision, seed=seed ^ 7)
@@ -652,7 +774,12 @@ def run_persistent(a):
                                       "serr_Ha": float(dE.std() / np.sqrt(W)),
                                       "median_abs_Ha": float(np.median(np.abs(dE))),
                                       "p99_abs_Ha": float(np.quantile(np.abs(dE), 0.99))}}
-        del pb, ens
+        if scaled:
+            ctx.set_proposal(1, HEAD_R0, HEAD_FMIN)
+        prec["outputs_vs_fp64"] = output_errors(ctx, b.walkers[0][:4096], a.precision, step,
+                                                seed ^ 11)
+        ctx.set_proposal(0)
+        del ens
 
     e2e = None
     if not a.no_e2e:
@@ -693,6 +820,9 @@ def run_persistent(a):
     line = {
         "metric": "decorrelated samples/s (walker-steps/s / tau_int) vs plain FP64, H2O 64k walkers",
         "value": value, "unit": "decorrelated samples/s", "n_gpus": world, "steps": K,
+        "steps_requested": a.steps,
+        "steps_note": f"the timed region replays whole 50-sweep launches for at least "
+                      f"{MIN_TIMED_S:g} s: {K} sweeps",
         "warmup": a.warmup, "ms_per_step": ms_max / K, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64" if a.precision == "mixed" else "f64",
@@ -723,9 +853,27 @@ def run_persistent(a):
                      "flops_per_walker_sweep": work["flops"],
                      "peak_source": "own FMA microkernel (oqmc_measure_peak), of measured"},
     }
+    line["tau_int_segments"] = kq
     if plain:
+        # relative uncertainty of a ratio of decorrelated rates: the two
+        # kappas' standard errors (from their segments) in quadrature
+        def ratio(num, k_num, s_num, den, k_den, s_den):
+            r = num / den
+            return {"value": r, "serr": r * float(np.hypot(s_num / k_num, s_den / k_den))}
         line["plain_fp64"] = plain
-        line["speedup_vs_plain_fp64"] = value / plain["value"]
+        sp = ratio(value, kappa, kq["serr"], plain["value"], plain["tau_int"],
+                   plain["tau_int_segments"]["serr"])
+        line["speedup_vs_plain_fp64"] = sp["value"]
+        line["speedup_vs_plain_fp64_serr"] = sp["serr"]
+        if fp64s:
+            line["fp64_same_proposal"] = fp64s
+            line["mixed_vs_fp64_same_proposal"] = ratio(
+                value, kappa, kq["serr"], fp64s["value"], fp64s["tau_int"],
+                fp64s["tau_int_segments"]["serr"])
+            line["proposal_factor_fp64"] = ratio(
+                fp64s["value"], fp64s["tau_int"], fp64s["tau_int_segments"]["serr"],
+                plain["value"], plain["tau_int"], plain["tau_int_segments"]["serr"])
+            line["throughput_factor_mixed_vs_fp64"] = wss / fp64s["walker_sweeps_per_s"]
     if prec:
         line["precision_check"] = prec
     if e2e:
@@ -765,7 +913,6 @@ def run_batched(a):
     from omegaqmc_b200.batch import BatchedSampler
     from omegaqmc_b200.context import GTOContext
     from omegaqmc_b200.sampler import WalkerEnsemble, init_walkers_gaussian, NSUM, PREC
-    from oracle import gto_oracle as O  # noqa: F401  (tau estimator)
 
     rank, world, local = dist_env()
     if world > 1:
@@ -889,7 +1036,7 @@ def run_batched(a):
     for k, (n, s, W) in enumerate(zip(names, systems, Ws)):
         sm = sums_np[k]
         ser = sm[:, 3] / np.maximum(sm[:, 6], 1)
-        e_mean, e_serr, _, kappa = O.binning_analysis(ser)
+        e_mean, e_serr, _, kappa = binning_analysis(ser)
         acc = float(sm[:, 5].sum() / (K * W * s.n_e))
         share = busy[k] / tot_busy
         t_k = ms * share * 1e-3
@@ -966,7 +1113,6 @@ def run_learned(a):
     from omegaqmc_b200.context import GTOContext
     from omegaqmc_b200.learned import MLPProposal, collect_training_set, train_proposal
     from omegaqmc_b200.sampler import WalkerEnsemble, init_walkers_gaussian, NSUM
-    from oracle import gto_oracle as O  # noqa: F401  (tau estimator)
 
     rank, world, local = dist_env()
     if world > 1:
@@ -993,7 +1139,7 @@ def run_learned(a):
         torch.cuda.synchronize()
         sn = sums.cpu().numpy()
         ser = sn[:, 3] / np.maximum(sn[:, 6], 1)
-        m, se, _, kap = O.binning_analysis(ser)
+        m, se, _, kap = binning_analysis(ser)
         return (e0.elapsed_time(e1), m, se, kap, float(sn[:, 5].sum() / (n * W * system.n_e)))
 
     # training data and training (timed with events, outside the comparison)
@@ -1119,7 +1265,6 @@ def run_alle(a):
     from omegaqmc_b200 import replicas as RP
     from omegaqmc_b200.context import GTOContext
     from omegaqmc_b200.sampler import WalkerEnsemble, init_walkers_gaussian, NSUM
-    from oracle import gto_oracle as O  # noqa: F401  (tau estimator is the oracle's restatement)
 
     rank, world, local = dist_env()
     if world > 1:
@@ -1161,9 +1306,21 @@ def run_alle(a):
     ms_max = float(t[0])
     s_np = sums.cpu().numpy()
     series = s_np[:, 3] / np.maximum(s_np[:, 6], 1)
-    e_mean, e_serr, _, kappa = O.binning_analysis(series)
     acc = float(s_np[:, 5].sum() / (K * W * world * system.n_e))
     rate = W * world * K / (ms_max * 1e-3)
+    # tau_int from a series of at least 2,000 steps: the timed one when it is
+    # that long, else a separate untimed run continuing the chain
+    if K >= 2000:
+        tau_series, tau_src = series, f"timed series ({K} steps)"
+    else:
+        aux = torch.zeros(2000, NSUM, dtype=torch.float64, device=dev)
+        ens.run(2000, step, sums=aux)
+        if world > 1:
+            aux = RP.combine_sums(aux)
+        an = aux.cpu().numpy()
+        tau_series = an[:, 3] / np.maximum(an[:, 6], 1)
+        tau_src = "untimed 2000-step series"
+    e_mean, e_serr, _, kappa = binning_analysis(tau_series)
     if rank == 0:
         print(json.dumps({
             "metric": "decorrelated samples/s, all-electron steps (the reference's move) on the GPU",
@@ -1173,11 +1330,137 @@ def run_alle(a):
             "config": {"workload": f"{a.system} cc-pVDZ-shaped, {W} walkers/GPU, all-electron "
                                    "Gaussian steps, E_L every step, FP64",
                        "step": step, "parallelism": f"replicas x{world}"},
-            "walker_steps_per_s": rate, "tau_int": kappa, "acceptance": acc,
+            "walker_steps_per_s": rate, "tau_int": kappa, "tau_source": tau_src,
+            "acceptance": acc,
             "energy": {"mean": e_mean, "serr": e_serr}, "kernel_flags": ctx.flags(),
             "gpu_launches": n_launch, "roofline": None, "clocks": clk.summary()}), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+CONFIGS = {
+    # configuration 1: H2/STO-3G, RHF, Padé J2 b = 1, 1,024 walkers from
+    # N(nucleus, 0.5), fixed-width Gaussian step 0.3 bohr, 2,000 steps, FP64
+    "h2": {"system": "H2", "walkers": 1024, "sigma": 0.5, "sweeps": 2000,
+           "precisions": ("fp64",), "proposal": "plain", "step": 0.3, "j1": False},
+    # configuration 2: LiH cc-pVDZ-shaped, RHF, Padé J1 (a = -Z) + J2, 16,384
+    # walkers from N(nucleus, 1.0); FP64 against mixed with the same proposal
+    "lih": {"system": "LiH", "walkers": 16384, "sigma": 1.0, "sweeps": 2000,
+            "precisions": ("mixed", "fp64"), "proposal": "scaled", "step": 0.0, "j1": True},
+}
+
+
+def run_config(a):
+    """Configurations 1 (H2) and 2 (LiH) through the persistent path: per
+    precision, equilibration, then whole 50-sweep launches replayed from a
+    CUDA graph for the configuration's sweep count (repeated until at least
+    1 s is timed); tau_int from the timed series.  LiH adds the error of
+    every per-walker output of the mixed sampler against the FP64
+    evaluation on 4,096 fixed seeded configurations."""
+    import torch
+    from omegaqmc_b200 import _lib as L  # noqa: F401
+    from omegaqmc_b200 import molecules as M
+    from omegaqmc_b200.batch import BatchedSampler
+    from omegaqmc_b200.context import GTOContext
+    from omegaqmc_b200.sampler import init_walkers_gaussian
+    from omegaqmc_b200.system import build_system as bs
+
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    cf = CONFIGS[a.workload]
+    torch.cuda.set_device(local)
+    mf = M.make_mf(cf["system"])
+    system = bs(mf, M.default_params_corr(mf.mol, j1=cf["j1"]))
+    ctx = GTOContext(system)
+    ctx.specialize()
+    W, Kc = cf["walkers"], cf["sweeps"]
+    X0 = init_walkers_gaussian(system, W, cf["sigma"], seed=77)
+    stream = torch.cuda.current_stream()
+    arms = {}
+    launches = 0
+    clk_summary = None
+    for prec in cf["precisions"]:
+        b = BatchedSampler([ctx], [X0], [cf["step"] or 0.8], precision=prec,
+                           proposal=cf["proposal"], scale_r0=HEAD_R0, scale_fmin=HEAD_FMIN,
+                           cap=Kc)
+        if not cf["step"]:
+            b.adapt_steps(HEAD_ACC, seed=5)
+        b.reset(10**7)
+        for _ in range(max(a.warmup, 3) + 20):
+            b.run(REFRESH_EVERY, REFRESH_EVERY + 1, 9)
+        cfg, _ = b.tune(4, seed=6)
+        n_l = Kc // REFRESH_EVERY
+        b.capture(n_l, REFRESH_EVERY, 1, 9)
+        reps, total_ms, series = 0, 0.0, None
+        with ClockSampler(local) as clk:
+            while reps == 0 or (total_ms < 1000.0 and reps < 200):
+                b.reset(reps * Kc)
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                b.replay()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                total_ms += e0.elapsed_time(e1)
+                reps += 1
+                if series is None:
+                    sn = b.sums[0][:Kc].cpu().numpy()
+                    series = sn[:, 3] / np.maximum(sn[:, 6], 1)
+                    acc = float(sn[:, 5].sum() / (Kc * W * system.n_e))
+        launches += reps * n_l
+        clk_summary = clk.summary()
+        mean, serr, _, kappa = binning_analysis(series)
+        wss = W * Kc * reps / (total_ms * 1e-3)
+        arms[prec] = {"value": wss / kappa, "walker_sweeps_per_s": wss, "tau_int": kappa,
+                      "ms_per_step": total_ms / (Kc * reps), "timed_repeats": reps,
+                      "step": b.steps()[0], "acceptance": acc, "tile_shape": cfg,
+                      "energy": {"mean": mean, "serr": serr}, "kernel_flags": b.flags()}
+        b.close()
+        del b
+    main_prec = cf["precisions"][0]
+    m = arms[main_prec]
+    line = {
+        "metric": f"decorrelated samples/s (walker-steps/s / tau_int), {cf['system']} "
+                  f"{W} walkers",
+        "value": m["value"], "unit": "decorrelated samples/s", "n_gpus": 1, "steps": Kc,
+        "warmup": a.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if main_prec == "fp64" else "f32+f64", "data": "synthetic",
+        "config": {"workload": f"{a.workload}: {cf['system']} "
+                               f"{'STO-3G' if cf['system'] == 'H2' else 'cc-pVDZ-shaped'}, "
+                               f"RHF, Pade {'J1+J2' if cf['j1'] else 'J2'} (b=1), {W} walkers "
+                               f"from N(nucleus, {cf['sigma']}), {Kc} single-electron sweeps "
+                               "with E_L every sweep per timed repeat",
+                   "proposal": ("fixed-width Gaussian" if cf["proposal"] == "plain" else
+                                f"nucleus-scaled Gaussian (r0={HEAD_R0}, fmin={HEAD_FMIN})"),
+                   "precision": main_prec},
+        "tau_int": m["tau_int"], "energy": m["energy"], "acceptance": m["acceptance"],
+        "walker_sweeps_per_s": m["walker_sweeps_per_s"], "arms": arms,
+        "gpu_launches": launches, "roofline": None, "clocks": clk_summary}
+    if "fp64" in arms and main_prec != "fp64":
+        f = arms["fp64"]
+        line["mixed_vs_fp64"] = m["value"] / f["value"]
+        line["energy_diff_sigma"] = abs(m["energy"]["mean"] - f["energy"]["mean"]) / max(
+            np.hypot(m["energy"]["serr"], f["energy"]["serr"]), 1e-300)
+        Xf = torch.tensor(init_walkers_gaussian(system, 4096, cf["sigma"], seed=2024),
+                          dtype=torch.float64, device="cuda")
+        ctx.set_proposal(1, HEAD_R0, HEAD_FMIN)
+        line["outputs_vs_fp64"] = output_errors(ctx, Xf, main_prec, m["step"], 11)
+        ctx.set_proposal(0)
+    if not a.no_cpu:
+        cores = len(os.sched_getaffinity(0))
+        r, kap, acc_c, sample, ser = cpu_reference(system, a.cpu_seconds, cores,
+                                                   cf["step"] or (3 * 0.1) ** 0.5)
+        cm, cse, _, _ = binning_analysis(ser)
+        line["cpu_baseline"] = {"value": r / kap, "unit": "decorrelated samples/s",
+                                "cores": cores, "kind": "port", "sample": sample,
+                                "walker_steps_per_s": r, "tau_int": kap,
+                                "energy": {"mean": cm, "serr": cse}}
+        line["energy_vs_cpu_reference_sigma"] = abs(m["energy"]["mean"] - cm) / max(
+            np.hypot(m["energy"]["serr"], cse), 1e-300)
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -1186,6 +1469,8 @@ def main():
         run_reference(a)
     elif a.workload == "alle":
         run_alle(a)
+    elif a.workload in CONFIGS:
+        run_config(a)
     elif a.workload == "batched":
         run_batched(a)
     elif a.workload == "learned":
