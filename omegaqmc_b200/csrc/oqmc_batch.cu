@@ -98,13 +98,12 @@ std::string kernel_name(int precision, int v) {
          std::to_string(kVariants[v].minb) + ">";
 }
 
-// Shared memory of one tile (matches the carve-up in oq_batch_tile): the
-// reduction buffer only when several threads share a walker, then positions
-// and inverses.
+// Shared memory of one tile (matches the carve-up in oq_batch_tile):
+// positions and inverses (nt only sets the lanes per walker).
 size_t tile_smem(int nocc, int wt, int nt, int precision) {
+  (void)nt;
   const size_t real = precision == OQ_PREC_MIXED ? 4 : 8;
-  return (nt > wt ? (size_t)4 * nt * 8 : 0) + (size_t)6 * nocc * wt * 8 +
-         (size_t)2 * nocc * nocc * wt * real;
+  return (size_t)6 * nocc * wt * 8 + (size_t)2 * nocc * nocc * wt * real;
 }
 
 }  // namespace
