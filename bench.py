@@ -1130,11 +1130,14 @@ def run_learned(a):
     stream = torch.cuda.current_stream()
 
     def timed(e, n):
+        return timed_step(e, n, step)
+
+    def timed_step(e, n, stp):
         sums = torch.zeros(n, NSUM, dtype=torch.float64, device=dev)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        e.run(n, step, sums=sums)
+        e.run(n, stp, sums=sums)
         e1.record(stream)
         torch.cuda.synchronize()
         sn = sums.cpu().numpy()
@@ -1178,6 +1181,17 @@ def run_learned(a):
         torch.cuda.nvtx.range_pop()
     flags = (ctx.flags(), mlp.flags())
     ctx.set_mlp_proposal(None)
+    # the hand-built alternative at the same GPU time: the nucleus-scaled
+    # Gaussian (the headline's proposal), its width adapted to acceptance 0.5
+    sens = WalkerEnsemble(ctx, lens.X, "mixed", seed=77 + rank, refresh_every=REFRESH_EVERY)
+    ctx.set_proposal(1, HEAD_R0, HEAD_FMIN)
+    sstep = adapt_step(sens, 0.8, target=HEAD_ACC)
+    sens.run(500, sstep)
+    sprobe = timed_step(sens, 20, sstep)[0] / 20
+    K_s = max(200, int(ms_p / sprobe))
+    ms_s, e_s, se_s, tau_s, acc_s = timed_step(sens, K_s, sstep)
+    ctx.set_proposal(0)
+    del sens
     t = torch.tensor([ms_l, ms_p], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -1216,6 +1230,10 @@ def run_learned(a):
         "plain_random_walk": {"value": plain, "tau_int": tau_p, "acceptance": acc_p,
                               "energy": {"mean": e_p, "serr": se_p}, "step": step,
                               "ms_per_sweep": ms_p / K_p, "walker_sweeps_per_s": wss_p},
+        "nucleus_scaled": {"value": W * world * K_s / (ms_s * 1e-3) / tau_s, "tau_int": tau_s,
+                           "acceptance": acc_s, "energy": {"mean": e_s, "serr": se_s},
+                           "step": sstep, "ms_per_sweep": ms_s / K_s, "sweeps": K_s},
+        "gain_vs_scaled_equal_time": value / (W * world * K_s / (ms_s * 1e-3) / tau_s),
         "gain_equal_time": value / plain, "gain_per_sweep": tau_p / tau_l,
         "energy_diff_sigma": abs(e_l - e_p) / max(np.hypot(se_l, se_p), 1e-300),
         "training": {"collect_ms": collect_ms, "train_ms": train_ms, "loss": hist,

@@ -1256,7 +1256,7 @@ static int launch_moves(oqmc_ctx* ctx, const OqMoveArgs& m, int wpb, size_t sm, 
     void* args[5] = {(void*)&L.sys, (void*)&L.split, (void*)&C, (void*)&mm, (void*)&nw};
     const int G = ctx->mlp_groups == 4 ? 4 : 2;
     if (oq_rtc_launch(ctx->mlp_fn[G == 4 ? 1 : 0], dim3((m.W + 128 * G - 1) / (128 * G)),
-                      dim3(128 * G), oq_mlp_sweep_smem(G), L.stream, args) != 0)
+                      dim3(128 * G), oq_mlp_sweep_smem(G, ctx->n_e), L.stream, args) != 0)
       return set_err(ctx, OQ_ERR_CUDA, "learned-proposal move kernel launch failed%s");
     return OQ_OK;
   }

@@ -29,9 +29,23 @@
 #define OQ_MLPS_ACT 3072
 #define OQ_MLPS_MAXG 4
 
-// Shared memory of k_moves_mlp with G walker groups.
-__host__ __device__ constexpr size_t oq_mlp_sweep_smem(int groups) {
+// Shared memory of k_moves_mlp with G walker groups of ne-electron walkers:
+// header, the groups' activation tiles and the weights, plus, where it fits
+// in a CTA's 227 KB, an FP32 copy of each group's walker positions
+// ([3 ne][128] floats per group) that the features read instead of the
+// FP64 state in global memory.
+__host__ __device__ constexpr size_t oq_mlp_sweep_base(int groups) {
   return (size_t)OQ_MLPS_ACT + (size_t)groups * OQ_MLP_SM_ACT + OQ_MLP_SM_WEIGHTS;
+}
+__host__ __device__ constexpr size_t oq_mlp_posf_bytes(int groups, int ne) {
+  return (size_t)groups * 3 * ne * 128 * sizeof(float);
+}
+__host__ __device__ constexpr bool oq_mlp_posf_fits(int groups, int ne) {
+  return oq_mlp_sweep_base(groups) + oq_mlp_posf_bytes(groups, ne) <= (size_t)227 * 1024;
+}
+__host__ __device__ constexpr size_t oq_mlp_sweep_smem(int groups, int ne) {
+  return oq_mlp_sweep_base(groups) + (oq_mlp_posf_fits(groups, ne) ? oq_mlp_posf_bytes(groups, ne)
+                                                                    : 0);
 }
 
 struct OqMlpWeights {
@@ -97,11 +111,14 @@ k_moves_mlp(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gspli
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + OQ_MLPS_BAR);     // [G]
   uint32_t* slot = reinterpret_cast<uint32_t*>(smem + OQ_MLPS_BAR + 8 * OQ_MLPS_MAXG);
   unsigned char* wreg = smem + OQ_MLPS_ACT + G * OQ_MLP_SM_ACT;
+  constexpr bool POSF = oq_mlp_posf_fits(G, NE);
   const OqSystem& S = *gsys;
   const OqSplit& SP = *gsplit;
   const float* C = reinterpret_cast<const float*>(gC);
   const int g = threadIdx.x >> 7, r = threadIdx.x & 127, warp = threadIdx.x >> 5;
   unsigned char* act = smem + OQ_MLPS_ACT + g * OQ_MLP_SM_ACT;
+  // FP32 copy of the group's positions, [3 NE][128]: row r's walker only
+  float* posf = reinterpret_cast<float*>(smem + oq_mlp_sweep_base(G)) + (size_t)g * 3 * NE * 128;
   const int W = a.W;
   const int w = (blockIdx.x * G + g) * 128 + r;
   const bool live = w < W;
@@ -126,6 +143,12 @@ k_moves_mlp(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gspli
   int nacc = 0;
   bool ok = true;
   auto P = [&](int j, int c) { return pos[(size_t)(3 * j + c) * W + wr]; };
+  // the features read the other electrons from the FP32 copy where it fits
+  // (a fixed function of the state, so the proposal density of every state
+  // is well defined and the Metropolis-Hastings ratio stays exact)
+  auto PF = [&](int j, int c) { return (double)posf[(3 * j + c) * 128 + r]; };
+  if (POSF)
+    for (int k = 0; k < 3 * NE; ++k) posf[k * 128 + r] = (float)pos[(size_t)k * W + wr];
   for (int t = 0; t < a.n_steps && ok; ++t) {
     const uint32_t gstep = (uint32_t)(a.step_base + t);
     for (int e = 0; e < NE; ++e) {
@@ -136,7 +159,8 @@ k_moves_mlp(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gspli
       const float uc = ((float)rc.x + 0.5f) * 2.3283064365386963e-10f;
       const double ox = P(e, 0), oy = P(e, 1), oz = P(e, 2);
       float f[OQ_MLP_K0], out[OQ_MLP_NOUT];
-      oq_mlp_features_ne<NE>(J, P, e, ox, oy, oz, f);
+      if (POSF) oq_mlp_features_ne<NE>(J, PF, e, ox, oy, oz, f);
+      else oq_mlp_features_ne<NE>(J, P, e, ox, oy, oz, f);
       oq_mlp_store_features(act, r, f);
       ok = oq_mlp_forward_group(act, wreg, bias, tmem, bar, phase, r, bar_id, out);
       if (!ok) break;
@@ -144,14 +168,23 @@ k_moves_mlp(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gspli
       oq_mix_sample_f(out, uc, n3, d);
       const float lqf = oq_mix_logq_f(out, (float)d[0], (float)d[1], (float)d[2]);
       const double nx = ox + d[0], ny = oy + d[1], nz = oz + d[2];
-      oq_mlp_features_ne<NE>(J, P, e, nx, ny, nz, f);
+      if (POSF) oq_mlp_features_ne<NE>(J, PF, e, nx, ny, nz, f);
+      else oq_mlp_features_ne<NE>(J, P, e, nx, ny, nz, f);
       oq_mlp_store_features(act, r, f);
       ok = oq_mlp_forward_group(act, wreg, bias, tmem, bar, phase, r, bar_id, out);
       if (!ok) break;
       const float lqr = oq_mix_logq_f(out, (float)(ox - nx), (float)(oy - ny), (float)(oz - nz));
-      if (live)
-        nacc += oq_try_move<NOCC, float, float, B>(J, S, SP, C, pos, Ai, W, w, e, nx, ny, nz,
-                                                   (double)(lqr - lqf), 1.0, u, logdet);
+      if (live) {
+        const bool acc = oq_try_move<NOCC, float, float, B>(J, S, SP, C, pos, Ai, W, w, e, nx,
+                                                            ny, nz, (double)(lqr - lqf), 1.0, u,
+                                                            logdet);
+        nacc += acc;
+        if (POSF && acc) {
+          posf[(3 * e) * 128 + r] = (float)nx;
+          posf[(3 * e + 1) * 128 + r] = (float)ny;
+          posf[(3 * e + 2) * 128 + r] = (float)nz;
+        }
+      }
     }
   }
   if (live) a.logdet[w] = logdet;
