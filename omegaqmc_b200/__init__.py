@@ -35,7 +35,7 @@ def __getattr__(name):
 
 
 def generate_molecular_orbitals(astr, units="Bohr", basis="cc-pvdz-shaped", spin=0,
-                                charge=0, ao_splines=None, **kw):
+                                charge=0, ao_splines=None, symmetrization_level=1, **kw):
     """RHF mean-field object for ``astr`` (``OmegaQMC/vmc_gto.py:217-452`` runs
     PySCF; here the package's own RHF).  ``basis`` is a PySCF-format dict
     ``{element: [[am, [alpha, c...], ...], ...]}``, basis-set text in NWChem
@@ -44,7 +44,11 @@ def generate_molecular_orbitals(astr, units="Bohr", basis="cc-pvdz-shaped", spin
     ``"cc-pvdz-shaped"`` / ``"sto-3g"`` (H only).  ``ao_splines``
     (True or a dict of grid options) switches on the quintic radial-spline
     AO transform, stored on ``mf.mol.ao_radial_transform`` as in the
-    reference (``vmc_gto.py:278-290, 415``)."""
+    reference (``vmc_gto.py:278-290, 415``).  With ``symmetrization_level``
+    >= 1 (the reference's default) a molecule without point-group symmetry
+    is moved to the reference's canonical frame (centre of nuclear charge,
+    charge-inertia principal axes; :mod:`omegaqmc_b200.frame`); molecules
+    with symmetry keep their input frame."""
     from . import molecules as M
     from .rhf import run_rhf
     if spin != 0:
@@ -66,5 +70,10 @@ def generate_molecular_orbitals(astr, units="Bohr", basis="cc-pvdz-shaped", spin
     elif isinstance(basis, dict) and any(isinstance(v, str) for v in basis.values()):
         basis = load_basis(basis, syms)
     mol = Mole(astr, basis, unit=units, charge=charge, basis_name="gen")
+    if symmetrization_level >= 1:
+        from .frame import canonical_coordinates
+        xyz = canonical_coordinates(mol.atom_coords(), mol.atom_charges())
+        mol = Mole([(a, tuple(c)) for (a, _), c in zip(mol._atom, xyz)], basis, unit="Bohr",
+                   charge=charge, basis_name="gen")
     mol.ao_radial_transform = ao_splines
     return run_rhf(mol, **kw)

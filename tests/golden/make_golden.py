@@ -90,6 +90,48 @@ def load_reference():
     return gto, shell, utils
 
 
+def load_point_groups():
+    """The reference's OmegaQMC/symm/point_groups.py (numpy only)."""
+    symm = types.ModuleType("OmegaQMC.symm")
+    symm.__path__ = [os.path.join(REF, "OmegaQMC", "symm")]
+    sys.modules["OmegaQMC.symm"] = symm
+    return importlib.import_module("OmegaQMC.symm.point_groups")
+
+
+# geometries (bohr) and charges for the canonical-frame fixture: asymmetric
+# molecules, one already near its frame, one with a planar fragment, and a
+# degenerate (linear) case
+FRAME_CASES = [
+    ([[0.1, -0.3, 0.2], [1.9, 0.4, -0.5], [-0.7, 1.6, 0.9], [0.3, -1.2, 2.4]], [8, 1, 9, 1]),
+    ([[0.0, 0.0, 0.0], [2.1, 0.3, 0.0], [-0.6, 1.9, 0.4]], [6, 1, 8]),
+    ([[1.0, 2.0, 3.0], [3.2, 2.4, 2.1], [0.2, 4.1, 3.3], [1.5, 0.2, 4.4], [2.5, 3.5, 0.9]],
+     [6, 1, 1, 9, 17]),
+    ([[0.0, 0.0, 0.0], [0.0, 0.0, 2.0], [0.0, 0.0, -3.1]], [1, 6, 7]),
+]
+
+
+def frame_fixture(pg):
+    """Reference outputs of charge_inertia_axes for FRAME_CASES, each
+    geometry also rotated and shifted."""
+    rng = np.random.default_rng(5)
+    out = {}
+    for k, (xyz, q) in enumerate(FRAME_CASES):
+        xyz = np.array(xyz, dtype=float)
+        A = np.linalg.qr(rng.normal(size=(3, 3)))[0]
+        if np.linalg.det(A) < 0:
+            A[:, 0] *= -1
+        for tag, c in (("a", xyz), ("b", xyz @ A.T + rng.normal(size=3))):
+            r = pg.charge_inertia_axes(c, np.array(q))
+            out[f"coords_{k}{tag}"] = c
+            out[f"charges_{k}{tag}"] = np.array(q)
+            if r is None:
+                out[f"none_{k}{tag}"] = np.array(1)
+            else:
+                out[f"centre_{k}{tag}"] = np.asarray(r[0])
+                out[f"axes_{k}{tag}"] = np.asarray(r[1])
+    return out
+
+
 class _RefMole:
     """Adapter exposing this package's Mole with tensor charges."""
 
@@ -485,6 +527,10 @@ def main():
     if args.verify:
         print(f"worst {worst:.3e}")
         return
+    if args.cases is None or "frame" in args.cases:
+        np.savez_compressed(os.path.join(HERE, "golden_frame.npz"),
+                            **frame_fixture(load_point_groups()))
+        print("frame fixture:", len(FRAME_CASES), "geometries")
     if args.cases is None or "eeI_map" in args.cases:
         maps = {}
         for n_ei, n_ee, rc in EEI_MAPS:

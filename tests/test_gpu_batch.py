@@ -55,12 +55,18 @@ def _per_system(ctx, X0, precision, prop, step, n_sweeps, me, seed, step_base):
     return X, sums
 
 
+# (threads per CTA, walkers per tile): lanes per walker threads / walkers,
+# (1, 2, 4) and (8, 4, 1) for H2, LiH, H2O
+SHAPES = [(128, [128, 64, 32]), (256, [32, 64, 256])]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
-def test_batch_reproduces_per_system_path(contexts, precision):
+def test_batch_reproduces_per_system_path(contexts, precision, shape):
     X0 = _walkers(contexts)
     b = BatchedSampler(contexts, [x.clone() for x in X0], STEPS, precision=precision,
                        proposal=PROPS, cap=16)
-    b.configure(128, [128, 64, 32], variant=0)
+    b.configure(shape[0], shape[1], variant=0)
     n, me, seed, base = 20, 5, 1234, 100
     b.reset(base)
     b.run(n, me, seed)
