@@ -4,6 +4,8 @@ region and reports every throttle reason seen there (no GPU needed)."""
 import os
 import sys
 
+import pytest
+
 sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 import bench  # noqa: E402
 
@@ -51,3 +53,26 @@ def test_sweep_launch_count_follows_the_ensemble_chunking():
     # measurements every 4 sweeps: a 48-sweep call (12 measurements), then 2
     # sweeps with no measurement still take a move kernel, then the refresh
     assert bench.sweep_launches(_Ens(0), 50, measure_every=4) == (2 + 24) + (2 + 0 + 1) + 2
+
+
+def test_kappa_spread_of_segments():
+    """tau_int's stated uncertainty: kappa of each consecutive segment, their
+    mean and standard error."""
+    import numpy as np
+    rng = np.random.default_rng(3)
+    x = np.zeros(40000)
+    for i in range(1, x.size):
+        x[i] = 0.6 * x[i - 1] + rng.standard_normal()
+    k = bench.kappa_spread(x, 4)
+    assert k["segments"] == 4 and k["segment_sweeps"] == 10000 and len(k["kappas"]) == 4
+    # AR(1) with phi = 0.6: tau_int = (1 + phi) / (1 - phi) = 4
+    assert abs(k["mean"] - 4.0) < 0.5 and 0 < k["serr"] < 0.5
+    assert bench.binning_analysis(x)[3] == pytest.approx(k["mean"], rel=0.2)
+
+
+def test_headline_config_constants():
+    # the timed region is long enough for the clock record and fits the sums buffer
+    assert bench.MIN_TIMED_S >= 2.0
+    assert bench.MAX_TIMED_SWEEPS % bench.REFRESH_EVERY == 0
+    assert bench.PLAIN_SEGS * bench.PLAIN_SEG >= 50000
+    assert set(bench.CONFIGS) == {"h2", "lih"}
