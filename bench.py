@@ -61,10 +61,15 @@ HEAD_R0, HEAD_FMIN, HEAD_ACC = 1.0, 0.02, 0.5
 # the headline's timed region lasts at least this long (s); its sweep count
 # is capped by the measurement buffer
 MIN_TIMED_S = 2.0
+# chunks of the end-to-end leg's overlapped walker copies
+E2E_CHUNKS = 4
 MAX_TIMED_SWEEPS = 60000
 # the plain FP64 sampler's tau_int (several hundred sweeps) comes from this
 # many consecutive segments of PLAIN_SEG sweeps: their kappas give the spread
 PLAIN_SEGS, PLAIN_SEG = 4, 12500
+# and is cross-checked on PLAIN_TRACE_W walkers' own E_L series of
+# PLAIN_TRACE_SWEEPS sweeps
+PLAIN_TRACE_W, PLAIN_TRACE_SWEEPS = 1024, 20000
 
 
 def parse():
@@ -250,6 +255,28 @@ def output_errors(ctx, X, precision, step, seed):
         out[f"after_{sweeps}_sweeps"] = st
         del ens
     return out
+
+
+def walker_series_kappa(ctx, X, step, seed, sweeps=None):
+    """Cross-check of a long tau_int: kappa of the reference's estimator on
+    each walker's own E_L series (W walkers, the given sweeps, FP64, the
+    context's proposal), averaged over the walkers with its standard error.
+    Walkers are independent, so each series has the tau_int of the
+    walker-mean series; the average of many short-series estimates is far
+    less noisy than one estimate on the mean series."""
+    import torch
+    from omegaqmc_b200.sampler import NSUM, WalkerEnsemble
+    sweeps = sweeps or PLAIN_TRACE_SWEEPS
+    W = int(X.shape[0])
+    ens = WalkerEnsemble(ctx, X, "fp64", seed=seed)
+    trace = torch.empty(sweeps, W, dtype=torch.float64, device=X.device)
+    sums = torch.zeros(sweeps, NSUM, dtype=torch.float64, device=X.device)
+    ens.run(sweeps, step, sums=sums, el_trace=trace)
+    tr = trace.cpu().numpy()
+    ks = np.array([binning_analysis(tr[:, w])[3] for w in range(W)])
+    del ens, trace
+    return {"walkers": W, "sweeps": sweeps, "mean": float(ks.mean()),
+            "serr": float(ks.std(ddof=1) / np.sqrt(W)), "median": float(np.median(ks))}
 
 
 def kappa_spread(series, parts):
@@ -699,7 +726,9 @@ def run_persistent(a):
                  "proposal": "fixed-width Gaussian", "step": pstep, "precision": "fp64",
                  "ms_per_step": pms / Kp, "steps": Kp, "path": "same persistent kernel, FP64",
                  "energy": {"mean": pm, "serr": pse},
-                 "energy_diff_sigma": abs(pm - e_mean) / max(np.hypot(pse, e_serr), 1e-300)}
+                 "energy_diff_sigma": abs(pm - e_mean) / max(np.hypot(pse, e_serr), 1e-300),
+                 "tau_int_walker_series": walker_series_kappa(
+                     ctx, pb.walkers[0][:PLAIN_TRACE_W], pstep, seed ^ 12)}
         del pb
         # FP64 with the headline's proposal: separates the precision factor
         # (mixed vs FP64, same proposal) from the proposal factor (scaled vs
@@ -786,19 +815,42 @@ def run_persistent(a):
         # host buffers through the public API: each call = 50 sweeps; the
         # walkers go host -> device before and device -> host after every
         # call, with the call's measurement sums
+        # The copies run in E2E_CHUNKS chunks on two copy streams, so that the
+        # device -> host copy of one chunk of a call's result overlaps the
+        # host -> device copy of the previous chunk for the next call (the
+        # two directions of the link run at once); each chunk still goes to
+        # host memory and back, and every call's kernel waits for all of its
+        # input
         Ke = min(n_launch, 10)
         hostX = b.walkers[0].detach().to("cpu").pin_memory()
         hsum = torch.empty(REFRESH_EVERY, NSUM, dtype=torch.float64).pin_memory()
+        dX, hX = b.walkers[0].view(-1), hostX.view(-1)
+        bounds = np.linspace(0, dX.numel(), E2E_CHUNKS + 1).astype(int)
+        s_out, s_in = torch.cuda.Stream(), torch.cuda.Stream()
         b.reset(E2E)
         torch.cuda.synchronize()
         f0 = torch.cuda.Event(enable_timing=True)
         f1 = torch.cuda.Event(enable_timing=True)
         f0.record(stream)
+        s_in.wait_stream(stream)
+        with torch.cuda.stream(s_in):
+            dX.copy_(hX, non_blocking=True)
         for r in range(Ke):
-            b.walkers[0].copy_(hostX, non_blocking=True)
+            stream.wait_stream(s_in)
             b.run(REFRESH_EVERY, 1, seed)
-            hostX.copy_(b.walkers[0], non_blocking=True)
-            hsum.copy_(b.sums[0][r * REFRESH_EVERY:(r + 1) * REFRESH_EVERY], non_blocking=True)
+            s_out.wait_stream(stream)
+            for c in range(E2E_CHUNKS):
+                lo, hi = bounds[c], bounds[c + 1]
+                with torch.cuda.stream(s_out):
+                    hX[lo:hi].copy_(dX[lo:hi], non_blocking=True)
+                    if c == E2E_CHUNKS - 1:
+                        hsum.copy_(b.sums[0][r * REFRESH_EVERY:(r + 1) * REFRESH_EVERY],
+                                   non_blocking=True)
+                if r + 1 < Ke:
+                    s_in.wait_stream(s_out)
+                    with torch.cuda.stream(s_in):
+                        dX[lo:hi].copy_(hX[lo:hi], non_blocking=True)
+        stream.wait_stream(s_out)
         f1.record(stream)
         torch.cuda.synchronize()
         bi = b.walkers[0].numel() * 8
@@ -865,6 +917,10 @@ def run_persistent(a):
                    plain["tau_int_segments"]["serr"])
         line["speedup_vs_plain_fp64"] = sp["value"]
         line["speedup_vs_plain_fp64_serr"] = sp["serr"]
+        wk = plain["tau_int_walker_series"]
+        line["speedup_vs_plain_fp64_walker_tau"] = ratio(
+            value, kappa, kq["serr"], plain["walker_sweeps_per_s"] / wk["mean"], wk["mean"],
+            wk["serr"])
         if fp64s:
             line["fp64_same_proposal"] = fp64s
             line["mixed_vs_fp64_same_proposal"] = ratio(

@@ -133,3 +133,24 @@ def test_md_optimiser_inputs_match_oracle():
     assert np.max(np.abs(de - ref_de) / (np.abs(ref_de).max(axis=0) + 1.0)) < 1e-9
     ref_e = O.evaluate(s, X)["e_loc"]
     assert np.max(np.abs(e - ref_e)) / (0.5 * np.abs(ref_e).max() + 1.0) < 1e-9
+
+
+def test_md_state_evaluate_matches_oracle():
+    """oqmc_state_eval on a multi-determinant sampler state: log|psi| (tracked
+    determinant sum + Jastrow), gradient, Laplacian and E_L as the oracle
+    evaluates them at the same positions, fresh and after 20 sweeps of
+    per-determinant Sherman-Morrison updates."""
+    s, _ = golden_system("h2o_md")
+    ctx = GTOContext(s)
+    W = 256
+    ens = WalkerEnsemble(ctx, seeded_walkers(s, W, 0.9, 5), "fp64", seed=3, refresh_every=10**9)
+    for sweeps, tol in ((0, 1e-10), (20, 1e-8)):
+        if sweeps:
+            ens.run(sweeps, 0.4)
+        out = {k: v.cpu().numpy() for k, v in ens.state_evaluate().items()}
+        ref = O.evaluate(s, ens.X.cpu().numpy())
+        sc = 0.5 * (np.sum(np.abs(ref["lap"]), axis=1) + np.sum(ref["grad"] ** 2, axis=(1, 2))) + 1
+        assert np.max(np.abs(out["logpsi"] - ref["logpsi"]) / (np.abs(ref["logpsi"]) + 1)) < tol
+        assert np.max(np.abs(out["grad"] - ref["grad"]) / (np.abs(ref["grad"]) + 1)) < tol
+        assert np.max(np.abs(out["e_loc"] - ref["e_loc"]) / sc) < tol
+    assert ctx.flags() == 0
