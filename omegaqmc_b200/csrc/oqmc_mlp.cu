@@ -257,26 +257,31 @@ k_mlp_forward(const unsigned short* __restrict__ feat, int R,
   const int t = threadIdx.x, warp = t >> 5;
   const int row = blockIdx.x * 128 + t;
   const bool valid = row < R;
-  if (warp == 0) oq_tmem_alloc(slot, 128);
+  (void)act;
+  // TMEM: accumulator in columns [0, 128), BF16 activations in [128, 192)
+  if (warp == 0) oq_tmem_alloc(slot, 256);
   if (t == 0) oq_mbar_init(bar, 1);
-  {
-    uint4 q[4] = {};
-    if (valid) {
-      const uint4* s = reinterpret_cast<const uint4*>(feat + (size_t)row * OQ_MLP_K0);
-      for (int k = 0; k < 4; ++k) q[k] = s[k];
-    }
-    for (int c = 0; c < 4; ++c)
-      *reinterpret_cast<uint4*>(act + (((t >> 3) * 4 + c) << 7) + ((t & 7) << 4)) = q[c];
-  }
   oq_mlp_load_weights(wreg, wbf);
   oq_mlp_load_bias(bias, theta);
   oq_tc_fence_before();
   __syncthreads();
   oq_tc_fence_after();
   const uint32_t tmem = *slot;
+  {
+    uint32_t f2[16] = {};
+    if (valid) {
+      const uint4* s = reinterpret_cast<const uint4*>(feat + (size_t)row * OQ_MLP_K0);
+      for (int k = 0; k < 4; ++k) {
+        const uint4 q = s[k];
+        f2[4 * k] = q.x; f2[4 * k + 1] = q.y; f2[4 * k + 2] = q.z; f2[4 * k + 3] = q.w;
+      }
+    }
+    oq_mlp_store_features_ta(tmem + ((uint32_t)((t >> 5) * 32) << 16), f2);
+    oq_tmem_wait_st();
+  }
   OqMlpSync sy{bar, 0u};
   float out[OQ_MLP_NOUT];
-  const bool ok = oq_mlp_forward_tile(act, wreg, bias, tmem, sy, out, nullptr, nullptr);
+  const bool ok = oq_mlp_forward_tile_ta(wreg, bias, tmem, sy, out);
   if (ok && valid)
     for (int j = 0; j < OQ_MLP_NOUT; ++j) out_g[(size_t)row * OQ_MLP_NOUT + j] = out[j];
   oq_tc_fence_before();
@@ -284,7 +289,7 @@ k_mlp_forward(const unsigned short* __restrict__ feat, int R,
   if (warp == 0) {
     oq_tc_fence_after();
     if (!ok) oq_mbar_wait(bar, sy.phase ^ 1u);
-    oq_tmem_dealloc(tmem, 128);
+    oq_tmem_dealloc(tmem, 256);
   }
   if (!ok && t == 0) atomicOr(flags, OQ_FLAG_TIMEOUT);
 }

@@ -224,6 +224,89 @@ __device__ __forceinline__ bool oq_mlp_forward_tile(unsigned char* act, const un
 }
 
 // ---------------------------------------------------------------------------
+// Forward pass with the activations in tensor memory.  Each group of 128
+// rows owns 192 TMEM columns from `tmem`: the FP32 accumulator D in
+// columns [0, 128) and the BF16 A operand (the layer input, two elements per
+// column) in [128, 192).  Thread r writes its row's features, and after each
+// hidden layer its ReLU outputs, into its own lane of the A columns with
+// tcgen05.st, so no activation tile sits in shared memory and the MMA reads
+// A straight from TMEM.
+#define OQ_MLP_TA_COL 128u
+
+__device__ __forceinline__ void oq_mlp_mma_ta(uint32_t tmem_d, uint32_t tmem_a,
+                                              const unsigned char* Bm, int N, int K,
+                                              uint64_t* bar) {
+  const uint32_t b0 = oq_smem_addr(Bm);
+  const uint32_t sbo = (uint32_t)(K / 8) * 128u;
+  const uint32_t idesc = oq_idesc_bf16(128, N);
+  for (int ks = 0; ks < K / 16; ++ks) {
+    const uint64_t bd = oq_desc_kmajor(b0 + (uint32_t)ks * 256u, 128u, sbo);
+    oq_mma_bf16_ta(tmem_d, tmem_a + (uint32_t)ks * 8u, bd, idesc, ks > 0 ? 1u : 0u);
+  }
+  if (bar) oq_mma_commit(bar);
+}
+
+// Row r's 32 BF16 features (16 packed words, the lower half the even
+// feature) into its lane of the A columns.
+__device__ __forceinline__ void oq_mlp_store_features_ta(uint32_t trow, const uint32_t f2[16]) {
+  oq_tmem_st16(trow + OQ_MLP_TA_COL, f2);
+}
+
+// Hidden-layer epilogue into the A columns: D + bias, ReLU, BF16 pairs.
+__device__ __forceinline__ void oq_mlp_hidden_epilogue_ta(uint32_t trow, const float* bias) {
+#pragma unroll 1
+  for (int h0 = 0; h0 < OQ_MLP_H; h0 += 64) {
+    uint32_t raw[64];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) oq_tmem_ld16_nw(trow + (uint32_t)(h0 + 16 * q), raw + 16 * q);
+    oq_tmem_wait_ld();
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      uint32_t pk[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int c = h0 + 32 * q + 2 * j;
+        float z0 = __uint_as_float(raw[32 * q + 2 * j]) + bias[c];
+        float z1 = __uint_as_float(raw[32 * q + 2 * j + 1]) + bias[c + 1];
+        z0 = z0 > 0.0f ? z0 : 0.0f;
+        z1 = z1 > 0.0f ? z1 : 0.0f;
+        pk[j] = oq_bf16x2(z0, z1);
+      }
+      oq_tmem_st16(trow + OQ_MLP_TA_COL + (uint32_t)((h0 + 32 * q) >> 1), pk);
+    }
+  }
+  oq_tmem_wait_st();
+}
+
+// Forward pass of a 128-thread CTA's 128 rows with the activations in TMEM
+// (features already stored in the A columns, oq_tmem_wait_st done); leaves
+// row r's 48 outputs in `out` of thread r.  Returns false when an MMA wait
+// timed out (uniform over the CTA).
+__device__ __forceinline__ bool oq_mlp_forward_tile_ta(const unsigned char* wreg,
+                                                       const float* bias, uint32_t tmem,
+                                                       OqMlpSync& sy, float out[OQ_MLP_NOUT]) {
+  const int r = threadIdx.x & 127;
+  const uint32_t trow = tmem + ((uint32_t)((r >> 5) * 32) << 16);
+  const unsigned char* W[4] = {wreg, wreg + OQ_MLP_SM_W1, wreg + OQ_MLP_SM_W1 + OQ_MLP_SM_WH,
+                               wreg + OQ_MLP_SM_W1 + 2 * OQ_MLP_SM_WH};
+  for (int l = 0; l < 4; ++l) {
+    oq_tc_fence_before();
+    __syncthreads();
+    oq_tc_fence_after();
+    if (threadIdx.x == 0)
+      oq_mlp_mma_ta(tmem, tmem + OQ_MLP_TA_COL, W[l], l == 3 ? OQ_MLP_NOUT : OQ_MLP_H,
+                    l == 0 ? OQ_MLP_K0 : OQ_MLP_H, sy.bar);
+    if (!oq_mlp_wait(sy)) return false;
+    if (l < 3)
+      oq_mlp_hidden_epilogue_ta(trow, bias + l * OQ_MLP_H);
+    else
+      oq_mlp_out_epilogue(trow, bias + 3 * OQ_MLP_H, out);
+  }
+  oq_tc_fence_before();
+  return true;
+}
+
+// ---------------------------------------------------------------------------
 // Mixture density (double precision on the FP32 network outputs)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double oq_softplus(double x) {

@@ -538,7 +538,9 @@ __device__ __forceinline__ T oq_jastrow_delta(const SJ& J, const OqSystem& S, co
 }
 
 // One single-electron Metropolis move of electron e to (nx, ny, nz) against
-// shared-memory state; the proposal-density ratio q(old)/q(new) is
+// one walker's state: its positions pos[(3 j + c) ps] and its inverse
+// matrices A[k as] (either in shared or in global memory); the
+// proposal-density ratio q(old)/q(new) is
 // mul_extra * exp(log_extra) (1 for symmetric proposals).  The move is
 // accepted when u < |R|^2 exp(2 dJ) q(old)/q(new), the Metropolis-Hastings
 // test of metropolis_move_1w (OmegaQMC/vmc_gto.py:841-905) without
@@ -547,27 +549,25 @@ __device__ __forceinline__ T oq_jastrow_delta(const SJ& J, const OqSystem& S, co
 // has_j2, j2): the system struct itself or a compact copy of those fields;
 // S is handed to the basis policy.
 template <int NOCC, typename T, typename Real, class B, class SJ>
-__device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, const OqSplit& SP,
-                                            const Real* __restrict__ C, double* pos,
-                                            Real* Ai, int WPB, int tid, int e,
-                                            double nx, double ny, double nz,
-                                            double log_extra, double mul_extra, double u,
-                                            double& logdet) {
+__device__ __forceinline__ bool oq_try_move_s(const SJ& J, const OqSystem& S, const OqSplit& SP,
+                                              const Real* __restrict__ C, double* pos, int ps,
+                                              Real* A, int as, int e, double nx, double ny,
+                                              double nz, double log_extra, double mul_extra,
+                                              double u, double& logdet) {
   constexpr int NE = 2 * NOCC;
   constexpr int NN = NOCC * NOCC;
   const int s = e & 1, i = e >> 1;
-  const double ox = pos[(3 * e) * WPB + tid], oy = pos[(3 * e + 1) * WPB + tid],
-               oz = pos[(3 * e + 2) * WPB + tid];
+  const double ox = pos[(3 * e) * ps], oy = pos[(3 * e + 1) * ps], oz = pos[(3 * e + 2) * ps];
   // Jastrow change (arithmetic in T) and the MIN_DIST_THRESHOLD test (FP64)
   bool valid;
-  const T dJ = oq_jastrow_delta<NE, T>(J, S, pos + tid, WPB, e, ox, oy, oz, nx, ny, nz, valid);
+  const T dJ = oq_jastrow_delta<NE, T>(J, S, pos, ps, e, ox, oy, oz, nx, ny, nz, valid);
   // new MO row and the ratio R = sum_m v_m A[m][i] (column i of the inverse)
   T v[NOCC];
   B::template mo_val<T, Real>(S, SP, C, nx, ny, nz, v);
-  Real* As = Ai + (size_t)s * NN * WPB;
+  Real* As = A + (size_t)s * NN * as;
   T R = (T)0;
 #pragma unroll
-  for (int m = 0; m < NOCC; ++m) R += v[m] * (T)As[(m * NOCC + i) * WPB + tid];
+  for (int m = 0; m < NOCC; ++m) R += v[m] * (T)As[(m * NOCC + i) * as];
   const double Rd = (double)R;
   // the exponential in the working precision (accurate expf in FP32: its
   // ~1e-7 relative error moves acceptance probabilities far below any
@@ -583,25 +583,38 @@ __device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, cons
     const T rinv = (T)1 / R;
     T coli[NOCC];
 #pragma unroll
-    for (int k = 0; k < NOCC; ++k) coli[k] = (T)As[(k * NOCC + i) * WPB + tid];
+    for (int k = 0; k < NOCC; ++k) coli[k] = (T)As[(k * NOCC + i) * as];
 #pragma unroll
     for (int j = 0; j < NOCC; ++j) {
       T w = (T)0;
 #pragma unroll
-      for (int m = 0; m < NOCC; ++m) w += v[m] * (T)As[(m * NOCC + j) * WPB + tid];
+      for (int m = 0; m < NOCC; ++m) w += v[m] * (T)As[(m * NOCC + j) * as];
       const T f = (w - (j == i ? (T)1 : (T)0)) * rinv;
 #pragma unroll
       for (int k = 0; k < NOCC; ++k) {
-        Real& ref = As[(k * NOCC + j) * WPB + tid];
+        Real& ref = As[(k * NOCC + j) * as];
         ref = (Real)((T)ref - coli[k] * f);
       }
     }
-    pos[(3 * e) * WPB + tid] = nx;
-    pos[(3 * e + 1) * WPB + tid] = ny;
-    pos[(3 * e + 2) * WPB + tid] = nz;
+    pos[(3 * e) * ps] = nx;
+    pos[(3 * e + 1) * ps] = ny;
+    pos[(3 * e + 2) * ps] = nz;
     logdet += log(fabs(Rd));
   }
   return acc;
+}
+
+// The same move with positions and inverses in one walker-minor layout of
+// stride WPB (this walker at index tid).
+template <int NOCC, typename T, typename Real, class B, class SJ>
+__device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, const OqSplit& SP,
+                                            const Real* __restrict__ C, double* pos,
+                                            Real* Ai, int WPB, int tid, int e,
+                                            double nx, double ny, double nz,
+                                            double log_extra, double mul_extra, double u,
+                                            double& logdet) {
+  return oq_try_move_s<NOCC, T, Real, B>(J, S, SP, C, pos + tid, WPB, Ai + tid, WPB, e, nx, ny,
+                                         nz, log_extra, mul_extra, u, logdet);
 }
 
 // Basin relocation proposal (basin_move_1w, OmegaQMC/vmc_gto.py:925-957):

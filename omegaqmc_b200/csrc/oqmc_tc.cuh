@@ -141,6 +141,32 @@ __device__ __forceinline__ void oq_tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Store 16 consecutive 32-bit columns of this thread's TMEM lane (32x32b
+// shape); the data reach tensor memory only after oq_tmem_wait_st().
+__device__ __forceinline__ void oq_tmem_st16(uint32_t taddr, const uint32_t r[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+      "%13,%14,%15,%16};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+      "r"(r[15])
+      : "memory");
+}
+__device__ __forceinline__ void oq_tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+// D[tmem] (+)= A[tmem] * B[smem]^T (kind::f16, BF16): A as 128 lanes (rows)
+// of K/2 32-bit columns, two consecutive K elements per column (the lower
+// 16 bits hold the even element), issued by one thread.
+__device__ __forceinline__ void oq_mma_bf16_ta(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc,
+                                               uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}" ::"r"(tmem_d),
+      "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
 // Round an FP32 value to TF32 (round to nearest, ties away) and return the
 // rounded value; v - oq_tf32(v) is the low part of a 2-term split.
 __device__ __forceinline__ float oq_tf32(float v) {
