@@ -58,9 +58,12 @@ const Variant kVariants[] = {{256, 1}, {128, 3}, {256, 2}};
 const int kNumVariants = 3;
 const size_t kMaxSmem = 227 * 1024;   // opt-in shared memory per CTA on sm_100
 
+// modes[k]: the move code compiled for molecule k (oq_batch_tile's MODE);
+// empty = 0 for every molecule.
 std::string batch_source(const std::vector<const OqSystem*>& S,
                          const std::vector<const OqSplit*>& SP,
-                         const std::vector<const double*>& C, const std::vector<int>& nocc) {
+                         const std::vector<const double*>& C, const std::vector<int>& nocc,
+                         const std::vector<int>& modes = {}) {
   std::string src = "#include \"oqmc_batch.cuh\"\n\n";
   for (size_t k = 0; k < S.size(); ++k)
     src += oq_spec_basis_source(*S[k], *SP[k], C[k], nocc[k], "OqSpecBasis_" + std::to_string(k)) +
@@ -79,9 +82,10 @@ std::string batch_source(const std::vector<const OqSystem*>& S,
       "    switch (tl.sys) {\n";
   for (size_t k = 0; k < S.size(); ++k) {
     const std::string ks = std::to_string(k);
+    const int mode = modes.empty() ? 0 : modes[k];
     src += "      case " + ks + ": oq_batch_tile<" + std::to_string(nocc[k]) +
-           ", T, Real, OqSpecBasis_" + ks + ">(a, d, oq_jas_" + ks +
-           ", tl.w0, step0, slot0, smem); break;\n";
+           ", T, Real, OqSpecBasis_" + ks + ", " + std::to_string(mode) + ">(a, d, oq_jas_" +
+           ks + ", tl.w0, step0, slot0, smem); break;\n";
   }
   src +=
       "      default: break;\n"
@@ -113,6 +117,12 @@ struct oqmc_batch {
   std::vector<oqmc_ctx*> ctx;
   std::vector<void*> mods;       // one module per register variant
   std::vector<void*> fn;
+  // module generated after tuning for the tuned shape only (each molecule's
+  // move code fixed to one lane or several); used while that shape is set
+  void* mod_final = nullptr;
+  void* fn_final = nullptr;
+  int final_threads = 0, final_variant = -1;
+  std::vector<int> final_wt;
   std::vector<OqBatchSys> hsys;
   std::vector<double> cost;      // relative cost of one walker (orders the tiles)
   OqBatchSys* d_sys = nullptr;
@@ -144,6 +154,15 @@ static int berr(oqmc_batch* b, int code, const std::string& msg) {
                                                            cudaGetErrorString(_e));     \
   } while (0)
 
+// The kernel for the current shape: the post-tuning module while the shape
+// is the tuned one, else the general module of the register variant.
+static void* kernel_fn(const oqmc_batch* b) {
+  if (b->fn_final && b->threads == b->final_threads && b->variant == b->final_variant &&
+      b->wt == b->final_wt)
+    return b->fn_final;
+  return b->fn[b->variant];
+}
+
 static void release_graph(oqmc_batch* b) {
   if (b->gexec) cudaGraphExecDestroy(b->gexec);
   if (b->graph) cudaGraphDestroy(b->graph);
@@ -166,7 +185,7 @@ static int plan(oqmc_batch* b) {
     smem = std::max(smem, tile_smem(b->ctx[k]->nocc, wt, nt, b->precision));
   }
   int occ = 0;
-  if (oq_rtc_occupancy(b->fn[b->variant], nt, smem, &occ) != 0)
+  if (oq_rtc_occupancy(kernel_fn(b), nt, smem, &occ) != 0)
     return berr(b, OQ_ERR_CUDA, "occupancy query failed");
   if (occ < 1) return berr(b, OQ_ERR_ARG, "tile configuration does not fit on an SM");
   // tiles, most expensive first
@@ -212,8 +231,41 @@ static int launch(oqmc_batch* b, int n_sweeps, int measure_every, uint64_t seed,
   a.write_sums = write_sums;
   a.seed = seed;
   void* args[1] = {(void*)&a};
-  if (oq_rtc_launch(b->fn[b->variant], dim3(b->grid), dim3(b->threads), b->smem, s, args) != 0)
+  if (oq_rtc_launch(kernel_fn(b), dim3(b->grid), dim3(b->threads), b->smem, s, args) != 0)
     return berr(b, OQ_ERR_CUDA, "batched kernel launch failed");
+  return OQ_OK;
+}
+
+// Compile and load the batch kernel for the current shape with every
+// molecule's move code fixed (one lane per walker, or several), in the
+// current register variant only.
+static int finalize_module(oqmc_batch* b) {
+  std::vector<const OqSystem*> S;
+  std::vector<const OqSplit*> SP;
+  std::vector<const double*> C;
+  std::vector<int> nocc, modes;
+  for (int k = 0; k < b->n; ++k) {
+    S.push_back(&b->ctx[k]->hsys);
+    SP.push_back(&b->ctx[k]->hsplit);
+    C.push_back(b->ctx[k]->h_C);
+    nocc.push_back(b->ctx[k]->nocc);
+    modes.push_back(b->threads / b->wt[k] > 1 ? 2 : 1);
+  }
+  std::vector<char> cubin;
+  std::vector<std::string> lowered;
+  std::string e;
+  if (oq_rtc_compile(batch_source(S, SP, C, nocc, modes), {kernel_name(b->precision, b->variant)},
+                     &cubin, &lowered, &e) != 0)
+    return OQ_ERR_UNSUPPORTED;
+  void* mod = nullptr;
+  std::vector<void*> f;
+  if (oq_rtc_load(cubin, lowered, &mod, &f, &e) != 0) return OQ_ERR_UNSUPPORTED;
+  if (b->mod_final) oq_rtc_unload(b->mod_final);
+  b->mod_final = mod;
+  b->fn_final = f[0];
+  b->final_threads = b->threads;
+  b->final_variant = b->variant;
+  b->final_wt = b->wt;
   return OQ_OK;
 }
 
@@ -234,6 +286,7 @@ int oqmc_batch_destroy(oqmc_batch* b) {
   if (b->d_busy) cudaFree(b->d_busy);
   if (b->d_flags) cudaFree(b->d_flags);
   for (void* m : b->mods) oq_rtc_unload(m);
+  if (b->mod_final) oq_rtc_unload(b->mod_final);
   delete b;
   return OQ_OK;
 }
@@ -391,8 +444,8 @@ int oqmc_batch_get_config(const oqmc_batch* b, int* threads, int* walkers_per_ti
   if (variant) *variant = b->variant;
   if (grid) *grid = b->grid;
   if (smem) *smem = b->smem;
-  if (regs) *regs = oq_rtc_regs(b->fn[b->variant]);
-  if (local_bytes) *local_bytes = oq_rtc_local_bytes(b->fn[b->variant]);
+  if (regs) *regs = oq_rtc_regs(kernel_fn(b));
+  if (local_bytes) *local_bytes = oq_rtc_local_bytes(kernel_fn(b));
   return OQ_OK;
 }
 
@@ -556,6 +609,14 @@ int oqmc_batch_tune(oqmc_batch* b, int n_sweeps, uint64_t seed, void* stream, fl
   if (!found) return berr(b, OQ_ERR_ARG, "no tile configuration fits");
   int rc = oqmc_batch_configure(b, best_t, best_wt.data(), best_v);
   if (rc != OQ_OK) return rc;
+  // the module for the tuned shape alone (smaller code: each molecule keeps
+  // only the move code of its lane count); the general one stays for other
+  // shapes, and is used if this compilation fails.  Several molecules only:
+  // one molecule's kernel gained nothing measurable for the extra compile
+  if (b->n > 1 && finalize_module(b) == OQ_OK) {
+    rc = plan(b);
+    if (rc != OQ_OK) return rc;
+  }
   // measured per-walker cost orders the tiles
   OQ_BCUDA(b, cudaMemsetAsync(b->d_busy, 0, b->n * sizeof(unsigned long long), s));
   rc = launch(b, n_sweeps, me, seed, 0, s);

@@ -294,7 +294,10 @@ __device__ __forceinline__ int oq_batch_sweep_lanes(const OqBatchArgs& a, const 
 // (see above) the refresh splits the two spin blocks over lanes 0 and 1,
 // the sweeps run in blocks of P electrons and the local energy splits the
 // electrons over the lanes; lane sums are combined with shuffles.
-template <int NOCC, typename T, typename Real, class B, class SJ>
+// MODE selects the move code compiled in: 0 both (lanes chosen at run time),
+// 1 one lane per walker only, 2 several lanes only (the module generated
+// after tuning, when every molecule's lane count is fixed).
+template <int NOCC, typename T, typename Real, class B, int MODE = 0, class SJ>
 __device__ __forceinline__ void oq_batch_tile(const OqBatchArgs& a, const OqBatchSys& d,
                                               const SJ& J, int w0, uint64_t step0,
                                               uint64_t slot0, unsigned char* smem) {
@@ -358,10 +361,10 @@ __device__ __forceinline__ void oq_batch_tile(const OqBatchArgs& a, const OqBatc
   int nacc = 0, meas = 0;
   for (int t = 0; t < a.n_sweeps; ++t) {
     const uint32_t gstep = (uint32_t)(step0 + t);
-    if (P > 1) {
+    if (MODE != 1 && P > 1) {
       nacc += oq_batch_sweep_lanes<NOCC, T, Real, B>(a, d, J, S, SP, C, pos, Ai, WT, wl, lane,
                                                      P, live, (uint32_t)w, gstep, logdet);
-    } else if (live) {
+    } else if (MODE != 2 && live) {
       for (int e = 0; e < NE; ++e) {
         double n3[3], u;
         oq_move_randoms(a.seed, (uint32_t)w, gstep, (uint32_t)e, n3, u);

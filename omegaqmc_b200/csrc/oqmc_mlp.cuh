@@ -165,8 +165,15 @@ __device__ __forceinline__ void oq_mlp_out_epilogue(uint32_t tmem_row, const flo
 #pragma unroll
   for (int q = 0; q < OQ_MLP_NOUT / 16; ++q) oq_tmem_ld16_nw(tmem_row + (uint32_t)(16 * q), raw + 16 * q);
   oq_tmem_wait_ld();
+  const float4* b4 = reinterpret_cast<const float4*>(bias);   // 16-byte aligned
 #pragma unroll
-  for (int j = 0; j < OQ_MLP_NOUT; ++j) out[j] = __uint_as_float(raw[j]) + bias[j];
+  for (int j = 0; j < OQ_MLP_NOUT / 4; ++j) {
+    const float4 bb = b4[j];
+    out[4 * j] = __uint_as_float(raw[4 * j]) + bb.x;
+    out[4 * j + 1] = __uint_as_float(raw[4 * j + 1]) + bb.y;
+    out[4 * j + 2] = __uint_as_float(raw[4 * j + 2]) + bb.z;
+    out[4 * j + 3] = __uint_as_float(raw[4 * j + 3]) + bb.w;
+  }
 }
 
 // Load biases b1..b3 (128 each) and b4 (48) from the FP32 parameter vector.
@@ -262,15 +269,18 @@ __device__ __forceinline__ void oq_mlp_hidden_epilogue_ta(uint32_t trow, const f
     oq_tmem_wait_ld();
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
+      // the biases as 16-byte shared-memory loads (the same words for every
+      // thread: broadcasts)
+      const float4* b4 = reinterpret_cast<const float4*>(bias + h0 + 32 * q);
       uint32_t pk[16];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int c = h0 + 32 * q + 2 * j;
-        float z0 = __uint_as_float(raw[32 * q + 2 * j]) + bias[c];
-        float z1 = __uint_as_float(raw[32 * q + 2 * j + 1]) + bias[c + 1];
-        z0 = z0 > 0.0f ? z0 : 0.0f;
-        z1 = z1 > 0.0f ? z1 : 0.0f;
-        pk[j] = oq_bf16x2(z0, z1);
+      for (int j = 0; j < 8; ++j) {
+        const float4 bb = b4[j];
+        const uint32_t* rw = raw + 32 * q + 4 * j;
+        pk[2 * j] = oq_bf16x2(fmaxf(__uint_as_float(rw[0]) + bb.x, 0.0f),
+                              fmaxf(__uint_as_float(rw[1]) + bb.y, 0.0f));
+        pk[2 * j + 1] = oq_bf16x2(fmaxf(__uint_as_float(rw[2]) + bb.z, 0.0f),
+                                  fmaxf(__uint_as_float(rw[3]) + bb.w, 0.0f));
       }
       oq_tmem_st16(trow + OQ_MLP_TA_COL + (uint32_t)((h0 + 32 * q) >> 1), pk);
     }
@@ -502,11 +512,12 @@ __device__ __forceinline__ void oq_mlp_features(const SJ& J, PosF P, int ne, int
   f[31] = 1.0f;
 }
 
-// The same features for a compile-time electron count: the squared
-// distances to the other electrons are computed once and kept in
-// registers, the 8 nearest are selected with branch-free compare/selects
-// (same order and tie rule as oq_mlp_features) and only their coordinates
-// are read again.
+// The same features for a compile-time electron count (the sweep's): the
+// squared distances to the other electrons are computed once in FP32 and
+// kept in registers, the 8 nearest are selected with branch-free
+// compare/selects (same order and tie rule as oq_mlp_features, which ranks
+// FP64 distances, so two nearly equidistant electrons can swap places) and
+// only their coordinates are read again.
 template <int NE, class SJ, class PosF>
 __device__ __forceinline__ void oq_mlp_features_ne(const SJ& J, PosF P, int e, double xe,
                                                    double ye, double ze, float f[OQ_MLP_K0]) {
@@ -524,15 +535,18 @@ __device__ __forceinline__ void oq_mlp_features_ne(const SJ& J, PosF P, int e, d
   if (J.natm == 1) i1 = i0;
   f[0] = (float)(xe - J.nuc[i0][0]); f[1] = (float)(ye - J.nuc[i0][1]); f[2] = (float)(ze - J.nuc[i0][2]);
   f[3] = (float)(xe - J.nuc[i1][0]); f[4] = (float)(ye - J.nuc[i1][1]); f[5] = (float)(ze - J.nuc[i1][2]);
-  double r2[NE];
+  // squared distances in FP32 from the FP64 coordinate differences: the
+  // ranking only has to be a fixed function of the configuration
+  float r2[NE];
 #pragma unroll
   for (int j = 0; j < NE; ++j) {
-    const double ax = P(j, 0) - xe, ay = P(j, 1) - ye, az = P(j, 2) - ze;
-    r2[j] = (j == e) ? 1e300 : ax * ax + ay * ay + az * az;
+    const float ax = (float)(P(j, 0) - xe), ay = (float)(P(j, 1) - ye),
+                az = (float)(P(j, 2) - ze);
+    r2[j] = (j == e) ? 3.0e38f : ax * ax + ay * ay + az * az;
   }
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    double best = 1e300;
+    float best = 3.0e38f;
     int bj = -1;
 #pragma unroll
     for (int j = 0; j < NE; ++j) {
@@ -541,7 +555,7 @@ __device__ __forceinline__ void oq_mlp_features_ne(const SJ& J, PosF P, int e, d
       bj = c ? j : bj;
     }
 #pragma unroll
-    for (int j = 0; j < NE; ++j) r2[j] = (j == bj) ? 1e300 : r2[j];
+    for (int j = 0; j < NE; ++j) r2[j] = (j == bj) ? 3.0e38f : r2[j];
     if (bj < 0) {
       f[6 + 3 * k] = 0.0f; f[7 + 3 * k] = 0.0f; f[8 + 3 * k] = 0.0f;
     } else {

@@ -33,8 +33,8 @@ def test_batch_source_dispatches_every_system():
                for n in ("H2", "LiH")]
     src = R.batch_source(systems)
     assert "struct OqSpecBasis_0" in src and "struct OqSpecBasis_1" in src
-    assert "oq_batch_tile<1, T, Real, OqSpecBasis_0>(a, d, oq_jas_0" in src
-    assert "oq_batch_tile<2, T, Real, OqSpecBasis_1>(a, d, oq_jas_1" in src
+    assert "oq_batch_tile<1, T, Real, OqSpecBasis_0, 0>(a, d, oq_jas_0" in src
+    assert "oq_batch_tile<2, T, Real, OqSpecBasis_1, 0>(a, d, oq_jas_1" in src
     assert "__constant__ OqJas oq_jas_1 = {2, " in src
 
 
