@@ -29,13 +29,15 @@ def _host_loop(ens, n, step, target=0.4, rate=0.05):
     return step, np.array(accs), np.array(steps)
 
 
-@pytest.mark.parametrize("name,prec,proposal", [("bench_h2o", "fp64", 0),
-                                                ("bench_h2o", "mixed", 1),
-                                                ("bench_lih", "fp64", 1)])
-def test_device_adaptation_follows_host_loop(name, prec, proposal):
+@pytest.mark.parametrize("name,prec,proposal,spec", [("bench_h2o", "fp64", 0, True),
+                                                     ("bench_h2o", "mixed", 1, True),
+                                                     ("bench_lih", "fp64", 1, True),
+                                                     ("bench_lih", "mixed", 0, False)])
+def test_device_adaptation_follows_host_loop(name, prec, proposal, spec):
     s, _ = golden_system(name)
     ctx = GTOContext(s)
-    ctx.specialize()
+    if spec:
+        ctx.specialize()            # else the table-driven move kernel
     if proposal:
         ctx.set_proposal(1, 1.0, 0.05)
     X0 = seeded_walkers(s, 2048, 1.0, 3)
