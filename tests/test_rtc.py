@@ -48,3 +48,22 @@ def test_batch_kernel_compiles_for_sm100a():
     ok, log, cubin = R.compile_source(R.batch_source(systems), R.BATCH_KERNELS[:1])
     assert ok, log
     assert len(cubin) > 10000
+
+
+def test_tuned_batch_module_compiles_for_sm100a():
+    """The module compiled after tuning fixes each molecule's move code (one
+    lane per walker: mode 1, several: mode 2); it must compile too."""
+    try:
+        R._nvrtc()
+    except OSError:
+        pytest.skip("NVRTC not installed")
+    systems = [build_system(M.make_mf(n), M.benchmark_params_corr(M.make_mf(n).mol))
+               for n in ("H2", "LiH")]
+    src = R.batch_source(systems)
+    fixed = (src.replace("OqSpecBasis_0, 0>(a, d,", "OqSpecBasis_0, 1>(a, d,")
+                .replace("OqSpecBasis_1, 0>(a, d,", "OqSpecBasis_1, 2>(a, d,"))
+    assert fixed != src
+    ok, log, cubin = R.compile_source(fixed, R.BATCH_KERNELS[:1])
+    assert ok, log
+    ok0, _, cubin0 = R.compile_source(src, R.BATCH_KERNELS[:1])
+    assert ok0 and len(cubin) < len(cubin0)
