@@ -192,3 +192,34 @@ def test_full_size_headline_launch_is_consistent():
     ref = ctx.evaluate(X, want_grad=False, want_lap=False)["e_loc"]
     e_last = s[-1, 3] / s[-1, 6]
     assert abs(e_last - float(ref.mean())) < 1e-4 * max(1.0, float(ref.abs().mean()) / 10)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_batch_lanes_with_bspline_and_three_body_jastrows(precision):
+    """The lanes path splits the Jastrow change over the lanes (B-spline
+    pairs and nuclei, the three-body term on lane 0): with B-spline and J3
+    trials (golden cases the reference evaluated) at 2 and 4 lanes per
+    walker a batched launch still leaves the per-system path's walkers."""
+    from helpers import golden_system
+    ctxs = []
+    for name in ("h2o_bspline", "h2o_j3"):
+        c = GTOContext(golden_system(name)[0])
+        c.specialize()
+        ctxs.append(c)
+    X0 = [torch.as_tensor(seeded_walkers(c.system, 200, 0.8, 9 + k), device="cuda")
+          for k, c in enumerate(ctxs)]
+    steps, props = [0.5, 0.5], ["plain", "scaled"]
+    b = BatchedSampler(ctxs, [x.clone() for x in X0], steps, precision=precision,
+                       proposal=props, cap=8)
+    b.configure(128, [64, 32], variant=0)            # 2 and 4 lanes per walker
+    n, me, seed, base = 12, 4, 321, 40
+    b.reset(base)
+    b.run(n, me, seed)
+    torch.cuda.synchronize()
+    assert b.flags() == 0
+    for k, ctx in enumerate(ctxs):
+        X, sums = _per_system(ctx, X0[k], precision, props[k], steps[k], n, me, seed, base)
+        same = torch.all((b.walkers[k] == X).reshape(X.shape[0], -1), dim=1)
+        assert float(same.float().mean()) > 0.98, k
+        bs = b.sums[k][: n // me].cpu().numpy()
+        np.testing.assert_array_equal(bs[:, 6], sums.cpu().numpy()[:, 6])
