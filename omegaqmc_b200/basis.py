@@ -114,7 +114,11 @@ def _parse_gaussian94(lines):
         scale = _num(toks[2]) if len(toks) > 2 else 1.0
         rows = []
         while len(rows) < nprim:
-            r = next(it).split("!", 1)[0].split()
+            line2 = next(it, None)
+            if line2 is None:
+                raise ValueError(f"shell {lab} of {elem}: {nprim} primitives announced, "
+                                 f"{len(rows)} found")
+            r = line2.split("!", 1)[0].split()
             if not r:
                 continue
             rows.append([_num(t) for t in r])

@@ -78,6 +78,8 @@ def test_bad_text_is_refused():
         parse_basis_text("H SP\n 1.0 1.0\n")
     with pytest.raises(ValueError):
         load_basis(NWCHEM, ["H", "O"])
+    with pytest.raises(ValueError):
+        parse_basis_text("****\nH 0\nS 3 1.00\n 1.0 0.5\n****\n")     # truncated shell
 
 
 def test_rhf_from_text_matches_dict(tmp_path):
