@@ -94,7 +94,8 @@ def parse():
                          "(H2O)2 in one persistent launch under a CUDA graph; learned: N2 "
                          "with the trained MLP proposal against the plain random walk; "
                          "alle: the reference's all-electron move; h2, lih: "
-                         "configurations 1 and 2 (H2 FP64; LiH FP64 against mixed, with "
+                         "the H2/STO-3G plain-method workload (FP64, 1,024 walkers) and the "
+                         "LiH workload (16,384 walkers, FP64 against mixed, with "
                          "per-output errors)")
     ap.add_argument("--path", default="persistent", choices=["persistent", "split"],
                     help="persistent: one fused launch per 50 sweeps (refresh, moves, E_L) "
@@ -1413,11 +1414,11 @@ def run_alle(a):
 
 
 CONFIGS = {
-    # configuration 1: H2/STO-3G, RHF, Padé J2 b = 1, 1,024 walkers from
+    # H2/STO-3G plain method: RHF, Padé J2 b = 1, 1,024 walkers from
     # N(nucleus, 0.5), fixed-width Gaussian step 0.3 bohr, 2,000 steps, FP64
     "h2": {"system": "H2", "walkers": 1024, "sigma": 0.5, "sweeps": 2000,
            "precisions": ("fp64",), "proposal": "plain", "step": 0.3, "j1": False},
-    # configuration 2: LiH cc-pVDZ-shaped, RHF, Padé J1 (a = -Z) + J2, 16,384
+    # LiH cc-pVDZ-shaped: RHF, Padé J1 (a = -Z) + J2, 16,384
     # walkers from N(nucleus, 1.0); FP64 against mixed with the same proposal
     "lih": {"system": "LiH", "walkers": 16384, "sigma": 1.0, "sweeps": 2000,
             "precisions": ("mixed", "fp64"), "proposal": "scaled", "step": 0.0, "j1": True},
@@ -1425,9 +1426,9 @@ CONFIGS = {
 
 
 def run_config(a):
-    """Configurations 1 (H2) and 2 (LiH) through the persistent path: per
+    """The H2/STO-3G and LiH workloads through the persistent path: per
     precision, equilibration, then whole 50-sweep launches replayed from a
-    CUDA graph for the configuration's sweep count (repeated until at least
+    CUDA graph for the workload's sweep count (repeated until at least
     1 s is timed); tau_int from the timed series.  LiH adds the error of
     every per-walker output of the mixed sampler against the FP64
     evaluation on 4,096 fixed seeded configurations."""

@@ -13,7 +13,7 @@ inputs from the builders instead.  ``--verify`` recomputes and compares with
 the stored outputs without writing.  The ``bench_*`` cases are the exact
 trials the benchmark runs: the synthetic cc-pVDZ-shaped basis, RHF orbitals
 from this package's SCF and the benchmark Jastrow (``h2o``, ``n2``), the
-configuration-1 H2 trial and the configuration-2 LiH trial.
+H2/STO-3G plain-method trial (Padé J2) and the LiH trial (Padé J1 + J2).
 
 JAX and PySCF are not installed, so the reference modules
 ``OmegaQMC/psi/shell.py``, ``OmegaQMC/psi/gto.py`` and ``OmegaQMC/utils.py``
@@ -302,8 +302,8 @@ CASES = {
                                             "unlike": np.array([0.5, 0.8])}},
                    1.0, 16),
     # the benchmark's own trials (RHF orbitals, see RHF_CASES): H2O and N2
-    # with the benchmark Jastrow (Padé J2, b = 3, no J1); configuration 1
-    # (H2/STO-3G, J2 b = 1); configuration 2 (LiH, Padé J1 with a = -Z and
+    # with the benchmark Jastrow (Padé J2, b = 3, no J1); the H2/STO-3G
+    # plain-method trial (J2 b = 1); the LiH trial (Padé J1 with a = -Z and
     # J2, b = 1)
     "bench_h2o": (lambda: M.named_system("H2O"), False, M.benchmark_params_corr, 1.0, 24),
     "bench_n2": (lambda: M.named_system("N2"), False, M.benchmark_params_corr, 1.0, 16),
