@@ -120,22 +120,37 @@ def work_per_walker_sweep(s, acc=0.5):
 
     Moves (per electron): distinct exponentials; radial sums 2 flops per
     (primitive, column); angular 3 (p) / 17 (d) / 12*(2l+1) (f, g); MO row
-    2 nbf nocc; ratio vector 2 nocc^2; Sherman-Morrison 2 nocc^2 x acceptance;
-    Jastrow change 2 x 14 flops per other particle.  Local energy (per
-    electron): exponentials; radial VGL 6 flops per (primitive, column);
-    angular VGL 12 per AO; MO VGL 10 nbf nocc; Slater assembly 8 nocc + 6;
-    Jastrow VGL 20 per partner; Coulomb 10 per pair.
+    2 per MO coefficient; ratio vector 2 nocc^2; Sherman-Morrison 2 nocc^2 x
+    acceptance; Jastrow change 2 x 14 flops per other particle.  Local
+    energy (per electron): exponentials; radial VGL 6 flops per (primitive,
+    column); angular VGL 12 per AO; MO VGL 10 per MO coefficient; Slater
+    assembly 8 nocc + 6; Jastrow VGL 20 per partner; Coulomb 10 per pair.
+    The MO coefficients counted are those the generated kernels evaluate
+    (``mo_terms``); ``flops_dense`` counts all nbf x nocc of them.
     """
     groups = s.prim_groups()
     n_exp = sum(len(a) for _, a, _ in groups)
     rad = sum(len(a) * len(ids) for _, a, ids in groups)
     ang_v = sum({0: 0, 1: 3, 2: 17}.get(sh.am, 12 * (2 * sh.am + 1)) for sh in s.shells)
     ne, no, nb, nn = s.n_e, s.nocc, s.nbf, s.natm
-    move = 2 * rad + ang_v + 2 * nb * no + 2 * no * no + 2 * no * no * acc + 28 * (ne - 1 + nn)
-    el = 6 * rad + 12 * nb + 10 * nb * no + 8 * no + 6 + 20 * (ne - 1 + nn)
-    coul = 10 * (ne * (ne - 1) // 2 + ne * nn)
-    flops = ne * (move + el) + coul
-    return {"flops": float(flops), "exps": float(2 * ne * n_exp)}
+
+    def total(nc):
+        move = 2 * rad + ang_v + 2 * nc + 2 * no * no + 2 * no * no * acc + 28 * (ne - 1 + nn)
+        el = 6 * rad + 12 * nb + 10 * nc + 8 * no + 6 + 20 * (ne - 1 + nn)
+        coul = 10 * (ne * (ne - 1) // 2 + ne * nn)
+        return float(ne * (move + el) + coul)
+
+    return {"flops": total(mo_terms(s)), "flops_dense": total(nb * no),
+            "mo_terms": mo_terms(s), "exps": float(2 * ne * n_exp)}
+
+
+def mo_terms(s):
+    """MO coefficients the generated kernels evaluate: those above 1e-12 of
+    their orbital's largest |coefficient| (the kernel generator leaves out
+    the round-off-level entries that point-group symmetry makes zero)."""
+    C = np.abs(np.asarray(s.C, dtype=np.float64))
+    cmax = C.max(axis=0, keepdims=True)
+    return int(np.count_nonzero((C != 0.0) & (C > 1e-12 * cmax)))
 
 
 class ClockSampler:
@@ -552,6 +567,8 @@ def run_ours(a):
                      "kernel_ms_per_launch": sweep_ms,
                      "refresh_ms_per_launch": refresh_ms,
                      "flops_per_walker_sweep": work["flops"],
+                     "flops_per_walker_sweep_dense": work["flops_dense"],
+                     "mo_terms": work["mo_terms"],
                      "peak_source": "own FMA microkernel (oqmc_measure_peak), of measured"},
     }
     if plain:
@@ -904,6 +921,8 @@ def run_persistent(a):
                      "kernel": "k_batch (one launch: refresh + 50 sweeps)",
                      "kernel_ms_per_launch": launch_ms,
                      "flops_per_walker_sweep": work["flops"],
+                     "flops_per_walker_sweep_dense": work["flops_dense"],
+                     "mo_terms": work["mo_terms"],
                      "peak_source": "own FMA microkernel (oqmc_measure_peak), of measured"},
     }
     line["tau_int_segments"] = kq

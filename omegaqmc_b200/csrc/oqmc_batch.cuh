@@ -259,7 +259,7 @@ __device__ __forceinline__ int oq_batch_sweep_lanes(const OqBatchArgs& a, const 
       // every lane has read column i before any lane updates it
       __syncwarp();
       if (acc) {
-        const T rinv = (T)1 / R;
+        const T rinv = oq_rcp(R);
         for (int j = lane; j < NOCC; j += P) {
           T wj = (T)0;
 #pragma unroll

@@ -165,11 +165,22 @@ __device__ __forceinline__ void oq_move_randoms(uint64_t seed, uint32_t walker,
   u = (double)lo * 2.3283064365386963e-10;                     // in [0, 1)
 }
 
-// reciprocal / reciprocal square root in the working precision
+// reciprocal / reciprocal square root in the working precision; in FP32 the
+// hardware approximations themselves (rcp.approx / rsqrt.approx, relative
+// error ~2^-23, subnormals flushed: the arguments here are distances and
+// Jastrow denominators, far from the subnormal range)
 __device__ __forceinline__ double oq_rcp(double x) { return __drcp_rn(x); }
-__device__ __forceinline__ float oq_rcp(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ float oq_rcp(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 __device__ __forceinline__ double oq_rsqrt(double x) { return rsqrt(x); }
-__device__ __forceinline__ float oq_rsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ float oq_rsqrt(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 
 // Padé u = a r / (1 + b r) from r and 1/r with one reciprocal:
 // q = 1/(1+br), u = a r q, u'/r = a q^2 / r, u'' + 2u'/r = -2ab q^3 + 2u'/r

@@ -4,11 +4,14 @@
 // straight-line CUDA: one displacement per nucleus, every exponential of every
 // exponent group, the contraction sums and the MO accumulation with the
 // exponents, normalised contraction coefficients and MO coefficients as
-// literals (zero MO coefficients dropped).  NVRTC compiles the move and
+// literals (MO coefficients at round-off level dropped, see Gen::keep).
+// NVRTC compiles the move and
 // local-energy kernels with that policy for sm_100a and the driver API loads
 // them; the sweep entry points then launch these instead of the table-driven
 // kernels.  NVRTC and the driver library are opened with dlopen, so the
 // library loads (and runs its table-driven kernels) where NVRTC is absent.
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <dlfcn.h>
@@ -101,7 +104,25 @@ struct Gen {
   int nocc;
   std::string o;
   bool contract = false;   // VGL contracted with an inverse column (mo_vgl_contract)
+  std::vector<double> cmax;  // largest |C[.][m]| of each orbital
   void add(const std::string& s) { o += s; }
+
+  // Whether C[ao][m] enters the generated code.  An orbital of a molecule
+  // with point-group symmetry has exact zeros on the AOs of other irreducible
+  // representations, which an eigensolver returns as round-off (1e-15 of the
+  // orbital's largest coefficient; half of the H2O coefficients).  Terms
+  // below 1e-12 of that largest coefficient change an orbital value by less
+  // than 1e-12 of its scale, far below the FP64 parity tolerance, so they
+  // are left out of the straight-line code.
+  bool keep(int ao, int m) {
+    if (cmax.empty()) {
+      cmax.assign(nocc, 0.0);
+      for (int mu = 0; mu < S.nbf; ++mu)
+        for (int k = 0; k < nocc; ++k) cmax[k] = std::max(cmax[k], std::fabs(C[mu * nocc + k]));
+    }
+    const double c = std::fabs(C[ao * nocc + m]);
+    return c != 0.0 && c > 1e-12 * cmax[m];
+  }
 
   static std::string num(double v) {
     char b[40];
@@ -131,15 +152,16 @@ struct Gen {
       if (vgl) add(", Rp" + ks + " = 0, Rl" + ks + ", Ra" + ks + " = 0");
       add(";\n");
     }
-    const std::string ex = (ty == "double") ? "exp" : "oq_exp<T>";
     for (int p = 0; p < np; ++p) {
       if ((sel == 1 && !tight(g, p)) || (sel == 2 && tight(g, p))) continue;
       const double a = S.alpha[off + p];
       if (tight_arg && tight(g, p))   // FP64 argument, see oq_exp_tight
         add("      { const " + ty + " e = oq_exp_tight<" + ty + ">(" + num(a) + " * r2d);\n");
-      else
-        add("      { const " + ty + " e = " + ex + "(-((" + ty + ")" + num(a) + ") * " + r2 +
-            ");\n");
+      else if (ty == "double")
+        add("      { const double e = exp(-((double)" + num(a) + ") * " + r2 + ");\n");
+      else   // a and a log2(e) folded here, see oq_exp_neg
+        add("      { const T e = oq_exp_neg<T>((T)" + num(a) + ", (T)" +
+            num(a * 1.4426950408889634) + ", " + r2 + ");\n");
       for (int k = 0; k < nc; ++k) {
         const double n = S.norm[S.s_norm[sh0 + k] + p];
         const std::string ks = std::to_string(k);
@@ -166,7 +188,7 @@ struct Gen {
       std::string ca;
       for (int m = 0; m < nocc; ++m) {
         const double c = C[ao * nocc + m];
-        if (c == 0.0) continue;
+        if (!keep(ao, m)) continue;
         ca += std::string(ca.empty() ? "" : " + ") + "(T)(" + num(c) + ") * ac[" +
               std::to_string(m) + "]";
       }
@@ -177,7 +199,7 @@ struct Gen {
     }
     for (int m = 0; m < nocc; ++m) {
       const double c = C[ao * nocc + m];
-      if (c == 0.0) continue;
+      if (!keep(ao, m)) continue;
       const std::string cl = "(T)(" + num(c) + ")", ms = std::to_string(m);
       add("      mv[" + ms + "] += " + cl + " * " + v + ";\n");
       if (g) {

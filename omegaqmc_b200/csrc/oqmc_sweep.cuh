@@ -30,6 +30,20 @@ template <typename T> __device__ __forceinline__ T oq_exp(T v);
 template <> __device__ __forceinline__ double oq_exp<double>(double v) { return exp(v); }
 template <> __device__ __forceinline__ float oq_exp<float>(float v) { return __expf(v); }
 
+// exp(-a r2) of a basis primitive in the generated code, given a and
+// al2 = a log2(e) as literals: FP64 exp in the FP64 build; in FP32 the
+// power of two 2^(-al2 r2) straight from the hardware approximation
+// (ex2.approx, relative error ~2^-22), one multiply per primitive.
+template <typename T> __device__ __forceinline__ T oq_exp_neg(T a, T al2, T r2);
+template <> __device__ __forceinline__ double oq_exp_neg<double>(double a, double, double r2) {
+  return exp(-a * r2);
+}
+template <> __device__ __forceinline__ float oq_exp_neg<float>(float, float al2, float r2) {
+  float p;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(p) : "f"(-al2 * r2));
+  return p;
+}
+
 // exp(-arg) for a tight exponent, arg = alpha r^2 formed in FP64.  In FP32
 // the rounding of a large argument would dominate the error, so the FP64
 // argument is split as arg log2(e) = k + f (k integer, f in [0, 1)) and only
@@ -580,7 +594,7 @@ __device__ __forceinline__ bool oq_try_move_s(const SJ& J, const OqSystem& S, co
   if (acc) {
     // Sherman-Morrison with the ratio vector w_j = sum_m v_m A[m][j]:
     // A[k][j] -= A[k][i] (w_j - delta_ij) / R, column i taken before the update
-    const T rinv = (T)1 / R;
+    const T rinv = oq_rcp(R);
     T coli[NOCC];
 #pragma unroll
     for (int k = 0; k < NOCC; ++k) coli[k] = (T)As[(k * NOCC + i) * as];
@@ -761,6 +775,13 @@ __device__ __forceinline__ void oq_jastrow_vgl_coulomb(const SJ& J, const OqSyst
                                                        double xe, double ye, double ze, T& jx,
                                                        T& jy, T& jz, T& jl, double& ee,
                                                        double& en) {
+  // The gradient sums run in FP64 on the FP64 displacements: in the mixed
+  // build that converts one value per pair (u'(r)/r) to FP64 instead of
+  // three displacement components to FP32.  The working-precision Coulomb
+  // terms of one electron are summed in T and converted once.  In the FP64
+  // build both forms are the same arithmetic in the same order.
+  double gx = 0.0, gy = 0.0, gz = 0.0;
+  T eet = (T)0, ent = (T)0;
   for (int j = 0; j < NE; ++j) {
     if (j == e) continue;
     const double dx = xe - pos[(size_t)(3 * j) * ps], dy = ye - pos[(size_t)(3 * j + 1) * ps],
@@ -770,12 +791,18 @@ __device__ __forceinline__ void oq_jastrow_vgl_coulomb(const SJ& J, const OqSyst
     // Coulomb: FP64 with the reference's eps in FP64 kernels; the working-
     // precision 1/r otherwise (eps is below FP32 resolution beyond the
     // 1e-4 bohr minimum distance)
-    if (j > e) ee += (sizeof(T) == 8) ? rsqrt(r2 + OQ_EPS) : (double)rinv;
+    if (j > e) {
+      if (sizeof(T) == 8)
+        ee += rsqrt(r2 + OQ_EPS);
+      else
+        eet += rinv;
+    }
     if (J.has_j2) {
       const int o = ((e & 1) == (j & 1)) ? 0 : 2;
       T upr, l;
       oq_pade_vgl_q((T)J.j2[o], (T)J.j2[o + 1], r2t * rinv, rinv, upr, l);
-      jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
+      const double u = (double)upr;
+      gx += u * dx; gy += u * dy; gz += u * dz; jl += l;
     }
     if (S.has_bs2) {
       const bool like = (e & 1) == (j & 1);
@@ -783,27 +810,38 @@ __device__ __forceinline__ void oq_jastrow_vgl_coulomb(const SJ& J, const OqSyst
       oq_bs_vgl<T>(like ? S.bs2_like : S.bs2_unlike, like ? S.bs2_n_like : S.bs2_n_unlike,
                    (T)(like ? S.bs2_dinv_like : S.bs2_dinv_unlike), (T)S.bs2_rcut, r2t * rinv,
                    rinv, upr, l);
-      jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
+      const double u = (double)upr;
+      gx += u * dx; gy += u * dy; gz += u * dz; jl += l;
     }
   }
   for (int I = 0; I < J.natm; ++I) {
     const double dx = xe - J.nuc[I][0], dy = ye - J.nuc[I][1], dz = ze - J.nuc[I][2];
     const double r2 = dx * dx + dy * dy + dz * dz;
     const T r2t = (T)r2, rinv = oq_rsqrt(r2t);
-    en -= J.Z[I] * ((sizeof(T) == 8) ? rsqrt(r2 + OQ_EPS) : (double)rinv);
+    if (sizeof(T) == 8)
+      en -= J.Z[I] * rsqrt(r2 + OQ_EPS);
+    else
+      ent -= (T)J.Z[I] * rinv;
     if (J.has_j1) {
       T upr, l;
       oq_pade_vgl_q((T)J.j1a[I], (T)J.j1b[I], r2t * rinv, rinv, upr, l);
-      jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
+      const double u = (double)upr;
+      gx += u * dx; gy += u * dy; gz += u * dz; jl += l;
     }
     if (S.has_bs1 && S.bs1_type[I] >= 0) {
       const int ty = S.bs1_type[I];
       T upr, l;
       oq_bs_vgl<T>(S.bs1_c[ty], S.bs1_n[ty], (T)S.bs1_dinv[ty], (T)S.bs1_rcut[ty], r2t * rinv,
                    rinv, upr, l);
-      jx += upr * (T)dx; jy += upr * (T)dy; jz += upr * (T)dz; jl += l;
+      const double u = (double)upr;
+      gx += u * dx; gy += u * dy; gz += u * dz; jl += l;
     }
   }
+  if (sizeof(T) != 8) {
+    ee += (double)eet;
+    en += (double)ent;
+  }
+  jx += (T)gx; jy += (T)gy; jz += (T)gz;
   if (S.has_j3) oq_j3_vgl_electron<T>(S, pos, ps, NE, e, xe, ye, ze, jx, jy, jz, jl);
 }
 

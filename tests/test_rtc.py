@@ -67,3 +67,24 @@ def test_tuned_batch_module_compiles_for_sm100a():
     assert ok, log
     ok0, _, cubin0 = R.compile_source(src, R.BATCH_KERNELS[:1])
     assert ok0 and len(cubin) < len(cubin0)
+
+
+def test_generated_code_leaves_out_round_off_coefficients():
+    """H2O (C2v) orbitals have exact zeros on the AOs of other irreducible
+    representations, which the eigensolver returns at ~1e-15: the generated
+    MO-value code evaluates only the coefficients above 1e-12 of their
+    orbital's largest one, and the benchmark's flop model counts the same."""
+    import re
+    import numpy as np
+    import bench
+    mf = M.make_mf("H2O")
+    s = build_system(mf, M.benchmark_params_corr(mf.mol))
+    src = R.spec_source(s)
+    mo_val = src.split("mo_vgl(")[0]
+    kept = re.findall(r"mv\[\d+\] \+= \(T\)\(([-0-9.eE+]+)\)", mo_val)
+    C = np.abs(np.asarray(s.C))
+    assert len(kept) == bench.mo_terms(s) < C.size
+    assert min(abs(float(c)) for c in kept) > 1e-6
+    # the dropped ones are round-off: below 1e-12 of their orbital's scale
+    small = C[(C > 0) & (C <= 1e-12 * C.max(axis=0, keepdims=True))]
+    assert small.size == C.size - len(kept) - np.count_nonzero(C == 0)
