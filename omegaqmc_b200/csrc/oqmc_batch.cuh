@@ -196,29 +196,32 @@ __device__ __forceinline__ int oq_batch_sweep_lanes(const OqBatchArgs& a, const 
                                                     const OqSplit& SP, const Real* C,
                                                     double* pos, Real* Ai, int WT, int wl,
                                                     int lane, int P, bool live, uint32_t w,
-                                                    uint32_t gstep, double& logdet) {
+                                                    uint32_t gstep, const OqScaledF& pf,
+                                                    double& logdet) {
   constexpr int NE = 2 * NOCC;
   constexpr int NN = NOCC * NOCC;
   int nacc = 0;
   for (int e0 = 0; e0 < NE; e0 += P) {
     // this lane's electron of the block: proposal and orbital row
     const int e = e0 + lane;
-    double nx = 0.0, ny = 0.0, nz = 0.0, u = 2.0, mul = 1.0, lx = 0.0;
+    double nx = 0.0, ny = 0.0, nz = 0.0;
+    T u = (T)2, mul = (T)1, lx = (T)0;
     T v[NOCC];
 #pragma unroll
     for (int m = 0; m < NOCC; ++m) v[m] = (T)0;
     if (live && e < NE) {
-      double n3[3];
-      oq_move_randoms(a.seed, w, gstep, (uint32_t)e, n3, u);
+      float nf[3];
+      uint32_t ub;
+      oq_move_normals(a.seed, w, gstep, (uint32_t)e, nf, ub);
+      u = oq_uniform<T>(ub);
       const double ox = pos[(3 * e) * WT + wl], oy = pos[(3 * e + 1) * WT + wl],
                    oz = pos[(3 * e + 2) * WT + wl];
       if (d.proposal == 0) {
-        nx = ox + d.step * n3[0];
-        ny = oy + d.step * n3[1];
-        nz = oz + d.step * n3[2];
+        nx = ox + d.step * (double)nf[0];
+        ny = oy + d.step * (double)nf[1];
+        nz = oz + d.step * (double)nf[2];
       } else {
-        oq_scaled_propose(J, ox, oy, oz, n3, d.step, d.scale_r0, d.scale_fmin, nx, ny, nz, mul,
-                          lx);
+        oq_scaled_propose_t<T>(J, ox, oy, oz, nf, pf, nx, ny, nz, mul, lx);
       }
       B::template mo_val<T, Real>(S, SP, C, nx, ny, nz, v);
     }
@@ -229,9 +232,9 @@ __device__ __forceinline__ int oq_batch_sweep_lanes(const OqBatchArgs& a, const 
       const double bx = __shfl_sync(0xffffffffu, nx, q, P);
       const double by = __shfl_sync(0xffffffffu, ny, q, P);
       const double bz = __shfl_sync(0xffffffffu, nz, q, P);
-      const double bu = __shfl_sync(0xffffffffu, u, q, P);
-      const double bmul = __shfl_sync(0xffffffffu, mul, q, P);
-      const double blx = __shfl_sync(0xffffffffu, lx, q, P);
+      const T bu = __shfl_sync(0xffffffffu, u, q, P);
+      const T bmul = __shfl_sync(0xffffffffu, mul, q, P);
+      const T blx = __shfl_sync(0xffffffffu, lx, q, P);
       T bv[NOCC];
 #pragma unroll
       for (int m = 0; m < NOCC; ++m) bv[m] = __shfl_sync(0xffffffffu, v[m], q, P);
@@ -250,12 +253,7 @@ __device__ __forceinline__ int oq_batch_sweep_lanes(const OqBatchArgs& a, const 
         coli[k] = (T)As[(k * NOCC + i) * WT + wl];
         R += bv[k] * coli[k];
       }
-      const double Rd = (double)R;
-      const double ex = (sizeof(T) == 8) ? exp(2.0 * (double)dJ + blx)
-                                         : (double)expf((float)(2.0 * (double)dJ + blx));
-      const double ratio = Rd * Rd * bmul * ex;
-      const bool acc = live && valid && (Rd != 0.0) && isfinite(Rd) && isfinite((double)dJ) &&
-                       isfinite(blx) && (bu < ratio);
+      const bool acc = live && oq_accept<T>(R, dJ, blx, bmul, bu, valid);
       // every lane has read column i before any lane updates it
       __syncwarp();
       if (acc) {
@@ -277,7 +275,7 @@ __device__ __forceinline__ int oq_batch_sweep_lanes(const OqBatchArgs& a, const 
           pos[(3 * ee + 2) * WT + wl] = bz;
           ++nacc;
         }
-        logdet += log(fabs(Rd));
+        logdet += log(fabs((double)R));
       }
       // the move is visible to every lane before the next one
       __syncwarp();
@@ -359,32 +357,39 @@ __device__ __forceinline__ void oq_batch_tile(const OqBatchArgs& a, const OqBatc
   }
   __syncthreads();
   int nacc = 0, meas = 0;
+  const OqScaledF pf = oq_scaled_f(d.step, d.scale_r0, d.scale_fmin);
   for (int t = 0; t < a.n_sweeps; ++t) {
     const uint32_t gstep = (uint32_t)(step0 + t);
     if (MODE != 1 && P > 1) {
       nacc += oq_batch_sweep_lanes<NOCC, T, Real, B>(a, d, J, S, SP, C, pos, Ai, WT, wl, lane,
-                                                     P, live, (uint32_t)w, gstep, logdet);
+                                                     P, live, (uint32_t)w, gstep, pf, logdet);
     } else if (MODE != 2 && live) {
       for (int e = 0; e < NE; ++e) {
-        double n3[3], u;
-        oq_move_randoms(a.seed, (uint32_t)w, gstep, (uint32_t)e, n3, u);
+        float nf[3];
+        uint32_t ub;
+        oq_move_normals(a.seed, (uint32_t)w, gstep, (uint32_t)e, nf, ub);
+        const T u = oq_uniform<T>(ub);
         const double ox = pos[(3 * e) * WT + wl], oy = pos[(3 * e + 1) * WT + wl],
                      oz = pos[(3 * e + 2) * WT + wl];
         if (d.proposal == 0) {
           nacc += oq_try_move<NOCC, T, Real, B>(J, S, SP, C, pos, Ai, WT, wl, e,
-                                                ox + d.step * n3[0], oy + d.step * n3[1],
-                                                oz + d.step * n3[2], 0.0, 1.0, u, logdet);
+                                                ox + d.step * (double)nf[0],
+                                                oy + d.step * (double)nf[1],
+                                                oz + d.step * (double)nf[2], (T)0, (T)1, u,
+                                                logdet);
         } else {
-          double nx, ny, nz, mul, lx;
-          oq_scaled_propose(J, ox, oy, oz, n3, d.step, d.scale_r0, d.scale_fmin, nx, ny, nz, mul,
-                            lx);
+          double nx, ny, nz;
+          T mul, lx;
+          oq_scaled_propose_t<T>(J, ox, oy, oz, nf, pf, nx, ny, nz, mul, lx);
           nacc += oq_try_move<NOCC, T, Real, B>(J, S, SP, C, pos, Ai, WT, wl, e, nx, ny, nz, lx,
                                                 mul, u, logdet);
         }
       }
     }
     if ((t + 1) % a.measure_every != 0) continue;
-    __syncthreads();
+    // a walker's state is read and written only by its own lanes, which
+    // share one warp: the moves are complete for them after a warp barrier
+    __syncwarp();
     // local energy: electrons e = lane, lane + P, ... of walker wl
     double see = 0.0, sen = 0.0, slp = 0.0, sg2 = 0.0;
     if (live)

@@ -140,29 +140,54 @@ __device__ __forceinline__ double oq_u01(uint32_t v) {
   return ((double)v + 1.0) * 2.3283064365386963e-10;
 }
 
-// Three standard normals and one uniform for a single-electron proposal
-// from one Philox4x32-10 block, counter = (walker, step, electron, 0), key =
-// seed.  Box-Muller in FP32 on the top 24 bits of the four words (the
-// deviates only set proposal widths, 24-bit resolution is ample and the FP32
-// transcendental units are cheap); the acceptance uniform from the four low
-// bytes, bits disjoint from those, so all deviates are independent.
+// Three standard normals and the 32 bits of the acceptance uniform for a
+// single-electron proposal from one Philox4x32-10 block, counter = (walker,
+// step, electron, 0), key = seed.  Box-Muller in FP32 on the top 23 bits of
+// the four words (the deviates only set proposal widths, 23-bit resolution
+// is ample and the FP32 transcendental units are cheap; square roots by
+// sqrt.approx); the uniform's bits are the four low bytes, disjoint from
+// those, so all deviates are independent.
+__device__ __forceinline__ void oq_move_normals(uint64_t seed, uint32_t walker, uint32_t step,
+                                                uint32_t elec, float nf[3], uint32_t& ubits) {
+  const OqU4 c0 = {walker, step, elec, 0u};
+  const OqU4 r0 = oq_philox(c0, (uint32_t)seed, (uint32_t)(seed >> 32));
+  // uniforms from the top 23 bits of each word as the mantissa of a float
+  // in [1, 2) (no conversion instruction): m - 1 in [0, 1), 2 - m in (0, 1]
+  auto m = [](uint32_t v) { return __uint_as_float(0x3f800000u | (v >> 9)); };
+  float a, b;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(a) : "f"(-2.0f * __logf(2.0f - m(r0.x))));
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(b) : "f"(-2.0f * __logf(2.0f - m(r0.z))));
+  float s, c;
+  __sincosf(6.283185307179586f * (m(r0.y) - 1.0f), &s, &c);
+  const float c2 = __cosf(6.283185307179586f * (m(r0.w) - 1.0f));   // third normal only
+  nf[0] = a * c;
+  nf[1] = a * s;
+  nf[2] = b * c2;
+  ubits = ((r0.x & 255u) << 24) | ((r0.y & 255u) << 16) | ((r0.z & 255u) << 8) | (r0.w & 255u);
+}
+
+// The acceptance uniform in [0, 1) in the working precision: all 32 bits in
+// FP64; in FP32 the top 23 bits as the mantissa of a float in [1, 2) minus 1
+// (no conversion instruction).  Both compare u < ratio on the same bits.
+template <typename T> __device__ __forceinline__ T oq_uniform(uint32_t ubits);
+template <> __device__ __forceinline__ double oq_uniform<double>(uint32_t ubits) {
+  return (double)ubits * 2.3283064365386963e-10;
+}
+template <> __device__ __forceinline__ float oq_uniform<float>(uint32_t ubits) {
+  return __uint_as_float(0x3f800000u | (ubits >> 9)) - 1.0f;
+}
+
+// The normals and the uniform as doubles (the FP64 proposals).
 __device__ __forceinline__ void oq_move_randoms(uint64_t seed, uint32_t walker,
                                                 uint32_t step, uint32_t elec,
                                                 double n3[3], double& u) {
-  const OqU4 c0 = {walker, step, elec, 0u};
-  const OqU4 r0 = oq_philox(c0, (uint32_t)seed, (uint32_t)(seed >> 32));
-  const float k24 = 5.9604644775390625e-08f;                  // 2^-24
-  const float a = sqrtf(-2.0f * __logf(((float)(r0.x >> 8) + 1.0f) * k24));   // (0, 1]
-  const float b = sqrtf(-2.0f * __logf(((float)(r0.z >> 8) + 1.0f) * k24));
-  float s, c;
-  __sincosf(6.283185307179586f * ((float)(r0.y >> 8) * k24), &s, &c);
-  const float c2 = __cosf(6.283185307179586f * ((float)(r0.w >> 8) * k24));   // third normal only
-  n3[0] = (double)(a * c);
-  n3[1] = (double)(a * s);
-  n3[2] = (double)(b * c2);
-  const uint32_t lo = ((r0.x & 255u) << 24) | ((r0.y & 255u) << 16) | ((r0.z & 255u) << 8) |
-                      (r0.w & 255u);
-  u = (double)lo * 2.3283064365386963e-10;                     // in [0, 1)
+  float nf[3];
+  uint32_t ubits;
+  oq_move_normals(seed, walker, step, elec, nf, ubits);
+  n3[0] = (double)nf[0];
+  n3[1] = (double)nf[1];
+  n3[2] = (double)nf[2];
+  u = oq_uniform<double>(ubits);
 }
 
 // reciprocal / reciprocal square root in the working precision; in FP32 the

@@ -259,11 +259,11 @@ k_moves_mlp(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gspli
         bool acc;
         if (TA)
           acc = oq_try_move_s<NOCC, float, float, B>(J, S, SP, C, posd + r, 128, Ai + w, W, e,
-                                                     nx, ny, nz, (double)(lqr - lqf), 1.0, u,
+                                                     nx, ny, nz, lqr - lqf, 1.0f, (float)u,
                                                      logdet);
         else
           acc = oq_try_move<NOCC, float, float, B>(J, S, SP, C, pos, Ai, W, w, e, nx, ny, nz,
-                                                   (double)(lqr - lqf), 1.0, u, logdet);
+                                                   lqr - lqf, 1.0f, (float)u, logdet);
         nacc += acc;
         if (POSF && acc) {
           posf[(3 * e) * 128 + r] = (float)nx;

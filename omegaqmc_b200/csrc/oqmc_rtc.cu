@@ -156,7 +156,8 @@ struct Gen {
       if ((sel == 1 && !tight(g, p)) || (sel == 2 && tight(g, p))) continue;
       const double a = S.alpha[off + p];
       if (tight_arg && tight(g, p))   // FP64 argument, see oq_exp_tight
-        add("      { const " + ty + " e = oq_exp_tight<" + ty + ">(" + num(a) + " * r2d);\n");
+        add("      { const " + ty + " e = oq_exp_tight<" + ty + ">(" + num(a) + ", " +
+            num(a * 1.4426950408889634) + ", r2d);\n");
       else if (ty == "double")
         add("      { const double e = exp(-((double)" + num(a) + ") * " + r2 + ");\n");
       else   // a and a log2(e) folded here, see oq_exp_neg
@@ -180,23 +181,19 @@ struct Gen {
       }
   }
 
+  // ca = sum_m C[ao][m] ac[m] over the kept coefficients ("" when none)
+  std::string ca_expr(int ao) {
+    std::string ca;
+    for (int m = 0; m < nocc; ++m) {
+      if (!keep(ao, m)) continue;
+      ca += std::string(ca.empty() ? "" : " + ") + "(T)(" + num(C[ao * nocc + m]) + ") * ac[" +
+            std::to_string(m) + "]";
+    }
+    return ca;
+  }
+
   // accumulate one AO into the MOs (value expression v; grad g[3], lap l)
   void accum(int ao, const std::string& v, const std::string* g, const std::string* l) {
-    if (contract) {
-      // ca = sum_m C[ao][m] ac[m], then the AO's gradient and Laplacian
-      // weighted by ca: one contraction per AO instead of one per MO
-      std::string ca;
-      for (int m = 0; m < nocc; ++m) {
-        const double c = C[ao * nocc + m];
-        if (!keep(ao, m)) continue;
-        ca += std::string(ca.empty() ? "" : " + ") + "(T)(" + num(c) + ") * ac[" +
-              std::to_string(m) + "]";
-      }
-      if (ca.empty()) return;
-      add("      { const T ca = " + ca + ";\n        gx += ca * " + g[0] + "; gy += ca * " + g[1] +
-          "; gz += ca * " + g[2] + "; lp += ca * " + *l + "; }\n");
-      return;
-    }
     for (int m = 0; m < nocc; ++m) {
       const double c = C[ao * nocc + m];
       if (!keep(ao, m)) continue;
@@ -215,6 +212,10 @@ struct Gen {
                const std::string& Rl) {
     const int am = S.g_am[g];
     const int ao = S.s_ao[S.g_shell0[g] + k];
+    if (contract) {
+      angular_contract(am, ao, R, Rp, Rl);
+      return;
+    }
     add("    {\n");
     if (am == 0) {
       if (!vgl) {
@@ -231,7 +232,7 @@ struct Gen {
         std::string Y, d0, d1, d2;
         if (am == 1) {
           Y = c == 0 ? "dx" : c == 1 ? "dy" : "dz";
-          d0 = c == 0 ? "(T)1" : "(T)0"; d1 = c == 1 ? "(T)1" : "(T)0"; d2 = c == 2 ? "(T)1" : "(T)0";
+          d0 = c == 0 ? "(T)1" : ""; d1 = c == 1 ? "(T)1" : ""; d2 = c == 2 ? "(T)1" : "";
         } else if (am == 2) {
           Y = "Y[" + cs + "]"; d0 = "dY[" + cs + "][0]"; d1 = "dY[" + cs + "][1]"; d2 = "dY[" + cs + "][2]";
         } else {
@@ -242,14 +243,79 @@ struct Gen {
         if (!vgl) {
           accum(ao + c, "(" + R + " * " + Y + ")", nullptr, nullptr);
         } else {
-          std::string gg[3] = {"(" + Rp + " * dx * " + Y + " + " + R + " * " + d0 + ")",
-                               "(" + Rp + " * dy * " + Y + " + " + R + " * " + d1 + ")",
-                               "(" + Rp + " * dz * " + Y + " + " + R + " * " + d2 + ")"};
+          // (a p function's gradient has R in one component only: no R * 0 terms)
+          auto term = [&](const char* dc, const std::string& dy) {
+            return "(" + Rp + " * " + dc + " * " + Y + (dy.empty() ? "" : " + " + R + " * " + dy) +
+                   ")";
+          };
+          std::string gg[3] = {term("dx", d0), term("dy", d1), term("dz", d2)};
           std::string ll = "(lfac * " + Y + ")";
           accum(ao + c, "(" + R + " * " + Y + ")", gg, &ll);
         }
       }
     }
+    add("    }\n");
+  }
+
+  // Contracted VGL of one shell column (angular momentum am, AOs ao ...
+  // ao + 2 am): with c_q = ca of AO q, A = sum_q c_q Y_q and G = sum_q c_q
+  // grad Y_q, the column adds Rp A d to the gradient (summed per nucleus in
+  // sR, multiplied by d once), R G to the gradient and (Rl + 2 am Rp) A to
+  // the Laplacian (solid harmonics have no Laplacian of their own).  Columns
+  // whose AOs no kept coefficient reaches are left out.
+  void angular_contract(int am, int ao, const std::string& R, const std::string& Rp,
+                        const std::string& Rl) {
+    const int nq = 2 * am + 1;
+    std::vector<std::string> cq(nq);
+    bool any = false;
+    for (int q = 0; q < nq; ++q) {
+      cq[q] = ca_expr(ao + q);
+      any = any || !cq[q].empty();
+    }
+    if (!any) return;
+    add("    {\n");
+    if (am == 0) {
+      add("      const T c0 = " + cq[0] + ";\n      sR += " + Rp + " * c0; lp += " + Rl +
+          " * c0;\n    }\n");
+      return;
+    }
+    for (int q = 0; q < nq; ++q)
+      if (!cq[q].empty()) add("      const T c" + std::to_string(q) + " = " + cq[q] + ";\n");
+    std::string A, G[3];
+    auto plus = [](std::string& acc, const std::string& t) {
+      acc += (acc.empty() ? "" : " + ") + t;
+    };
+    if (am == 1) {
+      const char* dn[3] = {"dx", "dy", "dz"};
+      for (int q = 0; q < 3; ++q)
+        if (!cq[q].empty()) {
+          plus(A, "c" + std::to_string(q) + " * " + dn[q]);
+          G[q] = "c" + std::to_string(q);
+        }
+    } else {
+      if (am == 2) add("      T Y[5], dY[5][3]; oq_harm_d<T>(dx, dy, dz, Y, dY);\n");
+      for (int q = 0; q < nq; ++q) {
+        if (cq[q].empty()) continue;
+        const std::string qs = std::to_string(q), cn = "c" + qs;
+        std::string Y, dY;
+        if (am == 2) {
+          Y = "Y[" + qs + "]";
+          dY = "dY[" + qs + "]";
+        } else {
+          add("      T Y" + qs + ", dY" + qs + "[3]; oq_harm_table<T>(S.harm, " +
+              std::to_string(am) + ", " + qs + ", dx, dy, dz, Y" + qs + ", dY" + qs + ");\n");
+          Y = "Y" + qs;
+          dY = "dY" + qs;
+        }
+        plus(A, cn + " * " + Y);
+        for (int j = 0; j < 3; ++j) plus(G[j], cn + " * " + dY + "[" + std::to_string(j) + "]");
+      }
+    }
+    add("      const T A = " + A + ";\n      sR += " + Rp + " * A; lp += (" + Rl + " + (T)" +
+        std::to_string(2 * am) + " * " + Rp + ") * A;\n");
+    const char* gn[3] = {"gx", "gy", "gz"};
+    for (int j = 0; j < 3; ++j)
+      if (!G[j].empty()) add("      " + std::string(gn[j]) + " += " + R + " * (" + G[j] + ");\n");
     add("    }\n");
   }
 
@@ -271,6 +337,7 @@ struct Gen {
           num(S.nuc[ia][1]) + "), dzd = z - (" + num(S.nuc[ia][2]) + ");\n"
           "  const double r2d = dxd * dxd + dyd * dyd + dzd * dzd;\n"
           "  const T dx = (T)dxd, dy = (T)dyd, dz = (T)dzd, r2 = (T)r2d;\n  (void)r2;\n");
+      if (contract) add("  T sR = (T)0;\n");
       for (int g = 0; g < S.ngroup; ++g) {
         if (S.g_iat[g] != ia) continue;
         const int nc = S.g_ncol[g], sh0 = S.g_shell0[g];
@@ -343,6 +410,7 @@ struct Gen {
         }
         add("  }\n");
       }
+      if (contract) add("  gx += sR * dx; gy += sR * dy; gz += sR * dz;\n");
       add("  }\n");
     }
   }

@@ -44,22 +44,27 @@ template <> __device__ __forceinline__ float oq_exp_neg<float>(float, float al2,
   return p;
 }
 
-// exp(-arg) for a tight exponent, arg = alpha r^2 formed in FP64.  In FP32
-// the rounding of a large argument would dominate the error, so the FP64
-// argument is split as arg log2(e) = k + f (k integer, f in [0, 1)) and only
-// 2^-f is evaluated in FP32, then scaled by 2^-k: FP32 relative accuracy for
+// exp(-a r2d) for a tight exponent a, the argument formed in FP64 (in FP32
+// the rounding of a large argument would dominate the error), given a and
+// al2 = a log2(e) as literals.  FP32 form: t = al2 r2d = k + f with k the
+// nearest integer, taken by adding 1.5 * 2^52 (t < 2^51, so the sum is an
+// integer whose low word is k: no conversion instruction) and f = t - k in
+// [-1/2, 1/2] exactly; only 2^-f is evaluated in FP32 (ex2.approx), then
+// scaled by 2^-k through the exponent field.  FP32 relative accuracy for
 // every argument, without an FP64 exponential or a branch.
-template <typename T> __device__ __forceinline__ T oq_exp_tight(double arg);
-template <> __device__ __forceinline__ double oq_exp_tight<double>(double arg) {
-  return exp(-arg);
+template <typename T> __device__ __forceinline__ T oq_exp_tight(double a, double al2, double r2d);
+template <> __device__ __forceinline__ double oq_exp_tight<double>(double a, double, double r2d) {
+  return exp(-(a * r2d));
 }
-template <> __device__ __forceinline__ float oq_exp_tight<float>(double arg) {
-  const double t = arg * 1.4426950408889634;        // >= 0
-  const int k = (int)fmin(t, 126.0);                 // truncation = floor here
-  const float f = (float)(t - (double)k);            // in [0, 1) (or >= 1 past 2^-126)
+template <> __device__ __forceinline__ float oq_exp_tight<float>(double, double al2, double r2d) {
+  const double shift = 6755399441055744.0;                    // 1.5 * 2^52
+  const double t = fmin(al2 * r2d, 125.0);                    // >= 0; 2^-125 is a normal float
+  const double y = t + shift;
+  const int k = __double2loint(y);                            // round(t), in [0, 125]
+  const float f = (float)(t - (y - shift));                  // exact, in [-1/2, 1/2]
   float p;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(p) : "f"(-f));
-  return p * __int_as_float((127 - k) << 23);        // 2^-k, a normal float for k <= 126
+  return p * __int_as_float((127 - k) << 23);                // 2^-k
 }
 
 // per-group "tight" split radius squared (FP64 evaluation inside it);
@@ -454,40 +459,82 @@ struct OqMoveArgs {
                           // adaptation, oqmc_equilibrate); else `step`
 };
 
-// Proposal width at x for the nucleus-scaled Gaussian move.
+// The nucleus-scaled proposal's constants in FP32 (set once per launch or tile).
+struct OqScaledF {
+  float step, inv_r0, fmin;
+};
+__device__ __forceinline__ OqScaledF oq_scaled_f(double step, double r0, double fmn) {
+  return {(float)step, 1.0f / (float)r0, (float)fmn};
+}
+
+// Proposal width at x for the nucleus-scaled Gaussian move,
+// sigma(x) = step * clamp(r_near(x) / r0, fmin, 1): the nearest nucleus's
+// squared distance in FP64, then sqrt.approx, the clamp and the product in
+// FP32.  The width only has to be the same function of position on both
+// sides of the ratio; the FP64 and the mixed samplers use this same
+// function, so for the same random numbers they propose the same positions.
 template <class SJ>
-__device__ __forceinline__ double oq_scaled_width(const SJ& S, double x, double y,
-                                                  double z, double step, double r0,
-                                                  double fmn) {
+__device__ __forceinline__ float oq_scaled_width_f(const SJ& S, double x, double y, double z,
+                                                   const OqScaledF& p) {
   double r2 = 1e300;
   for (int I = 0; I < S.natm; ++I) {
     const double dx = x - S.nuc[I][0], dy = y - S.nuc[I][1], dz = z - S.nuc[I][2];
     r2 = fmin(r2, dx * dx + dy * dy + dz * dz);
   }
-  // the width only has to be the same function of position on both sides
-  // of the ratio, so its square root runs in FP32
-  const double f = (double)(sqrtf((float)r2) / (float)r0);
-  return step * fmin(1.0, fmax(fmn, f));
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"((float)r2));
+  return p.step * fminf(1.0f, fmaxf(p.fmin, r * p.inv_r0));
 }
 
-// Nucleus-scaled Gaussian proposal from (ox, oy, oz) with standard normals
-// n3: the new position and the proposal-density ratio q(old | new) /
-// q(new | old) = (so / sn)^3 exp(d^2 (1 / so^2 - 1 / sn^2) / 2), returned as
-// a factor mul and an exponent lx (no logarithm on the move path).
 template <class SJ>
-__device__ __forceinline__ void oq_scaled_propose(const SJ& S, double ox, double oy, double oz,
-                                                  const double n3[3], double step, double r0,
-                                                  double fmn, double& nx, double& ny,
-                                                  double& nz, double& mul, double& lx) {
-  const double so = oq_scaled_width(S, ox, oy, oz, step, r0, fmn);
-  nx = ox + so * n3[0];
-  ny = oy + so * n3[1];
-  nz = oz + so * n3[2];
-  const double sn = oq_scaled_width(S, nx, ny, nz, step, r0, fmn);
-  // with d = so n3: d^2 (1 / so^2 - 1 / sn^2) = |n3|^2 (1 - q^2), q = so / sn
-  const double q = so / sn;
-  mul = q * q * q;
-  lx = 0.5 * (n3[0] * n3[0] + n3[1] * n3[1] + n3[2] * n3[2]) * (1.0 - q * q);
+__device__ __forceinline__ double oq_scaled_width(const SJ& S, double x, double y,
+                                                  double z, double step, double r0,
+                                                  double fmn) {
+  return (double)oq_scaled_width_f(S, x, y, z, oq_scaled_f(step, r0, fmn));
+}
+
+// Nucleus-scaled Gaussian proposal from (ox, oy, oz) with the FP32 standard
+// normals nf: the new position (FP64) and the proposal-density ratio
+// q(old | new) / q(new | old) = (so / sn)^3 exp(d^2 (1 / so^2 - 1 / sn^2) / 2),
+// with d = so n: (so / sn)^3 exp(|n|^2 (1 - (so / sn)^2) / 2), returned as a
+// factor mul and an exponent lx (no logarithm on the move path), in the
+// working precision T (FP32 in the mixed build: its rounding, ~1e-7
+// relative, is far below any statistical resolution).
+template <typename T, class SJ>
+__device__ __forceinline__ void oq_scaled_propose_t(const SJ& S, double ox, double oy, double oz,
+                                                    const float nf[3], const OqScaledF& pf,
+                                                    double& nx, double& ny, double& nz, T& mul,
+                                                    T& lx) {
+  const float so = oq_scaled_width_f(S, ox, oy, oz, pf);
+  const double sod = (double)so;
+  nx = ox + sod * (double)nf[0];
+  ny = oy + sod * (double)nf[1];
+  nz = oz + sod * (double)nf[2];
+  const float sn = oq_scaled_width_f(S, nx, ny, nz, pf);
+  if (sizeof(T) == 8) {
+    const double q = sod / (double)sn;
+    const double n2 = (double)nf[0] * (double)nf[0] + (double)nf[1] * (double)nf[1] +
+                      (double)nf[2] * (double)nf[2];
+    mul = (T)(q * q * q);
+    lx = (T)(0.5 * n2 * (1.0 - q * q));
+  } else {
+    const float q = so * oq_rcp(sn);
+    mul = (T)(q * q * q);
+    lx = (T)(0.5f * (nf[0] * nf[0] + nf[1] * nf[1] + nf[2] * nf[2]) * (1.0f - q * q));
+  }
+}
+
+// The Metropolis-Hastings test u < |R|^2 exp(2 dJ + log_extra) mul_extra in
+// the working precision T (FP32 in the mixed build: the accurate expf, whose
+// ~1e-7 relative error moves acceptance probabilities far below any
+// statistical resolution), without logarithms.
+template <typename T>
+__device__ __forceinline__ bool oq_accept(T R, T dJ, T log_extra, T mul_extra, T u, bool valid) {
+  const T ex = (sizeof(T) == 8) ? (T)exp((double)((T)2 * dJ + log_extra))
+                                : (T)expf((float)((T)2 * dJ + log_extra));
+  const T ratio = R * R * mul_extra * ex;
+  return valid && (R != (T)0) && isfinite(R) && isfinite(dJ) && isfinite(log_extra) &&
+         (u < ratio);
 }
 
 // Change of the Jastrow factor (arithmetic in T) when electron e moves from
@@ -566,8 +613,8 @@ template <int NOCC, typename T, typename Real, class B, class SJ>
 __device__ __forceinline__ bool oq_try_move_s(const SJ& J, const OqSystem& S, const OqSplit& SP,
                                               const Real* __restrict__ C, double* pos, int ps,
                                               Real* A, int as, int e, double nx, double ny,
-                                              double nz, double log_extra, double mul_extra,
-                                              double u, double& logdet) {
+                                              double nz, T log_extra, T mul_extra, T u,
+                                              double& logdet) {
   constexpr int NE = 2 * NOCC;
   constexpr int NN = NOCC * NOCC;
   const int s = e & 1, i = e >> 1;
@@ -582,15 +629,7 @@ __device__ __forceinline__ bool oq_try_move_s(const SJ& J, const OqSystem& S, co
   T R = (T)0;
 #pragma unroll
   for (int m = 0; m < NOCC; ++m) R += v[m] * (T)As[(m * NOCC + i) * as];
-  const double Rd = (double)R;
-  // the exponential in the working precision (accurate expf in FP32: its
-  // ~1e-7 relative error moves acceptance probabilities far below any
-  // statistical resolution)
-  const double ex = (sizeof(T) == 8) ? exp(2.0 * (double)dJ + log_extra)
-                                     : (double)expf((float)(2.0 * (double)dJ + log_extra));
-  const double ratio = Rd * Rd * mul_extra * ex;
-  const bool acc = valid && (Rd != 0.0) && isfinite(Rd) && isfinite((double)dJ) &&
-                   isfinite(log_extra) && (u < ratio);
+  const bool acc = oq_accept<T>(R, dJ, log_extra, mul_extra, u, valid);
   if (acc) {
     // Sherman-Morrison with the ratio vector w_j = sum_m v_m A[m][j]:
     // A[k][j] -= A[k][i] (w_j - delta_ij) / R, column i taken before the update
@@ -613,7 +652,7 @@ __device__ __forceinline__ bool oq_try_move_s(const SJ& J, const OqSystem& S, co
     pos[(3 * e) * ps] = nx;
     pos[(3 * e + 1) * ps] = ny;
     pos[(3 * e + 2) * ps] = nz;
-    logdet += log(fabs(Rd));
+    logdet += log(fabs((double)R));
   }
   return acc;
 }
@@ -625,7 +664,7 @@ __device__ __forceinline__ bool oq_try_move(const SJ& J, const OqSystem& S, cons
                                             const Real* __restrict__ C, double* pos,
                                             Real* Ai, int WPB, int tid, int e,
                                             double nx, double ny, double nz,
-                                            double log_extra, double mul_extra, double u,
+                                            T log_extra, T mul_extra, T u,
                                             double& logdet) {
   return oq_try_move_s<NOCC, T, Real, B>(J, S, SP, C, pos + tid, WPB, Ai + tid, WPB, e, nx, ny,
                                          nz, log_extra, mul_extra, u, logdet);
@@ -715,40 +754,43 @@ k_moves(const OqSystem* __restrict__ gsys, const OqSplit* __restrict__ gsplit,
   }
   __syncthreads();
   const double step = a.step_dev ? *a.step_dev : a.step;
+  const OqScaledF pf = oq_scaled_f(step, a.scale_r0, a.scale_fmin);
   double logdet = live ? a.logdet[w] : 0.0;
   int nacc = 0;
   for (int t = 0; t < (live ? a.n_steps : 0); ++t) {
     const uint32_t gstep = (uint32_t)(a.step_base + t);
     if (PROP == 0) {
       for (int e = 0; e < NE; ++e) {
-        double n3[3], u;
-        oq_move_randoms(a.seed, (uint32_t)w, gstep, (uint32_t)e, n3, u);
-        const double nx = pos[(3 * e) * WPB + tid] + step * n3[0];
-        const double ny = pos[(3 * e + 1) * WPB + tid] + step * n3[1];
-        const double nz = pos[(3 * e + 2) * WPB + tid] + step * n3[2];
-        nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz, 0.0,
-                                           1.0, u, logdet);
+        float nf[3];
+        uint32_t ub;
+        oq_move_normals(a.seed, (uint32_t)w, gstep, (uint32_t)e, nf, ub);
+        const double nx = pos[(3 * e) * WPB + tid] + step * (double)nf[0];
+        const double ny = pos[(3 * e + 1) * WPB + tid] + step * (double)nf[1];
+        const double nz = pos[(3 * e + 2) * WPB + tid] + step * (double)nf[2];
+        nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
+                                           (T)0, (T)1, oq_uniform<T>(ub), logdet);
       }
     } else if (PROP == 1) {
       // nucleus-scaled Gaussian: sigma(x) = step * clamp(r_near(x)/r0, fmin, 1);
       // exact MH with log q(x|x') - log q(x'|x) for the asymmetric proposal
       for (int e = 0; e < NE; ++e) {
-        double n3[3], u;
-        oq_move_randoms(a.seed, (uint32_t)w, gstep, (uint32_t)e, n3, u);
+        float nf[3];
+        uint32_t ub;
+        oq_move_normals(a.seed, (uint32_t)w, gstep, (uint32_t)e, nf, ub);
         const double ox = pos[(3 * e) * WPB + tid], oy = pos[(3 * e + 1) * WPB + tid],
                      oz = pos[(3 * e + 2) * WPB + tid];
-        double nx, ny, nz, mul, lx;
-        oq_scaled_propose(S, ox, oy, oz, n3, step, a.scale_r0, a.scale_fmin, nx, ny, nz, mul,
-                          lx);
+        double nx, ny, nz;
+        T mul, lx;
+        oq_scaled_propose_t<T>(S, ox, oy, oz, nf, pf, nx, ny, nz, mul, lx);
         nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz, lx,
-                                           mul, u, logdet);
+                                           mul, oq_uniform<T>(ub), logdet);
       }
     } else {
       double u, nx, ny, nz, log_qratio;
       const int e = oq_basin_propose<NE>(S, pos + tid, WPB, a.seed, (uint32_t)w, gstep, step,
                                          nx, ny, nz, log_qratio, u);
       nacc += oq_try_move<NOCC, T, Real, B>(S, S, SP, C, pos, Ai, WPB, tid, e, nx, ny, nz,
-                                         log_qratio, 1.0, u, logdet);
+                                         (T)log_qratio, (T)1, (T)u, logdet);
     }
   }
   if (live) {
