@@ -102,6 +102,9 @@ def parse():
                          "under a CUDA graph; split: separate move / local-energy kernels")
     ap.add_argument("--quick", action="store_true",
                     help="profiling mode: no equilibration, comparison, e2e or CPU legs")
+    ap.add_argument("--generic", action="store_true",
+                    help="split path only: the table-driven kernels (no per-molecule NVRTC "
+                         "specialisation), the library's path where NVRTC is absent")
     return ap.parse_args()
 
 
@@ -396,7 +399,8 @@ def run_ours(a):
     system = build_system(a.system)
     ctx = GTOContext(system)
     t_spec = time.perf_counter()
-    ctx.specialize()                 # NVRTC-compiled kernels for this molecule
+    if not a.generic:
+        ctx.specialize()             # NVRTC-compiled kernels for this molecule
     t_spec = time.perf_counter() - t_spec
     if a.proposal == "scaled":
         ctx.set_proposal(1, SCALED_R0, SCALED_FMIN)
@@ -549,7 +553,8 @@ def run_ours(a):
                    "precision": a.precision, "walkers_per_gpu": W, "step": step,
                    "parallelism": f"replicas x{world}",
                    "trial": "RHF determinant + Pade J2 (b=3)",
-                   "kernels": f"NVRTC-specialised to the molecule (compile {t_spec:.1f} s, untimed)",
+                   "kernels": ("table-driven (generic) kernels" if a.generic else
+                               f"NVRTC-specialised to the molecule (compile {t_spec:.1f} s, untimed)"),
                    "local_energy": "tcgen05 tensor cores (split TF32/BF16)" if a.eloc == "tc"
                                    else "CUDA cores",
                    "proposal": (f"nucleus-scaled Gaussian (r0={SCALED_R0}, fmin={SCALED_FMIN}), "
