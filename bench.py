@@ -534,6 +534,8 @@ def run_ours(a):
     wss = W * world * K / (ms_max * 1e-3)
     value = wss / kappa
     work = work_per_walker_sweep(system, acc)
+    if a.generic:   # the table-driven kernels evaluate every MO coefficient
+        work["flops"], work["mo_terms"] = work["flops_dense"], system.nbf * system.nocc
     peak_kind = 0 if a.precision == "fp64" else 1
     rate = ctypes_peak(L, peak_kind)
     achieved = work["flops"] * W * REFRESH_EVERY / (sweep_ms * 1e-3)
