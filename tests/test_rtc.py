@@ -88,3 +88,19 @@ def test_generated_code_leaves_out_round_off_coefficients():
     # the dropped ones are round-off: below 1e-12 of their orbital's scale
     small = C[(C > 0) & (C <= 1e-12 * C.max(axis=0, keepdims=True))]
     assert small.size == C.size - len(kept) - np.count_nonzero(C == 0)
+
+
+def test_spec_compiles_with_f_and_g_shells():
+    """The generated orbital code of a basis with f and g shells (the
+    reference-made golden case) compiles for sm_100a, contracted form
+    included."""
+    try:
+        R._nvrtc()
+    except OSError:
+        pytest.skip("NVRTC not installed")
+    from helpers import golden_system
+    s, _ = golden_system("fg_shells")
+    src = R.spec_source(s)
+    assert "oq_harm_table" in src
+    ok, log, cubin = R.compile_spec(s)
+    assert ok, log
