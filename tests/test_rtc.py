@@ -69,7 +69,8 @@ def test_tuned_batch_module_compiles_for_sm100a():
     assert ok0 and len(cubin) < len(cubin0)
 
 
-def test_generated_code_leaves_out_round_off_coefficients():
+@pytest.mark.parametrize("name", ["H2O", "LiH", "N2"])
+def test_generated_code_leaves_out_round_off_coefficients(name):
     """H2O (C2v) orbitals have exact zeros on the AOs of other irreducible
     representations, which the eigensolver returns at ~1e-15: the generated
     MO-value code evaluates only the coefficients above 1e-12 of their
@@ -77,7 +78,7 @@ def test_generated_code_leaves_out_round_off_coefficients():
     import re
     import numpy as np
     import bench
-    mf = M.make_mf("H2O")
+    mf = M.make_mf(name)
     s = build_system(mf, M.benchmark_params_corr(mf.mol))
     src = R.spec_source(s)
     mo_val = src.split("mo_vgl(")[0]
